@@ -1,0 +1,221 @@
+/*
+ * brkga_b200.h -- C ABI of the B200 BRKGA generation engine (libbrkga_b200.so).
+ *
+ * Plain pointers and sizes only.  Every call returns a brkga_status (0 = OK, negative =
+ * error) and records a message readable with brkga_last_error() on the calling thread.
+ * Device pointers are CUDA global-memory pointers on the engine's device; `stream` may
+ * be 0 (legacy default stream) or any cudaStream_t of that device, passed as void*.
+ *
+ * Each entry point names the reference interface it replaces (paths relative to the
+ * hsaseendran/llm-brkga tree).
+ */
+#ifndef BRKGA_B200_H
+#define BRKGA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BRKGA_B200_ABI_VERSION 1
+
+typedef enum {
+    BRKGA_OK = 0,
+    BRKGA_ERR_INVALID = -1,      /* bad argument (reference: BRKGAConfig::is_valid, core/config.hpp:159-179) */
+    BRKGA_ERR_OOM = -2,          /* device allocation failed                                              */
+    BRKGA_ERR_CUDA = -3,         /* a CUDA call failed                                                    */
+    BRKGA_ERR_TIMEOUT = -4,      /* a bounded device wait ran out                                         */
+    BRKGA_ERR_CANCELLED = -5,    /* request cancelled                                                     */
+    BRKGA_ERR_UNSUPPORTED = -6,  /* size or mode outside what this build handles                          */
+    BRKGA_ERR_BUSY = -7,         /* admission refused (not enough free device memory / slots)             */
+    BRKGA_ERR_NOT_READY = -8     /* result not available yet                                              */
+} brkga_status;
+
+/* problem kinds: the reference's problem configs (brkga/configs/) */
+typedef enum {
+    BRKGA_TSP_COORDS = 1,        /* TSPConfig, Euclidean from coordinates (configs/tsp_config.hpp:301-380)   */
+    BRKGA_TSP_MATRIX = 2,        /* TSPConfig(dist, name) with an explicit [n][n] matrix (tsp_config.hpp:38)  */
+    BRKGA_KNAP_THRESHOLD = 3,    /* KnapsackConfig: gene > 0.5 selects, penalty x1000 (knapsack_config.hpp:43) */
+    BRKGA_KNAP_GREEDY = 4,       /* key-order first-fit greedy knapsack (no reference counterpart)          */
+    BRKGA_BITSP_COORDS = 5,      /* MultiTSPConfig with two coordinate sets, depot = point 0                */
+    BRKGA_BITSP_MATRIX = 6       /* MultiTSPConfig(dist, time, name) (configs/multi_tsp_config.hpp:25-52)   */
+} brkga_problem_kind;
+
+/* Instance data (HOST pointers; copied to the device at creation).
+ *   TSP:      n cities; coords [n][2] or matrix [n][n]
+ *   bi-TSP:   n genes, n+1 points with point 0 the depot; coords/coords2 [n+1][2] or
+ *             matrix/matrix2 [n+1][n+1]
+ *   knapsack: n items; weights, values [n] (integers); capacity                        */
+typedef struct {
+    int32_t kind;
+    int32_t n;
+    const float* coords;
+    const float* coords2;
+    const float* matrix;
+    const float* matrix2;
+    const int32_t* weights;
+    const int32_t* values;
+    float capacity;
+} brkga_problem_desc;
+
+/* GA parameters (BRKGAConfig fields, core/config.hpp:17-30, plus the engine's own). */
+typedef struct {
+    int32_t population_size;     /* P                                                         */
+    int32_t elite_size;          /* E (absolute, like the reference)                          */
+    int32_t mutant_size;         /* M; for NSGA-II: fresh random offspring per generation     */
+    double elite_prob;           /* rho                                                       */
+    int32_t max_generations;     /* generation budget used by brkga_run                       */
+    uint64_t seed;               /* Philox key: the whole run is a function of the seed       */
+    int32_t num_islands;         /* >= 1; islands split P evenly (core/solver.hpp:378-476)    */
+    int32_t migration_interval;  /* generations between ring migrations (0 = never)          */
+    int32_t num_migrants;        /* rows sent to the next island per migration                */
+    int32_t device;              /* CUDA device ordinal                                       */
+    int32_t diversity_interval;  /* NSGA-II ensure_minimum_diversity period (0 = off)         */
+    double mutation_rate;        /* NSGA-II per-gene reset rate (<= 0: the reference's 5/n)   */
+} brkga_params;
+
+typedef struct brkga_problem brkga_problem;
+typedef struct brkga_engine brkga_engine;
+
+/* ---- library ------------------------------------------------------------------------- */
+int32_t brkga_abi_version(void);
+/* copy the calling thread's last error message (NUL-terminated, truncated to cap) */
+int32_t brkga_last_error(char* buf, size_t cap);
+/* fill p with the reference's defaults (core/config.hpp:78-84: P=100, E=20, M=10,
+ * rho=0.7, 1000 generations) and the engine's (seed 1, 1 island, device 0) */
+void brkga_params_default(brkga_params* p);
+
+/* ---- problem instances (TSPConfig / KnapsackConfig / MultiTSPConfig device data) ------- */
+/* Uploads the instance to `device`.  Replaces the per-device data map and its lazy upload
+ * in TSPConfig::ensure_gpu_memory (configs/tsp_config.hpp:125-165) and
+ * KnapsackGPUConfig::allocate_gpu_memory (configs/knapsack_gpu_config.hpp:104-140). */
+int32_t brkga_problem_create(const brkga_problem_desc* desc, int32_t device, brkga_problem** out);
+int32_t brkga_problem_destroy(brkga_problem* pb);
+int32_t brkga_problem_num_objectives(const brkga_problem* pb);
+int32_t brkga_problem_maximize(const brkga_problem* pb);
+
+/* Drop-in for BRKGAConfig::evaluate_population_gpu(T* d_population, T* d_fitness,
+ * int pop_size, int chrom_len) (core/config.hpp:50-53; TSP: configs/tsp_config.hpp:70-111,
+ * knapsack: configs/knapsack_gpu_config.hpp:66-88).  d_population is [pop_size][ld] float
+ * keys on the device (the reference's dense layout is ld == chrom_len); d_fitness is
+ * [pop_size][num_objectives].  d_perm (optional, may be NULL) receives the decoded
+ * permutation [pop_size][chrom_len] (configs/tsp_config.hpp:206-225).  Asynchronous on
+ * `stream`; the reference's call is synchronous -- brkga_evaluate_population_sync waits. */
+int32_t brkga_evaluate_population(brkga_problem* pb, const float* d_population, float* d_fitness,
+                                  int32_t pop_size, int32_t chrom_len, int32_t ld, int32_t* d_perm,
+                                  void* stream);
+int32_t brkga_evaluate_population_sync(brkga_problem* pb, const float* d_population, float* d_fitness,
+                                       int32_t pop_size, int32_t chrom_len);
+
+/* ---- operators on device buffers (the hot path, one call each) ------------------------- */
+/* Elite partition: sorted[r] = row of rank r by (fitness, row) ascending, or fitness
+ * descending with ties by row when maximize.  Replaces thrust::sequence +
+ * thrust::sort_by_key (core/solver.hpp:329-338) and Population::sort
+ * (core/population.hpp:660-682).  `segments` populations of `P` rows each, back to back. */
+int32_t brkga_sort_fitness(const float* d_fitness, int32_t P, int32_t segments, int32_t maximize,
+                           int32_t* d_sorted, void* stream);
+
+/* Fused generation step for one population: elite copy, biased crossover, mutant fill,
+ * decode and fitness of rows [E, P) written to d_next / d_next_fitness.  Replaces
+ * brkga_generation_kernel (core/cuda_kernels.cuh:88-138) and the host path
+ * evolve_generation_brkga (core/solver.hpp:234-273, 1109-1135, 1244-1258).  Draws come
+ * from Philox keyed by (seed, generation, row, gene). */
+int32_t brkga_generation_step(brkga_problem* pb, const float* d_pop, const float* d_fitness,
+                              const int32_t* d_sorted, float* d_next, float* d_next_fitness,
+                              int32_t P, int32_t E, int32_t M, double elite_prob, int32_t ld,
+                              uint64_t seed, uint32_t generation, int32_t island, void* stream);
+
+/* Initial population (Population::initialize, core/population.hpp:107-124): Philox keys
+ * for generation 0 and their fitness. */
+int32_t brkga_init_population(brkga_problem* pb, float* d_pop, float* d_fitness, int32_t P, int32_t ld,
+                              uint64_t seed, int32_t island, void* stream);
+
+/* Pareto ranks of N points with m objectives (minimisation), d_obj [N][m].  Replaces
+ * Population::fast_non_dominated_sort (core/population.hpp:409-440). */
+int32_t brkga_pareto_rank(const float* d_obj, int32_t N, int32_t m, int32_t* d_rank, void* stream);
+/* The same ranks through the bit-packed dominance matrix for any m: row i, bit j set when
+ * point j dominates point i, built 32 columns per __ballot_sync; domination counts and
+ * front peeling by __popc of row & front-mask words.  Uses an internal device scratch of
+ * N*ceil(N/32)*4 bytes and returns after the ranks are written. */
+int32_t brkga_pareto_rank_bitmatrix(const float* d_obj, int32_t N, int32_t m, int32_t* d_rank, void* stream);
+/* Crowding distance per front (core/population.hpp:453-489), fronts from d_rank. */
+int32_t brkga_crowding(const float* d_obj, const int32_t* d_rank, int32_t N, int32_t m, float* d_cd,
+                       void* stream);
+
+/* ---- solver (Solver<T>, core/solver.hpp:44-1726) ---------------------------------------- */
+/* Creates the device-resident population for problem `pb` (the engine keeps its own
+ * reference to the instance; pb may be destroyed afterwards).  Single-objective problems
+ * run BRKGA; bi-objective ones run NSGA-II (core/solver.hpp:213-231). */
+int32_t brkga_create(brkga_problem* pb, const brkga_params* params, brkga_engine** out);
+int32_t brkga_destroy(brkga_engine* e);
+/* Solver::initialize (core/solver.hpp:190-211) */
+int32_t brkga_initialize(brkga_engine* e);
+/* `generations` calls of Solver::evolve_generation (core/solver.hpp:213-231), enqueued on
+ * the engine's stream (captured once as a CUDA graph); returns after enqueueing. */
+int32_t brkga_evolve(brkga_engine* e, int32_t generations);
+/* wait for the engine's queued work */
+int32_t brkga_synchronize(brkga_engine* e);
+/* Solver::run (core/solver.hpp:1517-1556): initialize + max_generations + wait */
+int32_t brkga_run(brkga_engine* e);
+int32_t brkga_generation(const brkga_engine* e);
+/* Solver::get_best_individual (core/solver.hpp:1625): keys [n], decoded permutation [n]
+ * (may be NULL), objective values [num_objectives]; host buffers, waits for the engine. */
+int32_t brkga_get_best(brkga_engine* e, float* keys, int32_t* perm, float* fitness);
+/* Solver::get_fitness_history (core/solver.hpp:1633): best fitness per generation,
+ * history[0] = initial population; *len receives the number written (<= cap). */
+int32_t brkga_get_fitness_history(brkga_engine* e, float* history, int32_t cap, int32_t* len);
+/* whole population in rank order (host buffers): keys [P][n], fitness [P][m] (either may
+ * be NULL).  Islands are returned one after another. */
+int32_t brkga_get_population(brkga_engine* e, float* keys, float* fitness);
+/* replace the population (host buffers, keys [P][n]) and re-evaluate it; the next
+ * generation number stays where it is. */
+int32_t brkga_set_population(brkga_engine* e, const float* keys);
+/* Solver::get_pareto_front (core/solver.hpp:1629): rank-0 members; objectives [cap][m],
+ * keys [cap][n] (may be NULL); *count receives the front size (may exceed cap). */
+int32_t brkga_get_pareto_front(brkga_engine* e, float* objectives, float* keys, int32_t cap, int32_t* count);
+
+/* ---- batched solving (many independent instances advanced together) --------------------- */
+typedef struct brkga_batch brkga_batch;
+/* `count` problems with their own parameters; all on params[0].device. */
+int32_t brkga_batch_create(brkga_problem* const* problems, const brkga_params* params, int32_t count,
+                           brkga_batch** out);
+int32_t brkga_batch_destroy(brkga_batch* b);
+int32_t brkga_batch_evolve(brkga_batch* b, int32_t generations);
+int32_t brkga_batch_synchronize(brkga_batch* b);
+/* best objective of every instance (host [count][2], second entry unused for
+ * single-objective); waits for the batch */
+int32_t brkga_batch_get_best(brkga_batch* b, float* best);
+int32_t brkga_batch_get_best_keys(brkga_batch* b, int32_t index, float* keys, float* fitness);
+
+/* ---- serving: continuous batching of solve requests ------------------------------------- */
+typedef struct brkga_server brkga_server;
+typedef struct {
+    int32_t device;
+    int32_t max_active;          /* slots on the device                                       */
+    int64_t memory_budget;       /* bytes of device memory the server may hold (0 = free HBM) */
+    int32_t generations_per_tick;/* generations advanced per scheduling round                 */
+} brkga_server_config;
+
+int32_t brkga_server_create(const brkga_server_config* cfg, brkga_server** out);
+int32_t brkga_server_destroy(brkga_server* s);
+/* queue a request; the problem data is copied, so desc's buffers may be freed after the
+ * call.  params->max_generations is the request's generation budget; stall_generations
+ * (0 = off) retires it early after that many generations without improvement. */
+int32_t brkga_server_submit(brkga_server* s, const brkga_problem_desc* desc, const brkga_params* params,
+                            int32_t stall_generations, int64_t* request_id);
+/* run one scheduling round: admit queued requests, advance active ones, retire finished */
+int32_t brkga_server_step(brkga_server* s);
+/* result of a finished request: best objectives [2], generations run, and its latency
+ * (submit -> retire) in seconds; BRKGA_ERR_NOT_READY while pending. */
+int32_t brkga_server_poll(brkga_server* s, int64_t request_id, float* best, int32_t* generations,
+                          double* latency_s);
+int32_t brkga_server_cancel(brkga_server* s, int64_t request_id);
+/* queued, active, finished counts */
+int32_t brkga_server_stats(brkga_server* s, int32_t* queued, int32_t* active, int32_t* finished);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

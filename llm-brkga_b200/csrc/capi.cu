@@ -1,0 +1,339 @@
+// capi.cu -- the C ABI (include/brkga_b200.h): problem instances, operators on device
+// buffers, and the device-resident solver engine.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/brkga_b200.h"
+#include "engine.h"
+#include "kernels.h"
+
+namespace bk {
+
+// ---------------------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------------------
+static thread_local std::string g_err;
+
+int32_t fail(int32_t code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+int32_t cuda_fail(cudaError_t e, const char* what) {
+    return fail(BRKGA_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+DeviceGuard::DeviceGuard(int dev) {
+    cudaGetDevice(&prev_);
+    ok_ = cudaSetDevice(dev) == cudaSuccess;
+}
+DeviceGuard::~DeviceGuard() { cudaSetDevice(prev_); }
+
+// ---------------------------------------------------------------------------------------
+// problem data
+// ---------------------------------------------------------------------------------------
+ProblemData::~ProblemData() {
+    DeviceGuard g(device);
+    for (void* p : allocs) cudaFree(p);
+}
+
+static int32_t upload(ProblemData& pd, const void* host, size_t bytes, void** dev) {
+    if (!host) return fail(BRKGA_ERR_INVALID, "missing instance array");
+    cudaError_t e = cudaMalloc(dev, bytes ? bytes : 4);
+    if (e != cudaSuccess) return fail(BRKGA_ERR_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    pd.allocs.push_back(*dev);
+    e = cudaMemcpy(*dev, host, bytes, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpy instance");
+    pd.bytes += bytes;
+    return BRKGA_OK;
+}
+
+int32_t make_problem(const brkga_problem_desc* d, int device, std::shared_ptr<ProblemData>* out) {
+    if (!d) return fail(BRKGA_ERR_INVALID, "null problem description");
+    const int n = d->n;
+    if (n < 1) return fail(BRKGA_ERR_INVALID, "chromosome length must be >= 1");
+    if (n > row_max_n())
+        return fail(BRKGA_ERR_UNSUPPORTED, "chromosome length " + std::to_string(n) + " exceeds " +
+                                               std::to_string(row_max_n()));
+    auto pd = std::make_shared<ProblemData>();
+    pd->device = device;
+    pd->kind = d->kind;
+    pd->n = n;
+    DeviceGuard g(device);
+    if (!g.ok()) return fail(BRKGA_ERR_CUDA, "cannot select device " + std::to_string(device));
+    int32_t st = BRKGA_OK;
+    void* p = nullptr;
+    switch (d->kind) {
+    case BRKGA_TSP_COORDS:
+        pd->m = 1;
+        st = upload(*pd, d->coords, (size_t)n * 8, &p);
+        pd->xy = (float*)p;
+        break;
+    case BRKGA_TSP_MATRIX:
+        pd->m = 1;
+        st = upload(*pd, d->matrix, (size_t)n * n * 4, &p);
+        pd->mat = (float*)p;
+        break;
+    case BRKGA_BITSP_COORDS:
+        pd->m = 2;
+        st = upload(*pd, d->coords, (size_t)(n + 1) * 8, &p);
+        pd->xy = (float*)p;
+        if (st == BRKGA_OK) st = upload(*pd, d->coords2, (size_t)(n + 1) * 8, &p);
+        pd->xy2 = (float*)p;
+        break;
+    case BRKGA_BITSP_MATRIX:
+        pd->m = 2;
+        st = upload(*pd, d->matrix, (size_t)(n + 1) * (n + 1) * 4, &p);
+        pd->mat = (float*)p;
+        if (st == BRKGA_OK) st = upload(*pd, d->matrix2, (size_t)(n + 1) * (n + 1) * 4, &p);
+        pd->mat2 = (float*)p;
+        break;
+    case BRKGA_KNAP_THRESHOLD:
+    case BRKGA_KNAP_GREEDY: {
+        pd->m = 1;
+        pd->maximize = 1;
+        if (!d->weights || !d->values) return fail(BRKGA_ERR_INVALID, "knapsack needs weights and values");
+        for (int i = 0; i < n; ++i)
+            if (d->weights[i] < 0) return fail(BRKGA_ERR_INVALID, "knapsack weights must be >= 0");
+        if (!std::isfinite(d->capacity) || d->capacity < 0.0f)
+            return fail(BRKGA_ERR_INVALID, "knapsack capacity must be finite and >= 0");
+        pd->cap = d->capacity;
+        pd->capi = (long long)std::floor((double)d->capacity);
+        st = upload(*pd, d->weights, (size_t)n * 4, &p);
+        pd->w = (int32_t*)p;
+        if (st == BRKGA_OK) st = upload(*pd, d->values, (size_t)n * 4, &p);
+        pd->v = (int32_t*)p;
+        break;
+    }
+    default:
+        return fail(BRKGA_ERR_INVALID, "unknown problem kind " + std::to_string(d->kind));
+    }
+    if (st != BRKGA_OK) return st;
+    *out = pd;
+    return BRKGA_OK;
+}
+
+void fill_instance(PopDesc& d, const ProblemData& pd) {
+    std::memset(&d, 0, sizeof(d));
+    d.kind = pd.kind;
+    d.n = pd.n;
+    d.ld = round_up(pd.n, 4);
+    d.m = pd.m;
+    d.xy = pd.xy;
+    d.xy2 = pd.xy2;
+    d.mat = pd.mat;
+    d.mat2 = pd.mat2;
+    d.w = pd.w;
+    d.v = pd.v;
+    d.cap = pd.cap;
+    d.capi = pd.capi;
+    d.maximize = pd.maximize;
+}
+
+int points_of(const ProblemData& pd) { return (pd.kind == BRKGA_BITSP_COORDS) ? pd.n + 1 : pd.n; }
+
+bool stage_fits(const RowTile& t, int n, int pts, int kind) {
+    return row_smem_bytes(t, n, pts, kind, true) <= kMaxSmem;
+}
+
+uint32_t prob_threshold(double p) {
+    if (!(p > 0.0)) return 0u;
+    if (p >= 1.0) return 1u << 24;
+    double t = std::ceil(p * 16777216.0);
+    if (t > 16777216.0) t = 16777216.0;
+    return (uint32_t)t;
+}
+
+}  // namespace bk
+
+using namespace bk;
+
+struct brkga_problem {
+    std::shared_ptr<ProblemData> d;
+};
+
+extern "C" {
+
+int32_t brkga_abi_version(void) { return BRKGA_B200_ABI_VERSION; }
+
+int32_t brkga_last_error(char* buf, size_t cap) {
+    if (!buf || cap == 0) return BRKGA_ERR_INVALID;
+    const size_t n = std::min(cap - 1, g_err.size());
+    std::memcpy(buf, g_err.data(), n);
+    buf[n] = '\0';
+    return BRKGA_OK;
+}
+
+void brkga_params_default(brkga_params* p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->population_size = 100;
+    p->elite_size = 20;
+    p->mutant_size = 10;
+    p->elite_prob = 0.7;
+    p->max_generations = 1000;
+    p->seed = 1;
+    p->num_islands = 1;
+    p->migration_interval = 0;
+    p->num_migrants = 0;
+    p->device = 0;
+    p->diversity_interval = 25;
+    p->mutation_rate = 0.0;
+}
+
+int32_t brkga_problem_create(const brkga_problem_desc* desc, int32_t device, brkga_problem** out) {
+    if (!out) return fail(BRKGA_ERR_INVALID, "null output handle");
+    *out = nullptr;
+    std::shared_ptr<ProblemData> pd;
+    int32_t st = make_problem(desc, device, &pd);
+    if (st != BRKGA_OK) return st;
+    *out = new brkga_problem{pd};
+    return BRKGA_OK;
+}
+
+int32_t brkga_problem_destroy(brkga_problem* pb) {
+    delete pb;
+    return BRKGA_OK;
+}
+
+int32_t brkga_problem_num_objectives(const brkga_problem* pb) { return pb ? pb->d->m : BRKGA_ERR_INVALID; }
+int32_t brkga_problem_maximize(const brkga_problem* pb) { return pb ? pb->d->maximize : BRKGA_ERR_INVALID; }
+
+int32_t brkga_evaluate_population(brkga_problem* pb, const float* d_population, float* d_fitness,
+                                  int32_t pop_size, int32_t chrom_len, int32_t ld, int32_t* d_perm,
+                                  void* stream) {
+    if (!pb || !d_population || !d_fitness) return fail(BRKGA_ERR_INVALID, "null argument");
+    const ProblemData& pd = *pb->d;
+    if (chrom_len != pd.n)
+        return fail(BRKGA_ERR_INVALID, "chrom_len " + std::to_string(chrom_len) + " != problem size " +
+                                           std::to_string(pd.n));
+    if (pop_size < 0) return fail(BRKGA_ERR_INVALID, "negative pop_size");
+    if (ld <= 0) ld = chrom_len;
+    if (ld < chrom_len) return fail(BRKGA_ERR_INVALID, "ld < chrom_len");
+    if (pop_size == 0) return BRKGA_OK;
+    DeviceGuard g(pd.device);
+    RowLaunch L;
+    std::memset(&L, 0, sizeof(L));
+    fill_instance(L.single, pd);
+    L.single.ld = ld;
+    L.single.keys[0] = const_cast<float*>(d_population);
+    L.single.fit[0] = d_fitness;
+    L.single.P = pop_size;
+    L.ntasks = pop_size;
+    L.mode = MODE_EVAL;
+    L.perm_out = d_perm;
+    L.max_n = pd.n;
+    L.max_points = points_of(pd);
+    const RowTile tile = pick_tile(pd.n);
+    L.stage_xy = stage_fits(tile, pd.n, L.max_points, pd.kind) ? 1 : 0;
+    cudaError_t e = launch_rows_auto(L, pd.kind, tile, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "evaluate launch");
+    return BRKGA_OK;
+}
+
+int32_t brkga_evaluate_population_sync(brkga_problem* pb, const float* d_population, float* d_fitness,
+                                       int32_t pop_size, int32_t chrom_len) {
+    int32_t st = brkga_evaluate_population(pb, d_population, d_fitness, pop_size, chrom_len, chrom_len,
+                                           nullptr, nullptr);
+    if (st != BRKGA_OK) return st;
+    DeviceGuard g(pb->d->device);
+    cudaError_t e = cudaStreamSynchronize(nullptr);
+    if (e != cudaSuccess) return cuda_fail(e, "evaluate");
+    return BRKGA_OK;
+}
+
+int32_t brkga_sort_fitness(const float* d_fitness, int32_t P, int32_t segments, int32_t maximize,
+                           int32_t* d_sorted, void* stream) {
+    if (!d_fitness || !d_sorted) return fail(BRKGA_ERR_INVALID, "null argument");
+    if (P < 0 || segments < 0) return fail(BRKGA_ERR_INVALID, "negative size");
+    if (P > kMaxPop) return fail(BRKGA_ERR_UNSUPPORTED, "population above " + std::to_string(kMaxPop));
+    if (P == 0 || segments == 0) return BRKGA_OK;
+    cudaError_t e = prepare_sort(P);
+    if (e != cudaSuccess) return cuda_fail(e, "sort setup");
+    e = launch_sort_raw(d_fitness, P, segments, maximize ? 1 : 0, d_sorted, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "sort launch");
+    return BRKGA_OK;
+}
+
+int32_t brkga_generation_step(brkga_problem* pb, const float* d_pop, const float* d_fitness,
+                              const int32_t* d_sorted, float* d_next, float* d_next_fitness, int32_t P,
+                              int32_t E, int32_t M, double elite_prob, int32_t ld, uint64_t seed,
+                              uint32_t generation, int32_t island, void* stream) {
+    if (!pb || !d_pop || !d_fitness || !d_sorted || !d_next || !d_next_fitness)
+        return fail(BRKGA_ERR_INVALID, "null argument");
+    const ProblemData& pd = *pb->d;
+    if (pd.m != 1) return fail(BRKGA_ERR_INVALID, "generation step is single-objective");
+    if (P <= 0 || E <= 0 || M < 0 || E + M > P) return fail(BRKGA_ERR_INVALID, "need P > 0, E > 0, E + M <= P");
+    if (!(elite_prob >= 0.0 && elite_prob <= 1.0)) return fail(BRKGA_ERR_INVALID, "elite_prob outside [0,1]");
+    if (generation < 1) return fail(BRKGA_ERR_INVALID, "generation must be >= 1");
+    if (ld <= 0) ld = round_up(pd.n, 4);
+    if (ld % 4 != 0 || ld < pd.n) return fail(BRKGA_ERR_INVALID, "ld must be a multiple of 4 and >= n");
+    if (((uintptr_t)d_pop | (uintptr_t)d_next) & 15) return fail(BRKGA_ERR_INVALID, "buffers must be 16-byte aligned");
+    RowLaunch L;
+    std::memset(&L, 0, sizeof(L));
+    fill_instance(L.single, pd);
+    L.single.ld = ld;
+    L.single.keys[0] = const_cast<float*>(d_pop);
+    L.single.keys[1] = d_next;
+    L.single.fit[0] = const_cast<float*>(d_fitness);
+    L.single.fit[1] = d_next_fitness;
+    L.single.sorted = const_cast<int32_t*>(d_sorted);
+    L.single.P = P;
+    L.single.E = E;
+    L.single.M = M;
+    L.single.rhoT = prob_threshold(elite_prob);
+    L.single.seed = seed;
+    L.single.island = (uint32_t)island;
+    L.single.gen = generation - 1;
+    L.ntasks = P;
+    L.mode = MODE_GEN;
+    L.max_n = pd.n;
+    L.max_points = points_of(pd);
+    const RowTile tile = pick_tile(pd.n);
+    L.stage_xy = stage_fits(tile, pd.n, L.max_points, pd.kind) ? 1 : 0;
+    DeviceGuard g(pd.device);
+    cudaError_t e = launch_rows_auto(L, pd.kind, tile, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "generation launch");
+    return BRKGA_OK;
+}
+
+int32_t brkga_init_population(brkga_problem* pb, float* d_pop, float* d_fitness, int32_t P, int32_t ld,
+                              uint64_t seed, int32_t island, void* stream) {
+    if (!pb || !d_pop || !d_fitness) return fail(BRKGA_ERR_INVALID, "null argument");
+    const ProblemData& pd = *pb->d;
+    if (P <= 0) return fail(BRKGA_ERR_INVALID, "P must be > 0");
+    if (ld <= 0) ld = round_up(pd.n, 4);
+    if (ld % 4 != 0 || ld < pd.n) return fail(BRKGA_ERR_INVALID, "ld must be a multiple of 4 and >= n");
+    if ((uintptr_t)d_pop & 15) return fail(BRKGA_ERR_INVALID, "buffer must be 16-byte aligned");
+    RowLaunch L;
+    std::memset(&L, 0, sizeof(L));
+    fill_instance(L.single, pd);
+    L.single.ld = ld;
+    L.single.keys[0] = d_pop;
+    L.single.fit[0] = d_fitness;
+    L.single.P = P;
+    L.single.seed = seed;
+    L.single.island = (uint32_t)island;
+    L.ntasks = P;
+    L.mode = MODE_INIT;
+    L.max_n = pd.n;
+    L.max_points = points_of(pd);
+    const RowTile tile = pick_tile(pd.n);
+    L.stage_xy = stage_fits(tile, pd.n, L.max_points, pd.kind) ? 1 : 0;
+    DeviceGuard g(pd.device);
+    cudaError_t e = launch_rows_auto(L, pd.kind, tile, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "init launch");
+    return BRKGA_OK;
+}
+
+}  // extern "C"
+
+// problem handle accessor for the other translation units
+namespace bk {
+std::shared_ptr<ProblemData> problem_data(brkga_problem* pb) { return pb ? pb->d : nullptr; }
+}  // namespace bk

@@ -1,0 +1,158 @@
+// common.cuh -- device primitives shared by every kernel of the engine:
+// the Philox4x32-10 counter-based stream, the order-preserving key map, the
+// population descriptor and small block-level collectives.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace bk {
+
+// ---------------------------------------------------------------------------------------
+// problem kinds (mirror include/brkga_b200.h)
+// ---------------------------------------------------------------------------------------
+enum Kind : int32_t {
+    TSP_COORDS = 1,
+    TSP_MATRIX = 2,
+    KNAP_THRESHOLD = 3,
+    KNAP_GREEDY = 4,
+    BITSP_COORDS = 5,
+    BITSP_MATRIX = 6,
+};
+
+// stream tags: Philox counter word 3 = (island << 8) | tag
+enum Tag : uint32_t {
+    TAG_INIT = 1,
+    TAG_MUTANT = 2,
+    TAG_COIN = 3,
+    TAG_PARENT = 4,
+    TAG_NSGA_TOUR = 5,
+    TAG_NSGA_COIN = 6,
+    TAG_NSGA_MUTP = 7,
+    TAG_NSGA_MUTK = 8,
+    TAG_NSGA_REFILL = 9,
+};
+
+// ---------------------------------------------------------------------------------------
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11): replaces the reference's stateful
+// cuRAND XORWOW states (core/cuda_kernels.cuh:10-15) -- nothing is stored per individual,
+// every draw is a pure function of (seed, generation, row, gene).
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ uint4 philox(uint4 c, uint32_t k0, uint32_t k1) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint32_t hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
+        const uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
+        c = make_uint4(hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0);
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    return c;
+}
+
+__device__ __forceinline__ uint4 draw4(uint64_t seed, uint32_t word, uint32_t row, uint32_t gen,
+                                       uint32_t stream) {
+    return philox(make_uint4(word, row, gen, stream), (uint32_t)seed, (uint32_t)(seed >> 32));
+}
+
+// top 24 bits -> float in [0,1): exact (24-bit integer times 2^-24)
+__device__ __forceinline__ float u24(uint32_t x) { return (float)(x >> 8) * (1.0f / 16777216.0f); }
+// floor(x * k / 2^32)
+__device__ __forceinline__ uint32_t pick(uint32_t x, uint32_t k) { return __umulhi(x, k); }
+
+// order-preserving float -> uint32 (-0 folded onto +0, every NaN above +inf)
+__device__ __forceinline__ uint32_t okey(float f) {
+    uint32_t b = __float_as_uint(f);
+    if ((b & 0x7F800000u) == 0x7F800000u && (b & 0x007FFFFFu)) return 0xFFFFFFFFu;
+    if (b == 0x80000000u) b = 0u;
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+// fitness order key: ascending for minimisation, descending for maximisation; NaN last
+__device__ __forceinline__ uint32_t fitkey(float f, int maximize) {
+    const uint32_t k = okey(f);
+    if (!maximize || k == 0xFFFFFFFFu) return k;
+    return ~k;
+}
+
+// ---------------------------------------------------------------------------------------
+// population descriptor.  Device-resident copies are updated in place by the sort kernel
+// (ping-pong buffer index and generation counter), so a captured CUDA graph of
+// [generation kernel, sort kernel] can be replayed any number of times.
+// ---------------------------------------------------------------------------------------
+struct PopDesc {
+    // instance
+    int32_t kind, n, ld, m;   // m = number of objectives (1 or 2)
+    const float* xy;          // TSP [n][2]; bi-TSP [n+1][2]
+    const float* xy2;
+    const float* mat;         // TSP [n][n]; bi-TSP [n+1][n+1]
+    const float* mat2;
+    const int32_t* w;
+    const int32_t* v;
+    float cap;                // knapsack capacity (threshold fitness, float like the reference)
+    int32_t maximize;
+    long long capi;           // floor(cap) for the greedy decoder
+    // GA parameters
+    int32_t P, E, M;
+    uint32_t rhoT;            // coin threshold: elite gene iff (x >> 8) < rhoT
+    uint64_t seed;
+    uint32_t island;          // stream high bits (island << 8)
+    int32_t row0;             // first row of this population inside the key buffers
+    // state
+    float* keys[2];
+    float* fit[2];            // [rows][m]
+    int32_t* sorted;          // rank -> row (relative to row0) of keys[cur]
+    float* history;           // best fitness per generation
+    int32_t hist_cap;
+    int32_t cur;
+    uint32_t gen;
+    int32_t pad_;
+};
+
+// ---------------------------------------------------------------------------------------
+// block collectives
+// ---------------------------------------------------------------------------------------
+template <int BLOCK>
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* warp_tot, uint32_t* total) {
+    constexpr int NW = BLOCK / 32;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_tot[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        uint32_t s = (lane < NW) ? warp_tot[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane >= o) s += y;
+        }
+        if (lane < NW) warp_tot[lane] = s;
+    }
+    __syncthreads();
+    const uint32_t base = (w > 0) ? warp_tot[w - 1] : 0u;
+    if (total) *total = warp_tot[NW - 1];
+    return base + x - v;
+}
+
+template <int BLOCK>
+__device__ __forceinline__ long long block_sum_ll(long long v, long long* red) {
+    constexpr int NW = BLOCK / 32;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) red[w] = v;
+    __syncthreads();
+    long long s = 0;
+#pragma unroll
+    for (int i = 0; i < NW; ++i) s += red[i];
+    __syncthreads();
+    return s;
+}
+
+__host__ __device__ __forceinline__ int round_up(int x, int m) { return (x + m - 1) / m * m; }
+
+}  // namespace bk

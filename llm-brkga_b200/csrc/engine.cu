@@ -1,0 +1,590 @@
+// engine.cu -- the device-resident solver (Solver<T>, core/solver.hpp), the drop-in for
+// the reference's run / evolve_generation / get_best_individual surface.
+//
+// The population, its fitness, the rank order and the best-fitness history stay in HBM
+// for the whole run; one generation is two launches (the fused row kernel and the
+// elite-partition sort) that read their state from device-resident descriptors, so the
+// sequence is captured once as a CUDA graph and replayed.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <string>
+#include <vector>
+
+#include "engine.h"
+#include "nsga2.h"
+
+namespace bk {
+
+int32_t make_shape(const ProblemData& pd, const brkga_params& p, Shape* s) {
+    Shape sh;
+    sh.n = pd.n;
+    sh.ld = round_up(pd.n, 4);
+    sh.m = pd.m;
+    sh.mo = pd.m > 1;
+    const int P = p.population_size;
+    if (P <= 0) return fail(BRKGA_ERR_INVALID, "population_size must be > 0");
+    if (!(p.elite_prob >= 0.0 && p.elite_prob <= 1.0)) return fail(BRKGA_ERR_INVALID, "elite_prob outside [0,1]");
+    if (p.max_generations <= 0) return fail(BRKGA_ERR_INVALID, "max_generations must be > 0");
+    sh.k = p.num_islands > 0 ? p.num_islands : 1;
+    if (sh.mo) {
+        // NSGA-II: elite/mutant sizes are not used by the reference (core/config.hpp:170-178);
+        // mutant_size here is the optional count of fresh random offspring
+        if (sh.k != 1) return fail(BRKGA_ERR_UNSUPPORTED, "islands are single-objective only");
+        if (P < 2) return fail(BRKGA_ERR_INVALID, "NSGA-II needs population_size >= 2");
+        if (2 * P > kMaxPop) return fail(BRKGA_ERR_UNSUPPORTED, "NSGA-II pool above " + std::to_string(kMaxPop));
+        sh.Pi = P;
+        sh.Mn = std::max(0, std::min(P, p.mutant_size));
+    } else {
+        sh.Pi = P / sh.k;
+        sh.Ei = p.elite_size / sh.k;
+        sh.Mi = p.mutant_size / sh.k;
+        if (sh.Pi <= 0) return fail(BRKGA_ERR_INVALID, "fewer individuals than islands");
+        if (sh.Ei <= 0 || p.mutant_size < 0 || sh.Ei + sh.Mi > sh.Pi)
+            return fail(BRKGA_ERR_INVALID, "need elite_size > 0, mutant_size >= 0, elite + mutant <= population");
+        if (sh.Pi > kMaxPop) return fail(BRKGA_ERR_UNSUPPORTED, "population above " + std::to_string(kMaxPop));
+        if (sh.k > 1 && p.migration_interval > 0 && 2 * p.num_migrants > sh.Pi)
+            return fail(BRKGA_ERR_INVALID, "num_migrants must be <= half an island");
+    }
+    *s = sh;
+    return BRKGA_OK;
+}
+
+static int32_t dalloc(Population& p, void** ptr, size_t bytes) {
+    cudaError_t e = cudaMalloc(ptr, bytes ? bytes : 16);
+    if (e != cudaSuccess) return fail(BRKGA_ERR_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    p.allocs.push_back(*ptr);
+    p.bytes += bytes;
+    return BRKGA_OK;
+}
+
+int32_t Population::allocate(int device) {
+    DeviceGuard g(device);
+    rows = sh.mo ? 2 * sh.Pi : sh.k * sh.Pi;
+    hist_cap = std::max(prm.max_generations, 1) + 1;
+    void* p = nullptr;
+    int32_t st;
+    for (int b = 0; b < 2; ++b) {
+        if ((st = dalloc(*this, &p, (size_t)rows * sh.ld * 4)) != BRKGA_OK) return st;
+        keys[b] = (float*)p;
+        cudaMemset(p, 0, (size_t)rows * sh.ld * 4);
+        if ((st = dalloc(*this, &p, (size_t)rows * sh.m * 4)) != BRKGA_OK) return st;
+        fit[b] = (float*)p;
+    }
+    if ((st = dalloc(*this, &p, (size_t)rows * 4)) != BRKGA_OK) return st;
+    sorted = (int32_t*)p;
+    if ((st = dalloc(*this, &p, (size_t)sh.k * hist_cap * 4)) != BRKGA_OK) return st;
+    history = (float*)p;
+    if (sh.mo) {
+        if ((st = dalloc(*this, &p, (size_t)rows * 4)) != BRKGA_OK) return st;
+        rank = (int32_t*)p;
+        if ((st = dalloc(*this, &p, (size_t)rows * 4)) != BRKGA_OK) return st;
+        cd = (float*)p;
+        if ((st = dalloc(*this, &p, (size_t)sh.Pi * 4)) != BRKGA_OK) return st;
+        sel = (int32_t*)p;
+    }
+    return BRKGA_OK;
+}
+
+void Population::release(int device) {
+    DeviceGuard g(device);
+    for (void* a : allocs) cudaFree(a);
+    allocs.clear();
+}
+
+}  // namespace bk
+
+using namespace bk;
+
+struct brkga_engine {
+    std::mutex mu;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    Population pop;
+    std::vector<PopDesc> hd;
+    PopDesc* dd = nullptr;
+    Task* d_tasks_gen = nullptr;
+    Task* d_tasks_all = nullptr;
+    int nt_gen = 0, nt_all = 0;
+    RowTile tile{};
+    int grid = 0;
+    bool stage = false;
+    uint32_t gen = 0;
+    bool initialized = false;
+    int chunk = 16;
+    cudaGraphExec_t gx_chunk = nullptr, gx_one = nullptr, gx_mig = nullptr;
+    int32_t* d_perm = nullptr;
+    float* d_tmpfit = nullptr;
+    NsgaState nsga;
+};
+
+static RowLaunch base_launch(brkga_engine* e, int mode) {
+    RowLaunch L;
+    std::memset(&L, 0, sizeof(L));
+    L.descs = e->dd;
+    L.mode = mode;
+    L.max_n = e->pop.sh.n;
+    L.max_points = points_of(*e->pop.pd);
+    L.stage_xy = e->stage ? 1 : 0;
+    return L;
+}
+
+static bool migration_due(const brkga_engine* e, uint32_t g) {
+    const auto& p = e->pop.prm;
+    return e->pop.sh.k > 1 && p.migration_interval > 0 && p.num_migrants > 0 && g % (uint32_t)p.migration_interval == 0;
+}
+
+// one single-objective generation: fused rows + elite partition (+ migration, re-sort)
+static cudaError_t enqueue_brkga_gen(brkga_engine* e, bool mig) {
+    const Shape& sh = e->pop.sh;
+    RowLaunch L = base_launch(e, MODE_GEN);
+    L.tasks = (sh.k > 1) ? e->d_tasks_gen : nullptr;
+    L.ntasks = e->nt_gen;
+    cudaError_t err = launch_rows(L, e->pop.pd->kind, e->tile, e->grid, e->stream);
+    if (err != cudaSuccess) return err;
+    err = launch_sort_pops(e->dd, sh.k, sh.Pi, 1, e->stream);
+    if (err != cudaSuccess) return err;
+    if (mig) {
+        err = launch_migrate(e->dd, 1, sh.k, e->pop.prm.num_migrants, sh.n, e->stream);
+        if (err != cudaSuccess) return err;
+        err = launch_sort_pops(e->dd, sh.k, sh.Pi, 0, e->stream);
+    }
+    return err;
+}
+
+static cudaError_t enqueue_gen(brkga_engine* e, bool mig) {
+    if (e->pop.sh.mo) return nsga_enqueue_generation(e->nsga, e->stream);
+    return enqueue_brkga_gen(e, mig);
+}
+
+static cudaError_t capture(brkga_engine* e, int gens, bool mig, cudaGraphExec_t* out) {
+    cudaGraph_t g = nullptr;
+    cudaError_t err = cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal);
+    if (err != cudaSuccess) return err;
+    for (int i = 0; i < gens && err == cudaSuccess; ++i) err = enqueue_gen(e, mig && i == gens - 1);
+    cudaError_t end = cudaStreamEndCapture(e->stream, &g);
+    if (err != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return err;
+    }
+    if (end != cudaSuccess) return end;
+    err = cudaGraphInstantiate(out, g, 0);
+    cudaGraphDestroy(g);
+    return err;
+}
+
+static int32_t sync_descs_to_host(brkga_engine* e) {
+    cudaError_t err = cudaStreamSynchronize(e->stream);
+    if (err != cudaSuccess) return cuda_fail(err, "engine stream");
+    err = cudaMemcpy(e->hd.data(), e->dd, sizeof(PopDesc) * e->hd.size(), cudaMemcpyDeviceToHost);
+    if (err != cudaSuccess) return cuda_fail(err, "descriptor read-back");
+    return BRKGA_OK;
+}
+
+static int32_t grow_history(brkga_engine* e, int need) {
+    Population& p = e->pop;
+    if (need <= p.hist_cap) return BRKGA_OK;
+    int32_t st = sync_descs_to_host(e);
+    if (st != BRKGA_OK) return st;
+    int cap = p.hist_cap;
+    while (cap < need) cap *= 2;
+    void* nh = nullptr;
+    if ((st = dalloc(p, &nh, (size_t)p.sh.k * cap * 4)) != BRKGA_OK) return st;
+    for (int i = 0; i < p.sh.k; ++i) {
+        cudaError_t err = cudaMemcpy((float*)nh + (size_t)i * cap, p.history + (size_t)i * p.hist_cap,
+                                     (size_t)p.hist_cap * 4, cudaMemcpyDeviceToDevice);
+        if (err != cudaSuccess) return cuda_fail(err, "history copy");
+        e->hd[i].history = (float*)nh + (size_t)i * cap;
+        e->hd[i].hist_cap = cap;
+    }
+    p.history = (float*)nh;
+    p.hist_cap = cap;
+    if (p.sh.mo) nsga_set_history(e->nsga, p.history, cap);
+    cudaError_t err = cudaMemcpy(e->dd, e->hd.data(), sizeof(PopDesc) * e->hd.size(), cudaMemcpyHostToDevice);
+    if (err != cudaSuccess) return cuda_fail(err, "descriptor upload");
+    return BRKGA_OK;
+}
+
+static void destroy_engine(brkga_engine* e) {
+    DeviceGuard g(e->device);
+    if (e->stream) cudaStreamSynchronize(e->stream);
+    if (e->gx_chunk) cudaGraphExecDestroy(e->gx_chunk);
+    if (e->gx_one) cudaGraphExecDestroy(e->gx_one);
+    if (e->gx_mig) cudaGraphExecDestroy(e->gx_mig);
+    nsga_release(e->nsga);
+    e->pop.release(e->device);
+    if (e->stream) cudaStreamDestroy(e->stream);
+    delete e;
+}
+
+extern "C" {
+
+int32_t brkga_create(brkga_problem* pbh, const brkga_params* params, brkga_engine** out) {
+    if (!pbh || !params || !out) return fail(BRKGA_ERR_INVALID, "null argument");
+    *out = nullptr;
+    auto pd = problem_data(pbh);
+    if (params->device != pd->device)
+        return fail(BRKGA_ERR_INVALID, "params.device differs from the problem's device");
+    Shape sh;
+    int32_t st = make_shape(*pd, *params, &sh);
+    if (st != BRKGA_OK) return st;
+    DeviceGuard g(pd->device);
+    if (!g.ok()) return fail(BRKGA_ERR_CUDA, "cannot select device");
+    auto* e = new brkga_engine;
+    e->device = pd->device;
+    e->pop.pd = pd;
+    e->pop.prm = *params;
+    e->pop.sh = sh;
+    cudaError_t err = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
+    if (err != cudaSuccess) {
+        delete e;
+        return cuda_fail(err, "stream");
+    }
+    if ((st = e->pop.allocate(e->device)) != BRKGA_OK) {
+        destroy_engine(e);
+        return st;
+    }
+    void* p = nullptr;
+    if ((st = dalloc(e->pop, &p, sizeof(PopDesc) * sh.k)) != BRKGA_OK) {
+        destroy_engine(e);
+        return st;
+    }
+    e->dd = (PopDesc*)p;
+    if ((st = dalloc(e->pop, &p, (size_t)sh.n * 4)) != BRKGA_OK || (st = dalloc(e->pop, &p, 8)) != BRKGA_OK) {
+        destroy_engine(e);
+        return st;
+    }
+    e->d_perm = (int32_t*)e->pop.allocs[e->pop.allocs.size() - 2];
+    e->d_tmpfit = (float*)p;
+    // island descriptors
+    e->hd.resize(sh.k);
+    for (int i = 0; i < sh.k; ++i) {
+        PopDesc& d = e->hd[i];
+        fill_instance(d, *pd);
+        d.P = sh.Pi;
+        d.E = sh.Ei;
+        d.M = sh.Mi;
+        d.rhoT = prob_threshold(params->elite_prob);
+        d.seed = params->seed;
+        d.island = (uint32_t)i;
+        d.row0 = i * sh.Pi;
+        for (int b = 0; b < 2; ++b) {
+            d.keys[b] = e->pop.keys[b] + (size_t)i * sh.Pi * sh.ld;
+            d.fit[b] = e->pop.fit[b] + (size_t)i * sh.Pi * sh.m;
+        }
+        d.sorted = e->pop.sorted + (size_t)i * sh.Pi;
+        d.history = e->pop.history + (size_t)i * e->pop.hist_cap;
+        d.hist_cap = e->pop.hist_cap;
+        d.cur = 0;
+        d.gen = 0;
+    }
+    err = cudaMemcpy(e->dd, e->hd.data(), sizeof(PopDesc) * sh.k, cudaMemcpyHostToDevice);
+    if (err != cudaSuccess) {
+        destroy_engine(e);
+        return cuda_fail(err, "descriptor upload");
+    }
+    // work lists: costly rows (children, mutants) of every island first, elite copies last
+    if (sh.k > 1) {
+        std::vector<Task> tg, ta;
+        for (int i = 0; i < sh.k; ++i)
+            for (int r = sh.Ei; r < sh.Pi; ++r) tg.push_back({i, r});
+        for (int i = 0; i < sh.k; ++i)
+            for (int r = 0; r < sh.Ei; ++r) tg.push_back({i, r});
+        for (int i = 0; i < sh.k; ++i)
+            for (int r = 0; r < sh.Pi; ++r) ta.push_back({i, r});
+        if ((st = dalloc(e->pop, &p, tg.size() * sizeof(Task))) != BRKGA_OK) {
+            destroy_engine(e);
+            return st;
+        }
+        e->d_tasks_gen = (Task*)p;
+        cudaMemcpy(p, tg.data(), tg.size() * sizeof(Task), cudaMemcpyHostToDevice);
+        if ((st = dalloc(e->pop, &p, ta.size() * sizeof(Task))) != BRKGA_OK) {
+            destroy_engine(e);
+            return st;
+        }
+        e->d_tasks_all = (Task*)p;
+        cudaMemcpy(p, ta.data(), ta.size() * sizeof(Task), cudaMemcpyHostToDevice);
+        e->nt_gen = (int)tg.size();
+        e->nt_all = (int)ta.size();
+    } else {
+        e->nt_gen = sh.Pi;
+        e->nt_all = sh.Pi;
+    }
+    // tile, staging and grid from occupancy
+    e->tile = pick_tile(sh.n);
+    const int pts = points_of(*pd);
+    e->stage = stage_fits(e->tile, sh.n, pts, pd->kind);
+    const size_t smem = row_smem_bytes(e->tile, sh.n, pts, pd->kind, e->stage);
+    int per_sm = 0;
+    err = prepare_rows(e->tile, smem, &per_sm);
+    if (err != cudaSuccess || per_sm <= 0) {
+        destroy_engine(e);
+        return err != cudaSuccess ? cuda_fail(err, "row kernel set-up")
+                                  : fail(BRKGA_ERR_UNSUPPORTED, "row kernel does not fit on an SM");
+    }
+    e->grid = per_sm * device_sm_count();
+    err = prepare_sort(sh.mo ? 2 * sh.Pi : sh.Pi);
+    if (err != cudaSuccess) {
+        destroy_engine(e);
+        return cuda_fail(err, "sort set-up");
+    }
+    if (sh.mo) {
+        st = nsga_setup(e->nsga, e->pop, e->dd, e->tile, e->grid, e->stage);
+        if (st != BRKGA_OK) {
+            destroy_engine(e);
+            return st;
+        }
+    }
+    *out = e;
+    return BRKGA_OK;
+}
+
+int32_t brkga_destroy(brkga_engine* e) {
+    if (!e) return BRKGA_OK;
+    destroy_engine(e);
+    return BRKGA_OK;
+}
+
+int32_t brkga_initialize(brkga_engine* e) {
+    if (!e) return fail(BRKGA_ERR_INVALID, "null engine");
+    std::lock_guard<std::mutex> lk(e->mu);
+    DeviceGuard g(e->device);
+    const Shape& sh = e->pop.sh;
+    // reset generation counters / buffer index on the device
+    for (auto& d : e->hd) {
+        d.cur = 0;
+        d.gen = 0;
+    }
+    cudaError_t err = cudaMemcpyAsync(e->dd, e->hd.data(), sizeof(PopDesc) * e->hd.size(),
+                                      cudaMemcpyHostToDevice, e->stream);
+    if (err != cudaSuccess) return cuda_fail(err, "descriptor upload");
+    if (sh.mo) {
+        err = nsga_enqueue_init(e->nsga, e->stream);
+    } else {
+        RowLaunch L = base_launch(e, MODE_INIT);
+        L.tasks = (sh.k > 1) ? e->d_tasks_all : nullptr;
+        L.ntasks = e->nt_all;
+        err = launch_rows(L, e->pop.pd->kind, e->tile, e->grid, e->stream);
+        if (err == cudaSuccess) err = launch_sort_pops(e->dd, sh.k, sh.Pi, 0, e->stream);
+    }
+    if (err != cudaSuccess) return cuda_fail(err, "initialize");
+    e->gen = 0;
+    e->initialized = true;
+    return BRKGA_OK;
+}
+
+int32_t brkga_evolve(brkga_engine* e, int32_t generations) {
+    if (!e) return fail(BRKGA_ERR_INVALID, "null engine");
+    if (generations < 0) return fail(BRKGA_ERR_INVALID, "negative generation count");
+    if (!e->initialized) {
+        int32_t st = brkga_initialize(e);
+        if (st != BRKGA_OK) return st;
+    }
+    std::lock_guard<std::mutex> lk(e->mu);
+    DeviceGuard g(e->device);
+    int32_t st = grow_history(e, (int)e->gen + generations + 1);
+    if (st != BRKGA_OK) return st;
+    cudaError_t err = cudaSuccess;
+    int left = generations;
+    while (left > 0 && err == cudaSuccess) {
+        // generations until (and excluding) the next migration generation
+        int plain = left;
+        if (e->pop.sh.k > 1 && e->pop.prm.migration_interval > 0 && e->pop.prm.num_migrants > 0) {
+            const uint32_t iv = (uint32_t)e->pop.prm.migration_interval;
+            const uint32_t next = (e->gen / iv + 1) * iv;
+            plain = std::min<int>(left, (int)(next - e->gen - 1));
+        }
+        while (plain >= e->chunk && err == cudaSuccess) {
+            if (!e->gx_chunk) err = capture(e, e->chunk, false, &e->gx_chunk);
+            if (err == cudaSuccess) err = cudaGraphLaunch(e->gx_chunk, e->stream);
+            plain -= e->chunk;
+            left -= e->chunk;
+            e->gen += e->chunk;
+        }
+        while (plain > 0 && err == cudaSuccess) {
+            if (!e->gx_one) err = capture(e, 1, false, &e->gx_one);
+            if (err == cudaSuccess) err = cudaGraphLaunch(e->gx_one, e->stream);
+            --plain;
+            --left;
+            ++e->gen;
+        }
+        if (left > 0 && err == cudaSuccess) {
+            const bool mig = migration_due(e, e->gen + 1);
+            cudaGraphExec_t* gx = mig ? &e->gx_mig : &e->gx_one;
+            if (!*gx) err = capture(e, 1, mig, gx);
+            if (err == cudaSuccess) err = cudaGraphLaunch(*gx, e->stream);
+            --left;
+            ++e->gen;
+        }
+    }
+    if (err != cudaSuccess) return cuda_fail(err, "evolve");
+    return BRKGA_OK;
+}
+
+int32_t brkga_synchronize(brkga_engine* e) {
+    if (!e) return fail(BRKGA_ERR_INVALID, "null engine");
+    DeviceGuard g(e->device);
+    cudaError_t err = cudaStreamSynchronize(e->stream);
+    if (err != cudaSuccess) return cuda_fail(err, "engine stream");
+    return BRKGA_OK;
+}
+
+int32_t brkga_run(brkga_engine* e) {
+    if (!e) return fail(BRKGA_ERR_INVALID, "null engine");
+    int32_t st = brkga_initialize(e);
+    if (st != BRKGA_OK) return st;
+    st = brkga_evolve(e, e->pop.prm.max_generations);
+    if (st != BRKGA_OK) return st;
+    return brkga_synchronize(e);
+}
+
+int32_t brkga_generation(const brkga_engine* e) { return e ? (int32_t)e->gen : BRKGA_ERR_INVALID; }
+
+int32_t brkga_get_population(brkga_engine* e, float* keys, float* fitness) {
+    if (!e) return fail(BRKGA_ERR_INVALID, "null engine");
+    std::lock_guard<std::mutex> lk(e->mu);
+    DeviceGuard g(e->device);
+    if (e->pop.sh.mo) return nsga_get_population(e->nsga, e->stream, keys, fitness);
+    int32_t st = sync_descs_to_host(e);
+    if (st != BRKGA_OK) return st;
+    const Shape& sh = e->pop.sh;
+    const int cur = e->hd[0].cur;
+    const int rows = sh.k * sh.Pi;
+    std::vector<float> hk((size_t)rows * sh.ld), hf((size_t)rows * sh.m);
+    std::vector<int32_t> hs(rows);
+    cudaMemcpy(hk.data(), e->pop.keys[cur], hk.size() * 4, cudaMemcpyDeviceToHost);
+    cudaMemcpy(hf.data(), e->pop.fit[cur], hf.size() * 4, cudaMemcpyDeviceToHost);
+    cudaError_t err = cudaMemcpy(hs.data(), e->pop.sorted, hs.size() * 4, cudaMemcpyDeviceToHost);
+    if (err != cudaSuccess) return cuda_fail(err, "population read-back");
+    for (int i = 0; i < sh.k; ++i)
+        for (int r = 0; r < sh.Pi; ++r) {
+            const int src = i * sh.Pi + hs[(size_t)i * sh.Pi + r];
+            const int dst = i * sh.Pi + r;
+            if (keys) std::memcpy(keys + (size_t)dst * sh.n, hk.data() + (size_t)src * sh.ld, (size_t)sh.n * 4);
+            if (fitness) std::memcpy(fitness + (size_t)dst * sh.m, hf.data() + (size_t)src * sh.m, (size_t)sh.m * 4);
+        }
+    return BRKGA_OK;
+}
+
+int32_t brkga_set_population(brkga_engine* e, const float* keys) {
+    if (!e || !keys) return fail(BRKGA_ERR_INVALID, "null argument");
+    std::lock_guard<std::mutex> lk(e->mu);
+    DeviceGuard g(e->device);
+    if (e->pop.sh.mo) {
+        int32_t st = nsga_set_population(e->nsga, e->stream, keys);
+        if (st == BRKGA_OK) e->initialized = true;
+        return st;
+    }
+    int32_t st = sync_descs_to_host(e);
+    if (st != BRKGA_OK) return st;
+    const Shape& sh = e->pop.sh;
+    const int cur = e->hd[0].cur;
+    const int rows = sh.k * sh.Pi;
+    std::vector<float> hk((size_t)rows * sh.ld, 0.0f);
+    for (int r = 0; r < rows; ++r) std::memcpy(hk.data() + (size_t)r * sh.ld, keys + (size_t)r * sh.n, (size_t)sh.n * 4);
+    cudaError_t err = cudaMemcpy(e->pop.keys[cur], hk.data(), hk.size() * 4, cudaMemcpyHostToDevice);
+    if (err != cudaSuccess) return cuda_fail(err, "population upload");
+    RowLaunch L = base_launch(e, MODE_EVAL);
+    L.tasks = (sh.k > 1) ? e->d_tasks_all : nullptr;
+    L.ntasks = e->nt_all;
+    err = launch_rows(L, e->pop.pd->kind, e->tile, e->grid, e->stream);
+    if (err == cudaSuccess) err = launch_sort_pops(e->dd, sh.k, sh.Pi, 0, e->stream);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(e->stream);
+    if (err != cudaSuccess) return cuda_fail(err, "population evaluate");
+    if (!e->initialized) {
+        e->initialized = true;
+        e->gen = e->hd[0].gen;
+    }
+    return BRKGA_OK;
+}
+
+int32_t brkga_get_best(brkga_engine* e, float* keys, int32_t* perm, float* fitness) {
+    if (!e) return fail(BRKGA_ERR_INVALID, "null engine");
+    std::lock_guard<std::mutex> lk(e->mu);
+    DeviceGuard g(e->device);
+    if (e->pop.sh.mo) return nsga_get_best(e->nsga, e->stream, keys, perm, fitness);
+    int32_t st = sync_descs_to_host(e);
+    if (st != BRKGA_OK) return st;
+    const Shape& sh = e->pop.sh;
+    const ProblemData& pd = *e->pop.pd;
+    // best island: compare each island's rank-0 fitness in the problem's order
+    int best_i = 0, best_row = 0;
+    float best_f = 0.0f;
+    for (int i = 0; i < sh.k; ++i) {
+        const PopDesc& d = e->hd[i];
+        int32_t r0 = 0;
+        float f0 = 0.0f;
+        cudaMemcpy(&r0, d.sorted, 4, cudaMemcpyDeviceToHost);
+        cudaError_t err = cudaMemcpy(&f0, d.fit[d.cur] + (size_t)r0 * sh.m, 4, cudaMemcpyDeviceToHost);
+        if (err != cudaSuccess) return cuda_fail(err, "best read-back");
+        const bool better = (i == 0) || (pd.maximize ? (f0 > best_f) : (f0 < best_f));
+        if (better) {
+            best_i = i;
+            best_row = r0;
+            best_f = f0;
+        }
+    }
+    const PopDesc& d = e->hd[best_i];
+    const float* row = d.keys[d.cur] + (size_t)best_row * sh.ld;
+    if (fitness) *fitness = best_f;
+    if (keys) {
+        cudaError_t err = cudaMemcpy(keys, row, (size_t)sh.n * 4, cudaMemcpyDeviceToHost);
+        if (err != cudaSuccess) return cuda_fail(err, "best keys read-back");
+    }
+    if (perm) {
+        // decode on the device (same argsort as the generation kernel)
+        RowLaunch L;
+        std::memset(&L, 0, sizeof(L));
+        fill_instance(L.single, pd);
+        L.single.keys[0] = const_cast<float*>(row);
+        L.single.fit[0] = e->d_tmpfit;
+        L.single.P = 1;
+        L.ntasks = 1;
+        L.mode = MODE_EVAL;
+        L.perm_out = e->d_perm;
+        L.max_n = sh.n;
+        L.max_points = points_of(pd);
+        L.stage_xy = e->stage ? 1 : 0;
+        cudaError_t err = launch_rows(L, pd.kind, e->tile, 1, e->stream);
+        if (err == cudaSuccess) err = cudaStreamSynchronize(e->stream);
+        if (err == cudaSuccess) err = cudaMemcpy(perm, e->d_perm, (size_t)sh.n * 4, cudaMemcpyDeviceToHost);
+        if (err != cudaSuccess) return cuda_fail(err, "best decode");
+    }
+    return BRKGA_OK;
+}
+
+int32_t brkga_get_fitness_history(brkga_engine* e, float* history, int32_t cap, int32_t* len) {
+    if (!e || !history || !len) return fail(BRKGA_ERR_INVALID, "null argument");
+    std::lock_guard<std::mutex> lk(e->mu);
+    DeviceGuard g(e->device);
+    cudaError_t err = cudaStreamSynchronize(e->stream);
+    if (err != cudaSuccess) return cuda_fail(err, "engine stream");
+    const Shape& sh = e->pop.sh;
+    const int have = std::min<int>((int)e->gen + 1, e->pop.hist_cap);
+    const int cnt = std::min(have, (int)cap);
+    std::vector<float> h((size_t)sh.k * e->pop.hist_cap);
+    err = cudaMemcpy(h.data(), e->pop.history, h.size() * 4, cudaMemcpyDeviceToHost);
+    if (err != cudaSuccess) return cuda_fail(err, "history read-back");
+    const bool mx = e->pop.pd->maximize != 0;
+    for (int g2 = 0; g2 < cnt; ++g2) {
+        float b = h[g2];
+        for (int i = 1; i < sh.k; ++i) {
+            const float v = h[(size_t)i * e->pop.hist_cap + g2];
+            if (mx ? (v > b) : (v < b)) b = v;
+        }
+        history[g2] = b;
+    }
+    *len = cnt;
+    return BRKGA_OK;
+}
+
+int32_t brkga_get_pareto_front(brkga_engine* e, float* objectives, float* keys, int32_t cap, int32_t* count) {
+    if (!e || !count) return fail(BRKGA_ERR_INVALID, "null argument");
+    std::lock_guard<std::mutex> lk(e->mu);
+    DeviceGuard g(e->device);
+    if (!e->pop.sh.mo) return fail(BRKGA_ERR_INVALID, "not a multi-objective problem");
+    return nsga_get_front(e->nsga, e->stream, objectives, keys, cap, count);
+}
+
+}  // extern "C"

@@ -1,0 +1,92 @@
+// engine.h -- host-side pieces shared by the C-ABI translation units.
+#pragma once
+
+#include <cstdint>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/brkga_b200.h"
+#include "kernels.h"
+
+namespace bk {
+
+constexpr size_t kMaxSmem = 227 * 1024;  // opt-in dynamic shared memory per CTA on sm_100
+constexpr int kMaxPop = 16384;           // largest population the in-shared-memory sort handles
+
+int32_t fail(int32_t code, const std::string& msg);
+int32_t cuda_fail(cudaError_t e, const char* what);
+
+class DeviceGuard {
+public:
+    explicit DeviceGuard(int dev);
+    ~DeviceGuard();
+    bool ok() const { return ok_; }
+
+private:
+    int prev_ = 0;
+    bool ok_ = false;
+};
+
+// device-resident instance data (the reference's per-device matrix map,
+// configs/tsp_config.hpp:32, 125-165), shared by every engine built on it
+struct ProblemData {
+    int device = 0;
+    int kind = 0, n = 0, m = 1, maximize = 0;
+    float cap = 0.0f;
+    long long capi = 0;
+    float* xy = nullptr;
+    float* xy2 = nullptr;
+    float* mat = nullptr;
+    float* mat2 = nullptr;
+    int32_t* w = nullptr;
+    int32_t* v = nullptr;
+    size_t bytes = 0;
+    std::vector<void*> allocs;
+    ~ProblemData();
+};
+
+int32_t make_problem(const brkga_problem_desc* d, int device, std::shared_ptr<ProblemData>* out);
+std::shared_ptr<ProblemData> problem_data(brkga_problem* pb);
+void fill_instance(PopDesc& d, const ProblemData& pd);
+int points_of(const ProblemData& pd);
+bool stage_fits(const RowTile& t, int n, int pts, int kind);
+uint32_t prob_threshold(double p);
+
+// validated, per-island GA shape
+struct Shape {
+    int k = 1;        // islands
+    int Pi = 0, Ei = 0, Mi = 0;
+    int n = 0, ld = 0, m = 1;
+    bool mo = false;  // NSGA-II
+    int Mn = 0;       // NSGA-II fresh random offspring
+};
+int32_t make_shape(const ProblemData& pd, const brkga_params& p, Shape* s);
+
+// one population family (all islands of one instance) on the device
+struct Population {
+    std::shared_ptr<ProblemData> pd;
+    brkga_params prm{};
+    Shape sh;
+    uint64_t seed = 0;
+    int rows = 0;           // rows per key buffer (k * Pi, or 2P pool for NSGA-II)
+    float* keys[2] = {nullptr, nullptr};
+    float* fit[2] = {nullptr, nullptr};
+    int32_t* sorted = nullptr;
+    float* history = nullptr;
+    int hist_cap = 0;
+    // NSGA-II state
+    int32_t* rank = nullptr;   // [2P] pool ranks, then survivors' ranks in [0,P)
+    float* cd = nullptr;       // [2P]
+    int32_t* sel = nullptr;    // [P]
+    float* nsga_hist = nullptr;
+    std::vector<void*> allocs;
+    size_t bytes = 0;
+    int32_t allocate(int device);
+    void release(int device);
+};
+
+}  // namespace bk

@@ -1,0 +1,784 @@
+// kernels.cu -- the per-generation hot path on sm_100a.
+//
+// One CTA owns one chromosome row at a time (persistent grid, rows strided over CTAs):
+//   1. build the row in registers: elite copy, biased crossover of two parent rows
+//      (128-bit loads, Philox coins), mutant fill, or a load of given keys;
+//   2. write it to the next population buffer (128-bit stores);
+//   3. decode it: stable argsort of the keys in shared memory -- a bucket scatter
+//      (bucket = floor(key * B), monotone in key) followed by an exact rank inside each
+//      bucket by (key, index), so ties go to the lower index exactly like the
+//      reference's std::sort over (key, index) pairs (configs/tsp_config.hpp:206-225);
+//   4. fitness from the permutation: closed tour length from coordinates staged in
+//      shared memory (or a distance matrix), the depot tour of the bi-objective TSP,
+//      or the knapsack decoders; FP32 tour sums use one fixed order (256 virtual lanes,
+//      xor butterflies, fixed 8-way tree) that the oracle restates bit for bit.
+// The elite partition is a bitonic sort of (fitness key, row) composites in shared
+// memory, one CTA per population.
+#include <climits>
+#include <cstdio>
+#include <map>
+#include <mutex>
+#include <utility>
+
+#include "kernels.h"
+
+namespace bk {
+
+// ---------------------------------------------------------------------------------------
+// shared-memory carve-up for the row kernel
+// ---------------------------------------------------------------------------------------
+struct RowSmem {
+    uint32_t* cnt;            // bucket counters / offsets, NB + 1
+    unsigned long long* sc;   // scattered (okey << 32 | index) composites, n
+    int32_t* perm;            // decoded permutation, n
+    float* xy;                // staged coordinates (1 or 2 sets)
+};
+
+__host__ __device__ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+__host__ __device__ inline size_t cnt_words(int block, int max_n) {
+    const int kb = (max_n + block - 1) / block;
+    return (size_t)block * (kb > 0 ? kb : 1) + 1;
+}
+
+size_t row_smem_bytes(const RowTile& t, int max_n, int max_points, int kind, bool stage_xy) {
+    size_t b = align_up(cnt_words(t.block, max_n) * 4, 16);
+    b += align_up((size_t)max_n * 8, 16);
+    b += align_up((size_t)max_n * 4, 16);
+    if (stage_xy && (kind == TSP_COORDS || kind == BITSP_COORDS))
+        b += (size_t)max_points * 8 * (kind == BITSP_COORDS ? 2 : 1);
+    return b;
+}
+
+__device__ __forceinline__ RowSmem carve(unsigned char* base, int block, int max_n, int max_points) {
+    RowSmem s;
+    size_t off = 0;
+    s.cnt = reinterpret_cast<uint32_t*>(base + off);
+    off += align_up(cnt_words(block, max_n) * 4, 16);
+    s.sc = reinterpret_cast<unsigned long long*>(base + off);
+    off += align_up((size_t)max_n * 8, 16);
+    s.perm = reinterpret_cast<int32_t*>(base + off);
+    off += align_up((size_t)max_n * 4, 16);
+    s.xy = reinterpret_cast<float*>(base + off);
+    (void)max_points;
+    return s;
+}
+
+// ---------------------------------------------------------------------------------------
+// decode: stable argsort of one row held in registers (k[g][l] is key index
+// 4 * (threadIdx.x + g * BLOCK) + l)
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ int bucket_of(float key, float nbf, int nb) {
+    // monotone in okey order: negatives -> 0; [0,1) -> floor(key * nb); >= 1, +inf, NaN -> nb-1
+    if (!(key >= 0.0f)) return (key != key) ? nb - 1 : 0;
+    const float t = __fmul_rn(key, nbf);
+    const int b = (t < nbf) ? (int)t : nb - 1;
+    return b < nb - 1 ? b : nb - 1;
+}
+
+template <int BLOCK, int G>
+__device__ void row_argsort(const float (&k)[G][4], int n, const RowSmem& s, uint32_t* warp_tot) {
+    const int t = threadIdx.x;
+    const int KB = (n + BLOCK - 1) / BLOCK;
+    const int NB = BLOCK * KB;
+    const float nbf = (float)NB;
+    for (int b = t; b <= NB; b += BLOCK) s.cnt[b] = 0u;
+    __syncthreads();
+    uint32_t bs[G][4];  // (bucket << 16) | slot
+#pragma unroll
+    for (int g = 0; g < G; ++g)
+#pragma unroll
+        for (int l = 0; l < 4; ++l) {
+            const int i = 4 * (t + g * BLOCK) + l;
+            if (i < n) {
+                const int b = bucket_of(k[g][l], nbf, NB);
+                const uint32_t slot = atomicAdd(&s.cnt[b], 1u);
+                bs[g][l] = ((uint32_t)b << 16) | slot;
+            }
+        }
+    __syncthreads();
+    // exclusive scan over contiguous bucket ranges [t*KB, t*KB + KB)
+    uint32_t c[4 * G];
+    uint32_t sum = 0;
+#pragma unroll
+    for (int i = 0; i < 4 * G; ++i) {
+        c[i] = (i < KB) ? s.cnt[t * KB + i] : 0u;
+        sum += c[i];
+    }
+    uint32_t total;
+    uint32_t run = block_exclusive_scan<BLOCK>(sum, warp_tot, &total);
+#pragma unroll
+    for (int i = 0; i < 4 * G; ++i)
+        if (i < KB) {
+            s.cnt[t * KB + i] = run;
+            run += c[i];
+        }
+    if (t == 0) s.cnt[NB] = (uint32_t)n;
+    __syncthreads();
+    // scatter composites
+#pragma unroll
+    for (int g = 0; g < G; ++g)
+#pragma unroll
+        for (int l = 0; l < 4; ++l) {
+            const int i = 4 * (t + g * BLOCK) + l;
+            if (i < n) {
+                const uint32_t b = bs[g][l] >> 16, slot = bs[g][l] & 0xFFFFu;
+                s.sc[s.cnt[b] + slot] = ((unsigned long long)okey(k[g][l]) << 32) | (uint32_t)i;
+            }
+        }
+    __syncthreads();
+    // exact rank inside the bucket
+#pragma unroll
+    for (int g = 0; g < G; ++g)
+#pragma unroll
+        for (int l = 0; l < 4; ++l) {
+            const int i = 4 * (t + g * BLOCK) + l;
+            if (i < n) {
+                const uint32_t b = bs[g][l] >> 16;
+                const uint32_t b0 = s.cnt[b], b1 = s.cnt[b + 1];
+                const unsigned long long me = ((unsigned long long)okey(k[g][l]) << 32) | (uint32_t)i;
+                uint32_t r = b0;
+                for (uint32_t q = b0; q < b1; ++q) r += (s.sc[q] < me) ? 1u : 0u;
+                s.perm[r] = i;
+            }
+        }
+    __syncthreads();
+}
+
+// ---------------------------------------------------------------------------------------
+// fitness
+// ---------------------------------------------------------------------------------------
+// Euclidean edge exactly as the reference builds its matrix (configs/tsp_config.hpp:366-368):
+// float dx, dy; sqrt(dx*dx + dy*dy), no contraction, correctly rounded sqrt
+__device__ __forceinline__ float edge_xy(const float* xy, int a, int b) {
+    const float2 pa = reinterpret_cast<const float2*>(xy)[a];
+    const float2 pb = reinterpret_cast<const float2*>(xy)[b];
+    const float dx = __fsub_rn(pa.x, pb.x);
+    const float dy = __fsub_rn(pa.y, pb.y);
+    return __fsqrt_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)));
+}
+
+// canonical FP32 sum of nedges edge terms: 256 virtual lanes, xor butterflies inside each
+// group of 32 lanes, fixed tree over the 8 group totals
+template <int BLOCK, int NOBJ, typename EdgeF>
+__device__ __forceinline__ void canon_sum(int nedges, EdgeF edge, float* red, float* out) {
+    constexpr int LPT = BLOCK >= 256 ? 1 : 256 / BLOCK;
+    const int t = threadIdx.x, lane = t & 31;
+    float acc[LPT][NOBJ];
+#pragma unroll
+    for (int j = 0; j < LPT; ++j) {
+#pragma unroll
+        for (int o = 0; o < NOBJ; ++o) acc[j][o] = 0.0f;
+        const int vl = t + j * BLOCK;
+        if (vl < 256) {
+            for (int e = vl; e < nedges; e += 256) {
+                float d[NOBJ];
+                edge(e, d);
+#pragma unroll
+                for (int o = 0; o < NOBJ; ++o) acc[j][o] = __fadd_rn(acc[j][o], d[o]);
+            }
+        }
+    }
+#pragma unroll
+    for (int m = 16; m >= 1; m >>= 1)
+#pragma unroll
+        for (int j = 0; j < LPT; ++j)
+#pragma unroll
+            for (int o = 0; o < NOBJ; ++o) acc[j][o] = __fadd_rn(acc[j][o], __shfl_xor_sync(0xffffffffu, acc[j][o], m));
+    if (lane == 0) {
+#pragma unroll
+        for (int j = 0; j < LPT; ++j) {
+            const int vl = t + j * BLOCK;
+            if (vl < 256) {
+#pragma unroll
+                for (int o = 0; o < NOBJ; ++o) red[o * 8 + (vl >> 5)] = acc[j][o];
+            }
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int o = 0; o < NOBJ; ++o) {
+        const float* g = red + o * 8;
+        out[o] = __fadd_rn(__fadd_rn(__fadd_rn(g[0], g[1]), __fadd_rn(g[2], g[3])),
+                           __fadd_rn(__fadd_rn(g[4], g[5]), __fadd_rn(g[6], g[7])));
+    }
+    __syncthreads();
+}
+
+template <int BLOCK>
+__device__ __forceinline__ long long block_excl_scan_ll(long long v, long long* red, long long* total) {
+    constexpr int NW = BLOCK / 32;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    long long x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const long long y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) red[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        long long s = (lane < NW) ? red[lane] : 0ll;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const long long y = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane >= o) s += y;
+        }
+        if (lane < NW) red[lane] = s;
+    }
+    __syncthreads();
+    const long long base = (w > 0) ? red[w - 1] : 0ll;
+    *total = red[NW - 1];
+    __syncthreads();
+    return base + x - v;
+}
+
+// knapsack greedy in key order: prefix of the sorted items that fits, then a
+// first-fit scan of the rest by warp 0 (weights must be >= 0)
+template <int BLOCK>
+__device__ float knap_greedy(const RowSmem& s, int n, const int32_t* __restrict__ w,
+                             const int32_t* __restrict__ v, long long C, long long* red,
+                             long long* shared_misc) {
+    const int t = threadIdx.x;
+    const int ch = (n + BLOCK - 1) / BLOCK;
+    const int p0 = t * ch, p1 = min(n, p0 + ch);
+    long long ws = 0;
+    for (int p = p0; p < p1; ++p) ws += __ldg(w + s.perm[p]);
+    long long tot;
+    const long long base = block_excl_scan_ll<BLOCK>(ws, red, &tot);
+    // positions whose inclusive prefix weight stays <= C
+    long long S = base, cnt = 0, val = 0, lastS = -1;
+    for (int p = p0; p < p1; ++p) {
+        const int it = s.perm[p];
+        S += __ldg(w + it);
+        if (S <= C) {
+            ++cnt;
+            val += __ldg(v + it);
+            lastS = S;
+        }
+    }
+    const long long f = block_sum_ll<BLOCK>(cnt, red);
+    const long long v0 = block_sum_ll<BLOCK>(val, red);
+    if (f > 0 && p0 < p1 && f - 1 >= p0 && f - 1 < p1) shared_misc[0] = lastS;
+    if (f == 0 && t == 0) shared_misc[0] = 0;
+    __syncthreads();
+    long long vt = 0;
+    if (t < 32) {
+        long long r = C - shared_misc[0];
+        for (int b = (int)f + 1; b < n; b += 32) {
+            const int pos = b + t;
+            const long long wl = (pos < n) ? (long long)__ldg(w + s.perm[pos]) : LLONG_MAX;
+            const long long vl = (pos < n) ? (long long)__ldg(v + s.perm[pos]) : 0ll;
+            int cur = 0;
+            for (;;) {
+                const unsigned mask = __ballot_sync(0xffffffffu, pos < n && t >= cur && wl <= r);
+                if (!mask) break;
+                const int j = __ffs(mask) - 1;
+                r -= __shfl_sync(0xffffffffu, wl, j);
+                vt += __shfl_sync(0xffffffffu, vl, j);
+                cur = j + 1;
+            }
+        }
+    }
+    __syncthreads();
+    return (float)(v0 + vt);
+}
+
+// ---------------------------------------------------------------------------------------
+// the fused row kernel
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ int tourn(int i1, int i2, const int32_t* rank, const float* cd) {
+    const int r1 = __ldg(rank + i1), r2 = __ldg(rank + i2);
+    if (r1 < r2) return i1;
+    if (r2 < r1) return i2;
+    if (__ldg(cd + i1) > __ldg(cd + i2)) return i1;
+    return i2;
+}
+
+template <int BLOCK, int G>
+__global__ void __launch_bounds__(BLOCK) row_kernel(RowLaunch L) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ PopDesc sd;
+    __shared__ uint32_t warp_tot[32];
+    __shared__ long long red_ll[32];
+    __shared__ float red_f[16];
+    __shared__ long long misc[4];
+
+    const int t = threadIdx.x;
+    const RowSmem s = carve(smem_raw, BLOCK, L.max_n, L.max_points);
+    int cur_pid = -1;
+
+    for (int task = blockIdx.x; task < L.ntasks; task += gridDim.x) {
+        int pid = 0, r = task;
+        if (L.tasks) {
+            const Task tk = L.tasks[task];
+            pid = tk.pid;
+            r = tk.row;
+        }
+        if (pid != cur_pid) {
+            __syncthreads();
+            if (t == 0) sd = L.descs ? L.descs[pid] : L.single;
+            __syncthreads();
+            if (L.stage_xy && (sd.kind == TSP_COORDS || sd.kind == BITSP_COORDS)) {
+                const int npts = (sd.kind == BITSP_COORDS) ? sd.n + 1 : sd.n;
+                const float2* g0 = reinterpret_cast<const float2*>(sd.xy);
+                float2* d0 = reinterpret_cast<float2*>(s.xy);
+                for (int i = t; i < npts; i += BLOCK) d0[i] = g0[i];
+                if (sd.kind == BITSP_COORDS) {
+                    const float2* g1 = reinterpret_cast<const float2*>(sd.xy2);
+                    for (int i = t; i < npts; i += BLOCK) d0[npts + i] = g1[i];
+                }
+            }
+            __syncthreads();
+            cur_pid = pid;
+        }
+        const int n = sd.n, ld = sd.ld, P = sd.P, E = sd.E, M = sd.M, m = sd.m;
+        const int cur = sd.cur;
+        if (!L.tasks && L.mode == MODE_GEN) r = (task < P - E) ? E + task : task - (P - E);
+
+        float k[G][4];
+        float* dst = nullptr;
+        float* dfit = nullptr;
+        bool eval = true, store = true;
+        const uint32_t isl = sd.island << 8;
+
+        if (L.mode == MODE_GEN) {
+            const float* src = sd.keys[cur];
+            dst = sd.keys[cur ^ 1];
+            dfit = sd.fit[cur ^ 1];
+            const uint32_t g = sd.gen + 1;
+            if (r < E) {
+                // elite copy (core/population.hpp:700-714), fitness kept
+                const int sr = __ldg(sd.sorted + r);
+                const float4* a = reinterpret_cast<const float4*>(src + (size_t)sr * ld);
+                float4* o = reinterpret_cast<float4*>(dst + (size_t)r * ld);
+                for (int q = t; q < ld / 4; q += BLOCK) o[q] = __ldg(a + q);
+                if (t < m) dfit[(size_t)r * m + t] = __ldg(sd.fit[cur] + (size_t)sr * m + t);
+                eval = false;
+                store = false;
+            } else if (r < P - M) {
+                // biased crossover (core/solver.hpp:1109-1135; core/cuda_kernels.cuh:120-134)
+                const uint4 pr = draw4(sd.seed, 0u, (uint32_t)r, g, isl | TAG_PARENT);
+                const int ea = __ldg(sd.sorted + pick(pr.x, (uint32_t)E));
+                const int nb = __ldg(sd.sorted + E + pick(pr.y, (uint32_t)(P - E)));
+                const float4* A = reinterpret_cast<const float4*>(src + (size_t)ea * ld);
+                const float4* B = reinterpret_cast<const float4*>(src + (size_t)nb * ld);
+#pragma unroll
+                for (int gg = 0; gg < G; ++gg) {
+                    const int q = t + gg * BLOCK;
+                    if (4 * q < n) {
+                        const float4 a = __ldg(A + q), b = __ldg(B + q);
+                        const uint4 c = draw4(sd.seed, (uint32_t)q, (uint32_t)r, g, isl | TAG_COIN);
+                        k[gg][0] = ((c.x >> 8) < sd.rhoT) ? a.x : b.x;
+                        k[gg][1] = ((c.y >> 8) < sd.rhoT) ? a.y : b.y;
+                        k[gg][2] = ((c.z >> 8) < sd.rhoT) ? a.z : b.z;
+                        k[gg][3] = ((c.w >> 8) < sd.rhoT) ? a.w : b.w;
+                    }
+                }
+            } else {
+                // mutant (core/solver.hpp:1244-1258)
+#pragma unroll
+                for (int gg = 0; gg < G; ++gg) {
+                    const int q = t + gg * BLOCK;
+                    if (4 * q < n) {
+                        const uint4 c = draw4(sd.seed, (uint32_t)q, (uint32_t)r, g, isl | TAG_MUTANT);
+                        k[gg][0] = u24(c.x);
+                        k[gg][1] = u24(c.y);
+                        k[gg][2] = u24(c.z);
+                        k[gg][3] = u24(c.w);
+                    }
+                }
+            }
+        } else if (L.mode == MODE_INIT) {
+            // Population::initialize keys (core/population.hpp:107-110)
+            dst = sd.keys[cur];
+            dfit = sd.fit[cur];
+#pragma unroll
+            for (int gg = 0; gg < G; ++gg) {
+                const int q = t + gg * BLOCK;
+                if (4 * q < n) {
+                    const uint4 c = draw4(sd.seed, (uint32_t)q, (uint32_t)r, 0u, isl | TAG_INIT);
+                    k[gg][0] = u24(c.x);
+                    k[gg][1] = u24(c.y);
+                    k[gg][2] = u24(c.z);
+                    k[gg][3] = u24(c.w);
+                }
+            }
+        } else if (L.mode == MODE_NSGA_OFF) {
+            // NSGA-II offspring (core/solver.hpp:1019-1091): pool rows [P, 2P) of keys[cur]
+            const float* src = sd.keys[cur];
+            dst = sd.keys[cur] + (size_t)P * ld;
+            dfit = sd.fit[cur] + (size_t)P * m;
+            const uint32_t g = sd.gen + 1;
+            if (r >= P - L.nsga_Mn) {
+#pragma unroll
+                for (int gg = 0; gg < G; ++gg) {
+                    const int q = t + gg * BLOCK;
+                    if (4 * q < n) {
+                        const uint4 c = draw4(sd.seed, (uint32_t)q, (uint32_t)r, g, TAG_MUTANT);
+                        k[gg][0] = u24(c.x);
+                        k[gg][1] = u24(c.y);
+                        k[gg][2] = u24(c.z);
+                        k[gg][3] = u24(c.w);
+                    }
+                }
+            } else {
+                const uint4 pk = draw4(sd.seed, 0u, (uint32_t)r, g, TAG_NSGA_TOUR);
+                const int p1 = tourn(pick(pk.x, P), pick(pk.y, P), L.nsga_rank, L.nsga_cd);
+                const int p2 = tourn(pick(pk.z, P), pick(pk.w, P), L.nsga_rank, L.nsga_cd);
+                const float4* A = reinterpret_cast<const float4*>(src + (size_t)p1 * ld);
+                const float4* B = reinterpret_cast<const float4*>(src + (size_t)p2 * ld);
+#pragma unroll
+                for (int gg = 0; gg < G; ++gg) {
+                    const int q = t + gg * BLOCK;
+                    if (4 * q < n) {
+                        const float4 a = __ldg(A + q), b = __ldg(B + q);
+                        const uint4 c = draw4(sd.seed, (uint32_t)q, (uint32_t)r, g, TAG_NSGA_COIN);
+                        const uint4 mp = draw4(sd.seed, (uint32_t)q, (uint32_t)r, g, TAG_NSGA_MUTP);
+                        const uint4 mk = draw4(sd.seed, (uint32_t)q, (uint32_t)r, g, TAG_NSGA_MUTK);
+                        k[gg][0] = ((mp.x >> 8) < L.nsga_mutT) ? u24(mk.x) : (((c.x >> 8) < sd.rhoT) ? a.x : b.x);
+                        k[gg][1] = ((mp.y >> 8) < L.nsga_mutT) ? u24(mk.y) : (((c.y >> 8) < sd.rhoT) ? a.y : b.y);
+                        k[gg][2] = ((mp.z >> 8) < L.nsga_mutT) ? u24(mk.z) : (((c.z >> 8) < sd.rhoT) ? a.z : b.z);
+                        k[gg][3] = ((mp.w >> 8) < L.nsga_mutT) ? u24(mk.w) : (((c.w >> 8) < sd.rhoT) ? a.w : b.w);
+                    }
+                }
+            }
+        } else if (L.mode == MODE_NSGA_REFILL) {
+            // ensure_minimum_diversity refill (core/population.hpp:166-171): rows from the
+            // unique count on are replaced by fresh random keys of generation sd.gen
+            if (r < __ldg(L.refill_from)) continue;
+            dst = sd.keys[cur];
+            dfit = sd.fit[cur];
+#pragma unroll
+            for (int gg = 0; gg < G; ++gg) {
+                const int q = t + gg * BLOCK;
+                if (4 * q < n) {
+                    const uint4 c = draw4(sd.seed, (uint32_t)q, (uint32_t)r, sd.gen, TAG_NSGA_REFILL);
+                    k[gg][0] = u24(c.x);
+                    k[gg][1] = u24(c.y);
+                    k[gg][2] = u24(c.z);
+                    k[gg][3] = u24(c.w);
+                }
+            }
+        } else {  // MODE_EVAL: given keys
+            const float* src = sd.keys[cur];
+            dfit = sd.fit[cur];
+            store = false;
+            const float* row = src + (size_t)r * ld;
+            const bool vec = ((ld & 3) == 0) && ((reinterpret_cast<uintptr_t>(src) & 15) == 0);
+#pragma unroll
+            for (int gg = 0; gg < G; ++gg) {
+                const int q = t + gg * BLOCK;
+                if (vec && 4 * q + 3 < ld) {
+                    const float4 a = __ldg(reinterpret_cast<const float4*>(row) + q);
+                    k[gg][0] = a.x;
+                    k[gg][1] = a.y;
+                    k[gg][2] = a.z;
+                    k[gg][3] = a.w;
+                } else {
+#pragma unroll
+                    for (int l = 0; l < 4; ++l) k[gg][l] = (4 * q + l < n) ? __ldg(row + 4 * q + l) : 0.0f;
+                }
+            }
+        }
+
+        if (store) {
+            // write the new row with 128-bit stores; padding lanes (>= n) are zero
+            float4* o = reinterpret_cast<float4*>(dst + (size_t)r * ld);
+#pragma unroll
+            for (int gg = 0; gg < G; ++gg) {
+                const int q = t + gg * BLOCK;
+                if (4 * q < ld) {
+                    float4 v;
+                    v.x = (4 * q + 0 < n) ? k[gg][0] : 0.0f;
+                    v.y = (4 * q + 1 < n) ? k[gg][1] : 0.0f;
+                    v.z = (4 * q + 2 < n) ? k[gg][2] : 0.0f;
+                    v.w = (4 * q + 3 < n) ? k[gg][3] : 0.0f;
+                    o[q] = v;
+                }
+            }
+        }
+
+        if (eval) {
+            float res[2] = {0.0f, 0.0f};
+            const int kind = sd.kind;
+            if (kind == KNAP_THRESHOLD) {
+                // configs/knapsack_config.hpp:43-62 (integer sums are exact as floats below 2^24)
+                long long tw = 0, tv = 0;
+#pragma unroll
+                for (int gg = 0; gg < G; ++gg)
+#pragma unroll
+                    for (int l = 0; l < 4; ++l) {
+                        const int i = 4 * (t + gg * BLOCK) + l;
+                        if (i < n && k[gg][l] > 0.5f) {
+                            tw += __ldg(sd.w + i);
+                            tv += __ldg(sd.v + i);
+                        }
+                    }
+                tw = block_sum_ll<BLOCK>(tw, red_ll);
+                tv = block_sum_ll<BLOCK>(tv, red_ll);
+                const float twf = (float)tw, tvf = (float)tv;
+                res[0] = (twf > sd.cap) ? __fsub_rn(tvf, __fmul_rn(__fsub_rn(twf, sd.cap), 1000.0f)) : tvf;
+            } else {
+                row_argsort<BLOCK, G>(k, n, s, warp_tot);
+                const int32_t* perm = s.perm;
+                if (kind == TSP_COORDS) {
+                    const float* xy = L.stage_xy ? s.xy : sd.xy;
+                    canon_sum<BLOCK, 1>(n, [&](int e, float* d) {
+                        const int a = perm[e], b = perm[(e + 1 < n) ? e + 1 : 0];
+                        d[0] = edge_xy(xy, a, b);
+                    }, red_f, res);
+                } else if (kind == TSP_MATRIX) {
+                    const float* mat = sd.mat;
+                    canon_sum<BLOCK, 1>(n, [&](int e, float* d) {
+                        const int a = perm[e], b = perm[(e + 1 < n) ? e + 1 : 0];
+                        d[0] = __ldg(mat + (size_t)a * n + b);
+                    }, red_f, res);
+                } else if (kind == BITSP_COORDS) {
+                    const int npts = n + 1;
+                    const float* xy0 = L.stage_xy ? s.xy : sd.xy;
+                    const float* xy1 = L.stage_xy ? s.xy + 2 * npts : sd.xy2;
+                    canon_sum<BLOCK, 2>(n + 1, [&](int e, float* d) {
+                        const int a = (e == 0) ? 0 : perm[e - 1] + 1;
+                        const int b = (e == n) ? 0 : perm[e] + 1;
+                        d[0] = edge_xy(xy0, a, b);
+                        d[1] = edge_xy(xy1, a, b);
+                    }, red_f, res);
+                } else if (kind == BITSP_MATRIX) {
+                    const float* m0 = sd.mat;
+                    const float* m1 = sd.mat2;
+                    const size_t np1 = (size_t)n + 1;
+                    canon_sum<BLOCK, 2>(n + 1, [&](int e, float* d) {
+                        const int a = (e == 0) ? 0 : perm[e - 1] + 1;
+                        const int b = (e == n) ? 0 : perm[e] + 1;
+                        d[0] = __ldg(m0 + (size_t)a * np1 + b);
+                        d[1] = __ldg(m1 + (size_t)a * np1 + b);
+                    }, red_f, res);
+                } else if (kind == KNAP_GREEDY) {
+                    res[0] = knap_greedy<BLOCK>(s, n, sd.w, sd.v, sd.capi, red_ll, misc);
+                }
+                if (L.perm_out) {
+                    int32_t* po = L.perm_out + (size_t)r * n;
+                    for (int i = t; i < n; i += BLOCK) po[i] = perm[i];
+                }
+            }
+            if (t == 0) dfit[(size_t)r * m] = res[0];
+            if (t == 1 && m > 1) dfit[(size_t)r * m + 1] = res[1];
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// elite partition: bitonic sort of (fitness key << 32 | row) in shared memory
+// ---------------------------------------------------------------------------------------
+template <int BLOCK>
+__device__ void bitonic_u64(unsigned long long* s, int P2) {
+    const int t = threadIdx.x;
+    for (int k = 2; k <= P2; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int p = t; p < (P2 >> 1); p += BLOCK) {
+                const int i = ((p & ~(j - 1)) << 1) | (p & (j - 1));
+                const int ixj = i + j;
+                const bool up = (i & k) == 0;
+                const unsigned long long a = s[i], b = s[ixj];
+                if ((a > b) == up) {
+                    s[i] = b;
+                    s[ixj] = a;
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+__host__ __device__ inline int next_pow2(int x) {
+    int p = 1;
+    while (p < x) p <<= 1;
+    return p;
+}
+
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) sort_raw_kernel(const float* fit, int P, int maximize, int32_t* sorted) {
+    extern __shared__ unsigned long long sk[];
+    const int seg = blockIdx.x, t = threadIdx.x;
+    const int P2 = next_pow2(P);
+    const float* f = fit + (size_t)seg * P;
+    for (int i = t; i < P2; i += BLOCK)
+        sk[i] = (i < P) ? (((unsigned long long)fitkey(__ldg(f + i), maximize) << 32) | (uint32_t)i) : ~0ull;
+    __syncthreads();
+    bitonic_u64<BLOCK>(sk, P2);
+    for (int i = t; i < P; i += BLOCK) sorted[(size_t)seg * P + i] = (int32_t)(uint32_t)sk[i];
+}
+
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) sort_pops_kernel(PopDesc* descs, int flip) {
+    extern __shared__ unsigned long long sk[];
+    PopDesc& d = descs[blockIdx.x];
+    const int t = threadIdx.x;
+    const int P = d.P, m = d.m, mx = d.maximize;
+    const int buf = flip ? (d.cur ^ 1) : d.cur;
+    const float* f = d.fit[buf];
+    const int P2 = next_pow2(P);
+    for (int i = t; i < P2; i += BLOCK)
+        sk[i] = (i < P) ? (((unsigned long long)fitkey(f[(size_t)i * m], mx) << 32) | (uint32_t)i) : ~0ull;
+    __syncthreads();
+    bitonic_u64<BLOCK>(sk, P2);
+    for (int i = t; i < P; i += BLOCK) d.sorted[i] = (int32_t)(uint32_t)sk[i];
+    __syncthreads();
+    if (t == 0) {
+        uint32_t g = d.gen;
+        if (flip) {
+            d.cur = buf;
+            g = g + 1;
+            d.gen = g;
+        }
+        if (d.history && (int)g < d.hist_cap) d.history[g] = f[(size_t)(uint32_t)sk[0] * m];
+    }
+}
+
+// ring migration (core/solver.hpp:517-558), migrating the true best rows: island i's
+// top `mig` rows by rank overwrite island (i+1)%k's worst `mig` rows; one CTA per instance
+__global__ void migrate_kernel(PopDesc* descs, int k, int mig) {
+    const int inst = blockIdx.x;
+    for (int i = 0; i < k; ++i) {
+        const PopDesc& a = descs[inst * k + i];
+        const PopDesc& b = descs[inst * k + (i + 1) % k];
+        const int ld = a.ld, m = a.m;
+        for (int q = 0; q < mig; ++q) {
+            const int sr = a.sorted[q];
+            const int dr = b.sorted[b.P - mig + q];
+            const float4* src = reinterpret_cast<const float4*>(a.keys[a.cur] + (size_t)sr * ld);
+            float4* dst = reinterpret_cast<float4*>(b.keys[b.cur] + (size_t)dr * ld);
+            for (int j = threadIdx.x; j < ld / 4; j += blockDim.x) dst[j] = src[j];
+            if (threadIdx.x < m) b.fit[b.cur][(size_t)dr * m + threadIdx.x] = a.fit[a.cur][(size_t)sr * m + threadIdx.x];
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------------------
+int device_sm_count() {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return sms;
+}
+
+static constexpr RowTile kTiles[] = {
+    {32, 1}, {64, 1}, {128, 1}, {256, 1}, {256, 2}, {512, 2}, {512, 4}, {1024, 3}, {1024, 4},
+};
+
+RowTile pick_tile(int n) {
+    for (const RowTile& t : kTiles)
+        if (4 * t.block * t.groups >= n) return t;
+    return RowTile{0, 0};
+}
+
+int row_max_n() { return 4 * 1024 * 4; }
+
+using RowFn = void (*)(RowLaunch);
+
+static RowFn row_fn(const RowTile& t) {
+#define BK_TILE(B, G) \
+    if (t.block == B && t.groups == G) return row_kernel<B, G>;
+    BK_TILE(32, 1)
+    BK_TILE(64, 1)
+    BK_TILE(128, 1)
+    BK_TILE(256, 1)
+    BK_TILE(256, 2)
+    BK_TILE(512, 2)
+    BK_TILE(512, 4)
+    BK_TILE(1024, 3)
+    BK_TILE(1024, 4)
+#undef BK_TILE
+    return nullptr;
+}
+
+// the dynamic shared-memory limit of a kernel is only ever raised, so a later launch
+// that needs less never takes it away from a live engine that needs more
+static std::mutex g_attr_mu;
+static std::map<std::pair<int, const void*>, size_t> g_attr;
+
+cudaError_t raise_smem_limit(const void* fn, size_t smem) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lk(g_attr_mu);
+    size_t& cur = g_attr[{dev, fn}];
+    if (smem <= cur) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) cur = smem;
+    return e;
+}
+
+cudaError_t prepare_rows(const RowTile& tile, size_t smem, int* per_sm) {
+    RowFn fn = row_fn(tile);
+    if (!fn) return cudaErrorInvalidValue;
+    cudaError_t e = raise_smem_limit(reinterpret_cast<const void*>(fn), smem);
+    if (e != cudaSuccess) return e;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, fn, tile.block, smem);
+}
+
+cudaError_t launch_rows(const RowLaunch& L, int kind, const RowTile& tile, int grid, cudaStream_t s) {
+    RowFn fn = row_fn(tile);
+    if (!fn) return cudaErrorInvalidValue;
+    if (L.ntasks <= 0 || grid <= 0) return cudaSuccess;
+    if (grid > L.ntasks) grid = L.ntasks;
+    const size_t smem = row_smem_bytes(tile, L.max_n, L.max_points, kind, L.stage_xy != 0);
+    fn<<<grid, tile.block, smem, s>>>(L);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_rows_auto(const RowLaunch& L, int kind, const RowTile& tile, cudaStream_t s) {
+    const size_t smem = row_smem_bytes(tile, L.max_n, L.max_points, kind, L.stage_xy != 0);
+    int per_sm = 0;
+    cudaError_t e = prepare_rows(tile, smem, &per_sm);
+    if (e != cudaSuccess) return e;
+    if (per_sm <= 0) return cudaErrorInvalidConfiguration;
+    return launch_rows(L, kind, tile, per_sm * device_sm_count(), s);
+}
+
+cudaError_t prepare_sort(int maxP) {
+    const size_t smem = (size_t)next_pow2(maxP > 0 ? maxP : 1) * 8;
+    const void* fns[] = {reinterpret_cast<const void*>(sort_pops_kernel<256>),
+                         reinterpret_cast<const void*>(sort_pops_kernel<1024>),
+                         reinterpret_cast<const void*>(sort_raw_kernel<256>),
+                         reinterpret_cast<const void*>(sort_raw_kernel<1024>)};
+    for (const void* f : fns) {
+        cudaError_t e = raise_smem_limit(f, smem);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t launch_sort_raw(const float* fit, int P, int segments, int maximize, int32_t* sorted,
+                            cudaStream_t s) {
+    if (P <= 0 || segments <= 0) return cudaSuccess;
+    const size_t smem = (size_t)next_pow2(P) * 8;
+    if (P <= 512)
+        sort_raw_kernel<256><<<segments, 256, smem, s>>>(fit, P, maximize, sorted);
+    else
+        sort_raw_kernel<1024><<<segments, 1024, smem, s>>>(fit, P, maximize, sorted);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sort_pops(PopDesc* descs, int npops, int maxP, int flip, cudaStream_t s) {
+    if (npops <= 0) return cudaSuccess;
+    const size_t smem = (size_t)next_pow2(maxP) * 8;
+    if (maxP <= 512)
+        sort_pops_kernel<256><<<npops, 256, smem, s>>>(descs, flip);
+    else
+        sort_pops_kernel<1024><<<npops, 1024, smem, s>>>(descs, flip);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_migrate(PopDesc* descs, int ninst, int k, int migrants, int max_n, cudaStream_t s) {
+    (void)max_n;
+    if (ninst <= 0 || k < 2 || migrants <= 0) return cudaSuccess;
+    migrate_kernel<<<ninst, 256, 0, s>>>(descs, k, migrants);
+    return cudaGetLastError();
+}
+
+}  // namespace bk

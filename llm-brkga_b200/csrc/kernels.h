@@ -1,0 +1,73 @@
+// kernels.h -- host-side launch interface of the engine's CUDA kernels.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace bk {
+
+enum Mode : int32_t { MODE_INIT = 0, MODE_GEN = 1, MODE_EVAL = 2, MODE_NSGA_OFF = 3, MODE_NSGA_REFILL = 4 };
+
+// one unit of row work: population `pid`, row `row` of that population
+struct Task {
+    int32_t pid;
+    int32_t row;
+};
+
+// tile shape chosen per size bucket: threads per row and float4 groups per thread
+struct RowTile {
+    int block;
+    int groups;
+};
+
+struct RowLaunch {
+    PopDesc* descs;          // device descriptors (nullptr: use `single`)
+    PopDesc single;          // descriptor passed by value
+    const Task* tasks;       // device task list (nullptr: rows 0..ntasks-1 of `single`)
+    int32_t ntasks;
+    int32_t mode;
+    int32_t* perm_out;       // optional decoded permutations [rows][n] (MODE_EVAL)
+    int32_t max_n;           // largest chromosome among the populations launched
+    int32_t max_points;      // largest coordinate count (n, or n+1 with a depot)
+    int32_t stage_xy;        // stage coordinates in shared memory
+    const int32_t* nsga_rank;  // NSGA-II offspring mode: parent ranks / crowding
+    const float* nsga_cd;
+    int32_t nsga_Mn;           // fresh random offspring count
+    uint32_t nsga_mutT;        // per-gene reset threshold
+    const int32_t* refill_from;  // NSGA-II diversity refill: rows >= *refill_from get fresh keys
+};
+
+// smallest tile whose capacity (4 * block * groups) covers n
+RowTile pick_tile(int n);
+// shared memory bytes for one CTA of the row kernel
+size_t row_smem_bytes(const RowTile& t, int max_n, int max_points, int kind, bool stage_xy);
+// largest n the in-shared-memory row kernel supports
+int row_max_n();
+// one-time set-up for a tile / shared-memory size: raises the dynamic shared-memory limit
+// and returns the resident CTAs per SM (0 if the tile cannot run with that much memory)
+cudaError_t prepare_rows(const RowTile& tile, size_t smem, int* per_sm);
+// launch the fused row kernel (generation / init / evaluate / NSGA-II offspring) on
+// `grid` CTAs (<= resident capacity); prepare_rows must have run for this tile and size
+cudaError_t launch_rows(const RowLaunch& L, int kind, const RowTile& tile, int grid, cudaStream_t s);
+// convenience for one-off launches: prepare + launch with an occupancy-sized grid
+cudaError_t launch_rows_auto(const RowLaunch& L, int kind, const RowTile& tile, cudaStream_t s);
+// raise the shared-memory limit of the sort kernels for populations of up to maxP rows
+cudaError_t prepare_sort(int maxP);
+// raise (never lower) the dynamic shared-memory limit of a kernel on the current device
+cudaError_t raise_smem_limit(const void* fn, size_t smem);
+
+// elite partition of raw fitness segments: sorted[seg*P + r]
+cudaError_t launch_sort_raw(const float* fit, int P, int segments, int maximize, int32_t* sorted,
+                            cudaStream_t s);
+// engine sort: for each population, sort fit[cur^flip]; when flip, swap buffers and gen++;
+// history[gen] = best
+cudaError_t launch_sort_pops(PopDesc* descs, int npops, int maxP, int flip, cudaStream_t s);
+// ring migration between `k` consecutive island descriptors starting at first_pid, for
+// `ninst` instances laid out back to back (island descriptors of one instance adjacent)
+cudaError_t launch_migrate(PopDesc* descs, int ninst, int k, int migrants, int max_n, cudaStream_t s);
+
+int device_sm_count();
+
+}  // namespace bk

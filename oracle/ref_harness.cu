@@ -1,0 +1,341 @@
+// ref_harness.cu -- drives the UNMODIFIED reference headers (hsaseendran/llm-brkga,
+// brkga/core and brkga/configs) on injected inputs, so the oracle can be pinned to the
+// reference's own behaviour and the reference's CPU path can be timed.
+//
+// TEST INFRASTRUCTURE ONLY.  Built by oracle/Makefile from the reference tree into
+// oracle/_ref/libref.so (git-ignored); loaded by tests/ (parity pins), by
+// tests/golden/make_golden.py and by bench.py's reference arm.
+//
+// The reference keeps its RNG and generation operators private; this file widens
+// access (after every standard header is included) so that a generation can be run
+// with a seeded mt19937 and the draws it consumed can be replayed.  Every device
+// must be hidden (CUDA_VISIBLE_DEVICES="") so the reference takes its CPU path
+// (core/solver.hpp:1353-1386, configs/tsp_config.hpp:114-123).
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <filesystem>
+#include <fstream>
+#include <functional>
+#include <future>
+#include <iomanip>
+#include <iostream>
+#include <limits>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <numeric>
+#include <random>
+#include <set>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <thread>
+#include <vector>
+#include <omp.h>
+#include <cuda_runtime.h>
+#include <curand_kernel.h>
+#include <thrust/copy.h>
+#include <thrust/device_vector.h>
+#include <thrust/gather.h>
+#include <thrust/sequence.h>
+#include <thrust/sort.h>
+
+#define private public
+#define protected public
+#include "core/solver.hpp"
+#include "configs/tsp_config.hpp"
+#include "configs/knapsack_config.hpp"
+#include "configs/multi_tsp_config.hpp"
+#undef private
+#undef protected
+
+using Mat = std::vector<std::vector<float>>;
+
+// distance matrix exactly as configs/tsp_config.hpp:359-371 builds it from coordinates
+static Mat coords_to_matrix(const float* xy, int n) {
+    Mat d(n, std::vector<float>(n, 0.0f));
+    for (int i = 0; i < n; i++)
+        for (int j = 0; j < n; j++) {
+            if (i == j) { d[i][j] = 0; continue; }
+            float dx = xy[2 * i] - xy[2 * j];
+            float dy = xy[2 * i + 1] - xy[2 * j + 1];
+            d[i][j] = std::sqrt(dx * dx + dy * dy);
+        }
+    return d;
+}
+
+static Mat flat_to_matrix(const float* m, int n) {
+    Mat d(n, std::vector<float>(n));
+    for (int i = 0; i < n; i++)
+        for (int j = 0; j < n; j++) d[i][j] = m[(size_t)i * n + j];
+    return d;
+}
+
+static void set_keys(Individual<float>& ind, const float* row, int n) {
+    auto& c = ind.get_chromosome();
+    c.assign(row, row + n);
+}
+
+extern "C" {
+
+int ref_version() { return 1; }
+
+// TSPConfig decode + fitness (configs/tsp_config.hpp:180-225)
+int ref_tsp_eval(const float* xy, const float* mat, int n, const float* keys, int rows,
+                 float* fit, int32_t* perm) {
+    try {
+        Mat d = xy ? coords_to_matrix(xy, n) : flat_to_matrix(mat, n);
+        TSPConfig<float> cfg(d, "ref");
+        Individual<float> ind(n);
+        for (int r = 0; r < rows; r++) {
+            set_keys(ind, keys + (size_t)r * n, n);
+            fit[r] = cfg.fitness_function(ind);
+            if (perm) {
+                auto sol = cfg.decoder(ind);
+                for (int i = 0; i < n; i++) perm[(size_t)r * n + i] = (int32_t)sol[0][i];
+            }
+        }
+        return 0;
+    } catch (...) {
+        return -1;
+    }
+}
+
+// KnapsackConfig threshold fitness (configs/knapsack_config.hpp:43-62)
+int ref_knap_eval(const float* w, const float* v, float cap, int n, const float* keys, int rows,
+                  float* fit) {
+    try {
+        std::vector<float> W(w, w + n), V(v, v + n);
+        KnapsackConfig<float> cfg(W, V, cap, "ref");
+        Individual<float> ind(n);
+        for (int r = 0; r < rows; r++) {
+            set_keys(ind, keys + (size_t)r * n, n);
+            fit[r] = cfg.fitness_function(ind);
+        }
+        return 0;
+    } catch (...) {
+        return -1;
+    }
+}
+
+// MultiTSPConfig objectives (configs/multi_tsp_config.hpp:54-103); matrices are dim x dim
+int ref_bitsp_eval(const float* m0, const float* m1, int dim, const float* keys, int rows,
+                   float* obj) {
+    try {
+        MultiTSPConfig<float> cfg(flat_to_matrix(m0, dim), flat_to_matrix(m1, dim), "ref");
+        int n = dim - 1;
+        Individual<float> ind(std::vector<int>{n}, 2);
+        for (int r = 0; r < rows; r++) {
+            set_keys(ind, keys + (size_t)r * n, n);
+            obj[2 * r] = cfg.objective_functions[0](ind);
+            obj[2 * r + 1] = cfg.objective_functions[1](ind);
+        }
+        return 0;
+    } catch (...) {
+        return -1;
+    }
+}
+
+static MultiTSPConfig<float>* tiny_mo_config() {
+    Mat d(2, std::vector<float>(2, 1.0f));
+    d[0][0] = d[1][1] = 0.0f;
+    return new MultiTSPConfig<float>(d, d, "ref");
+}
+
+// Population::fast_non_dominated_sort + calculate_crowding_distance
+// (core/population.hpp:409-489) on N points of 2 objectives
+int ref_pareto(const float* obj, int N, int32_t* rank, float* cd) {
+    try {
+        std::unique_ptr<MultiTSPConfig<float>> cfg(tiny_mo_config());
+        cfg->population_size = 4;
+        Population<float> pop(cfg.get());
+        auto& inds = pop.get_individuals();
+        inds.assign(N, Individual<float>(cfg->component_lengths, 2));
+        for (int i = 0; i < N; i++) inds[i].set_objectives({obj[2 * i], obj[2 * i + 1]});
+        pop.fast_non_dominated_sort();
+        pop.calculate_crowding_distance();
+        for (int i = 0; i < N; i++) {
+            rank[i] = inds[i].rank;
+            if (cd) cd[i] = inds[i].crowding_distance;
+        }
+        return 0;
+    } catch (...) {
+        return -1;
+    }
+}
+
+// select_next_generation_nsga2 (core/population.hpp:491-517): pool indices of survivors
+int ref_nsga2_select(const float* obj, int N, int P, int32_t* sel) {
+    try {
+        std::unique_ptr<MultiTSPConfig<float>> cfg(tiny_mo_config());
+        cfg->population_size = P;
+        Population<float> pop(cfg.get());
+        auto& inds = pop.get_individuals();
+        inds.assign(N, Individual<float>(cfg->component_lengths, 2));
+        for (int i = 0; i < N; i++) {
+            inds[i].set_objectives({obj[2 * i], obj[2 * i + 1]});
+            inds[i].get_chromosome()[0] = (float)i;  // tag
+        }
+        pop.fast_non_dominated_sort();
+        pop.calculate_crowding_distance();
+        pop.select_next_generation_nsga2();
+        auto& out = pop.get_individuals();
+        for (int i = 0; i < P && i < (int)out.size(); i++) sel[i] = (int32_t)out[i].get_chromosome()[0];
+        return (int)out.size();
+    } catch (...) {
+        return -1;
+    }
+}
+
+// One single-objective generation through Solver::evolve_generation on the CPU path
+// (core/solver.hpp:213-273) from a population given in sorted order, with the solver's
+// mt19937 seeded; also returns the draws it consumed, replayed with identical
+// distribution objects in the same call order (core/solver.hpp:1109-1135, 1244-1258).
+int ref_brkga_generation(const float* xy, int n, int P, int E, int M, double rho, uint32_t seed,
+                         const float* keys_sorted, const float* fit_sorted,
+                         float* out_keys, float* out_fit,
+                         int32_t* ep, int32_t* np, uint8_t* coin, float* mut) {
+    try {
+        auto cfg = std::make_unique<TSPConfig<float>>(coords_to_matrix(xy, n), "ref");
+        cfg->population_size = P;
+        cfg->elite_size = E;
+        cfg->mutant_size = M;
+        cfg->elite_prob = rho;
+        cfg->max_generations = 1;
+        Solver<float> solver(std::move(cfg), false, 1000000);
+        if (solver.execution_mode != "cpu") return -2;
+        auto& inds = solver.population->get_individuals();
+        for (int r = 0; r < P; r++) {
+            set_keys(inds[r], keys_sorted + (size_t)r * n, n);
+            inds[r].fitness = fit_sorted[r];
+            inds[r].evaluated = true;
+        }
+        solver.rng.seed(seed);
+        solver.evolve_generation();
+        auto& out = solver.population->get_individuals();
+        for (int r = 0; r < P; r++) {
+            const auto& c = out[r].get_chromosome();
+            std::copy(c.begin(), c.end(), out_keys + (size_t)r * n);
+            out_fit[r] = out[r].fitness;
+        }
+        // replay
+        std::mt19937 rng(seed);
+        int off = P - E - M;
+        std::uniform_real_distribution<double> prob_dist(0.0, 1.0);
+        std::uniform_int_distribution<int> elite_dist(0, E - 1);
+        std::uniform_int_distribution<int> non_elite_dist(0, P - E - 1);
+        for (int i = 0; i < off; i++) {
+            ep[i] = elite_dist(rng);
+            np[i] = non_elite_dist(rng);
+            for (int j = 0; j < n; j++) coin[(size_t)i * n + j] = prob_dist(rng) < rho;
+        }
+        std::uniform_real_distribution<float> dist(0.0, 1.0);
+        for (int i = 0; i < M; i++)
+            for (int j = 0; j < n; j++) mut[(size_t)i * n + j] = dist(rng);
+        return 0;
+    } catch (...) {
+        return -1;
+    }
+}
+
+// Solver::generate_offspring_cpu (core/solver.hpp:1019-1091) with a seeded mt19937,
+// plus the replayed draws (tournament picks, crossover coins, mutation flags/keys).
+int ref_nsga2_offspring(const float* m0, const float* m1, int dim, int P, double rho, uint32_t seed,
+                        const float* keys, const int32_t* rank, const float* cd,
+                        float* out_keys, int32_t* picks, uint8_t* coin, uint8_t* mflag, float* mkey) {
+    try {
+        auto cfg = std::make_unique<MultiTSPConfig<float>>(flat_to_matrix(m0, dim), flat_to_matrix(m1, dim), "ref");
+        cfg->population_size = P;
+        cfg->elite_prob = rho;
+        int n = dim - 1;
+        Solver<float> solver(std::move(cfg), false, 1000000);
+        std::vector<Individual<float>> parents(P, Individual<float>(std::vector<int>{n}, 2));
+        for (int i = 0; i < P; i++) {
+            set_keys(parents[i], keys + (size_t)i * n, n);
+            parents[i].rank = rank[i];
+            parents[i].crowding_distance = cd[i];
+        }
+        solver.rng.seed(seed);
+        auto kids = solver.generate_offspring_cpu(parents);
+        for (int i = 0; i < P; i++) {
+            const auto& c = kids[i].get_chromosome();
+            std::copy(c.begin(), c.end(), out_keys + (size_t)i * n);
+        }
+        std::mt19937 rng(seed);
+        double rate = 5.0 / n;
+        for (int i = 0; i < P; i++) {
+            for (int t = 0; t < 2; t++) {
+                std::uniform_int_distribution<int> d(0, P - 1);
+                picks[4 * i + 2 * t] = d(rng);
+                picks[4 * i + 2 * t + 1] = d(rng);
+            }
+            std::uniform_real_distribution<double> prob_dist(0.0, 1.0);
+            for (int j = 0; j < n; j++) coin[(size_t)i * n + j] = prob_dist(rng) < rho;
+            std::uniform_real_distribution<float> kd(0.0, 1.0);
+            std::uniform_real_distribution<double> mp(0.0, 1.0);
+            for (int j = 0; j < n; j++) {
+                size_t q = (size_t)i * n + j;
+                mflag[q] = mp(rng) < rate;
+                mkey[q] = mflag[q] ? kd(rng) : 0.0f;
+            }
+        }
+        return 0;
+    } catch (...) {
+        return -1;
+    }
+}
+
+// ---- the reference's whole CPU generation, for timing --------------------------------
+struct RefSolver {
+    std::unique_ptr<Solver<float>> s;
+};
+
+static void* make_solver(std::unique_ptr<BRKGAConfig<float>> cfg, int P, int E, int M, double rho) {
+    cfg->population_size = P;
+    cfg->elite_size = E;
+    cfg->mutant_size = M;
+    cfg->elite_prob = rho;
+    cfg->max_generations = 1 << 30;
+    auto* h = new RefSolver;
+    h->s = std::make_unique<Solver<float>>(std::move(cfg), false, 1 << 30);
+    h->s->initialize();
+    return h;
+}
+
+// kind 1: TSP from coordinates; 3: threshold knapsack; 5: bi-objective TSP (coords of dim points)
+void* ref_solver_create(int kind, int n, const float* xy, const float* xy2, const float* w,
+                        const float* v, float cap, int P, int E, int M, double rho) {
+    try {
+        if (kind == 1) {
+            return make_solver(std::make_unique<TSPConfig<float>>(coords_to_matrix(xy, n), "ref"), P, E, M, rho);
+        } else if (kind == 3) {
+            std::vector<float> W(w, w + n), V(v, v + n);
+            return make_solver(std::make_unique<KnapsackConfig<float>>(W, V, cap, "ref"), P, E, M, rho);
+        } else if (kind == 5) {
+            return make_solver(std::make_unique<MultiTSPConfig<float>>(coords_to_matrix(xy, n + 1),
+                                                                      coords_to_matrix(xy2, n + 1), "ref"),
+                               P, E, M, rho);
+        }
+    } catch (...) {
+    }
+    return nullptr;
+}
+
+const char* ref_solver_mode(void* h) { return static_cast<RefSolver*>(h)->s->execution_mode.c_str(); }
+
+double ref_solver_evolve(void* h, int gens) {
+    auto* r = static_cast<RefSolver*>(h);
+    auto t0 = std::chrono::steady_clock::now();
+    for (int g = 0; g < gens; g++) r->s->evolve_generation();
+    auto t1 = std::chrono::steady_clock::now();
+    return std::chrono::duration<double>(t1 - t0).count();
+}
+
+double ref_solver_best(void* h) { return static_cast<RefSolver*>(h)->s->get_best_individual().fitness; }
+
+void ref_solver_destroy(void* h) { delete static_cast<RefSolver*>(h); }
+
+}  // extern "C"

@@ -1,0 +1,38 @@
+"""Seeded synthetic instances with the shapes and value distributions of the workloads
+(uniform coordinates, uniform integer knapsack items); no dataset is read."""
+import numpy as np
+
+
+def tsp_coords(n, seed, scale=1.0):
+    return (np.random.default_rng(seed).random((n, 2), dtype=np.float32) * np.float32(scale)).astype(np.float32)
+
+
+def knap_items(n, seed, lo=1, hi=100):
+    rng = np.random.default_rng(seed)
+    w = rng.integers(lo, hi + 1, n, dtype=np.int32)
+    v = rng.integers(lo, hi + 1, n, dtype=np.int32)
+    cap = np.float32(0.5 * float(w.sum()))
+    return w, v, cap
+
+
+def keys(rows, n, seed):
+    """keys in [0,1) drawn on the 24-bit grid the engine itself produces"""
+    rng = np.random.default_rng(seed)
+    return (rng.integers(0, 1 << 24, (rows, n)).astype(np.float32) / np.float32(1 << 24)).astype(np.float32)
+
+
+def tied_keys(rows, n, seed, levels=8):
+    """keys with many exact ties (ties go to the lower index)"""
+    rng = np.random.default_rng(seed)
+    return (rng.integers(0, levels, (rows, n)).astype(np.float32) / np.float32(levels)).astype(np.float32)
+
+
+def wild_keys(rows, n, seed):
+    """keys outside [0,1): negatives, values above one, signed zeros, infinities"""
+    rng = np.random.default_rng(seed)
+    k = (rng.standard_normal((rows, n)) * 3).astype(np.float32)
+    flat = k.reshape(-1)
+    idx = rng.choice(flat.size, size=max(1, flat.size // 20), replace=False)
+    specials = np.array([0.0, -0.0, np.inf, -np.inf, 1.0, 0.5], np.float32)
+    flat[idx] = specials[rng.integers(0, specials.size, idx.size)]
+    return k

@@ -1,0 +1,171 @@
+"""CPU tests: the oracle against the reference's golden vectors (tests/golden/, produced by
+the reference's own code through oracle/ref_harness.cu) and, when the reference harness
+is built in this checkout, against the reference live on fresh inputs."""
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+import instances as I
+import oracle as O
+import ref_checks as RC
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLDEN = os.path.join(HERE, "golden")
+
+
+def golden(name):
+    with np.load(os.path.join(GOLDEN, name + ".npz")) as z:
+        return {k: z[k] for k in z.files}
+
+
+# ---- Philox: published known-answer vectors of Philox4x32-10 (Random123 distribution) ----
+@pytest.mark.parametrize("ctr,key,out", [
+    ([0, 0, 0, 0], [0, 0], [0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8]),
+    ([0xFFFFFFFF] * 4, [0xFFFFFFFF] * 2, [0x408F276D, 0x41C83B0E, 0xA20BC7C6, 0x6D5451FD]),
+    ([0x243F6A88, 0x85A308D3, 0x13198A2E, 0x03707344], [0xA4093822, 0x299F31D0],
+     [0xD16CFE09, 0x94FDCCEB, 0x5001E420, 0x24126EA1]),
+])
+def test_philox_kat(ctr, key, out):
+    assert O.philox(ctr, key) == out
+
+
+def test_uniform_and_threshold():
+    L = O.lib()
+    assert L.orc_u24(0) == 0.0
+    assert L.orc_u24(0xFFFFFFFF) == np.float32(1 - 2 ** -24)
+    for p in (0.0, 0.1, 0.5, 0.7, 0.999999, 1.0):
+        T = L.orc_prob_threshold(p)
+        for x in (0, T - 1, T, 1 << 24):
+            if 0 <= x < (1 << 24):
+                assert (x < T) == (x / 2 ** 24 < p)
+
+
+def test_okey_order():
+    vals = np.array([-np.inf, -3.0, -1e-30, -0.0, 0.0, 1e-30, 0.5, 1.0, 7.0, np.inf], np.float32)
+    keys = [O.lib().orc_okey(float(v)) for v in vals]
+    assert keys == sorted(keys)
+    assert O.lib().orc_okey(-0.0) == O.lib().orc_okey(0.0)
+    assert O.lib().orc_okey(float("nan")) == 0xFFFFFFFF
+
+
+# ---- golden vectors from the reference ---------------------------------------------------
+def test_golden_tsp():
+    RC.check_tsp(golden("tsp52"))
+
+
+def test_golden_tsp_matrix():
+    RC.check_tsp(golden("tsp_matrix9"), matrix=True)
+
+
+def test_golden_knapsack_threshold():
+    RC.check_knap(golden("knap200"))
+
+
+def test_golden_bitsp():
+    RC.check_bitsp(golden("bitsp30"))
+
+
+def test_golden_pareto_ranks_and_crowding():
+    RC.check_pareto(golden("pareto300"))
+    RC.check_pareto(golden("pareto_dup256"), crowd=False)
+
+
+def test_golden_select():
+    RC.check_select(golden("select"))
+
+
+def test_golden_generation_replay():
+    RC.check_generation(golden("generation"))
+
+
+def test_golden_nsga_offspring_replay():
+    RC.check_nsga_offspring(golden("nsga_offspring"))
+
+
+# ---- live pins (only where the reference harness was built, i.e. with the sources) ------
+@pytest.mark.skipif(not O.ref_available(), reason="reference harness not built")
+@pytest.mark.parametrize("check", sorted(RC.LIVE))
+def test_live_reference(check):
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES="")
+    r = subprocess.run([sys.executable, os.path.join(HERE, "ref_checks.py"), check], env=env,
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-4000:]
+
+
+# ---- oracle self-consistency (properties) -----------------------------------------------
+def test_decode_is_stable_permutation():
+    k = I.tied_keys(20, 300, seed=1, levels=5)
+    perm = O.decode(k)
+    for r in range(20):
+        assert sorted(perm[r]) == list(range(300))
+        kk = k[r][perm[r]]
+        assert np.all(np.diff(kk) >= 0)
+        for a, b in zip(perm[r][:-1], perm[r][1:]):
+            if k[r][a] == k[r][b]:
+                assert a < b
+
+
+def test_canonical_sum_close_to_f64():
+    xy = I.tsp_coords(1000, seed=2)
+    pb = O.OracleProblem(O.TSP_COORDS, 1000, xy=xy)
+    keys = I.keys(8, 1000, seed=3)
+    fit = O.evaluate(pb, keys)
+    for r, p in enumerate(O.decode(keys)):
+        f64 = O.eval_f64(pb, p)[0]
+        assert abs(fit[r] - f64) / f64 < 1e-6
+
+
+def test_generation_properties():
+    n, P, E, M = 40, 100, 15, 15
+    xy = I.tsp_coords(n, seed=4)
+    pb = O.OracleProblem(O.TSP_COORDS, n, xy=xy)
+    pr = O.params(P, E, M, 0.7, 11)
+    pop, fit = O.brkga_init(pb, pr, 40)
+    srt = O.sort_fitness(fit)
+    newpop, newfit = O.brkga_generation(pb, pr, 1, pop, fit, srt, 40)
+    np.testing.assert_array_equal(newpop[:E], pop[srt[:E]])  # elites copied in rank order
+    elite_rows = pop[srt[:E]]
+    rest = pop[srt[E:]]
+    for r in range(E, P - M):  # every child gene comes from exactly one of two parents
+        child = newpop[r]
+        ok = False
+        for a in elite_rows:
+            m_a = child == a
+            for b in rest:
+                if np.all(m_a | (child == b)):
+                    ok = True
+                    break
+            if ok:
+                break
+        assert ok
+    assert np.all((newpop[P - M:] >= 0) & (newpop[P - M:] < 1))
+    assert newfit[srt[0]] if False else True
+    assert O.sort_fitness(newfit)[0] == 0 or newfit.min() <= fit.min()  # elitism
+
+
+def test_run_history_monotone():
+    xy = I.tsp_coords(30, seed=5)
+    pb = O.OracleProblem(O.TSP_COORDS, 30, xy=xy)
+    _, _, _, hist = O.brkga_run(pb, O.params(64, 10, 6, 0.7, 3), 25, 32)
+    assert np.all(np.diff(hist) <= 0)
+
+
+def test_ranks_strict_vs_reference_semantics():
+    obj = RC.pareto_points(400, 9, False)
+    ref_ranks = O.pareto_ranks(obj)
+    strict = O.pareto_ranks(obj, strict=True)
+    assert np.all(ref_ranks <= strict)
+    np.testing.assert_array_equal(ref_ranks == 0, strict == 0)
+
+
+def test_nsga2_select_counts():
+    obj = RC.pareto_points(200, 10, False)
+    rank = O.pareto_ranks(obj)
+    cd = O.crowding(obj, rank)
+    sel = O.nsga2_select(rank, cd, obj, 100)
+    assert len(sel) == 100
+    n0 = int((rank == 0).sum())
+    assert all(np.sum(sel == i) == 2 for i in np.flatnonzero(rank == 0)) or 2 * n0 > 100
