@@ -160,6 +160,13 @@ int32_t brkga_synchronize(brkga_engine* e);
 /* Solver::run (core/solver.hpp:1517-1556): initialize + max_generations + wait */
 int32_t brkga_run(brkga_engine* e);
 int32_t brkga_generation(const brkga_engine* e);
+/* the engine's CUDA stream (cudaStream_t as void*), for callers that order their own
+ * work or timing events after the engine's queued generations */
+int32_t brkga_get_stream(brkga_engine* e, void** stream);
+/* launch shape the engine chose (autotuned per size): info[0] threads per row CTA,
+ * info[1] float4 groups per thread, info[2] grid size, info[3] coordinates staged in
+ * shared memory (1/0); cap >= 4 */
+int32_t brkga_engine_info(brkga_engine* e, int32_t* info, int32_t cap);
 /* Solver::get_best_individual (core/solver.hpp:1625): keys [n], decoded permutation [n]
  * (may be NULL), objective values [num_objectives]; host buffers, waits for the engine. */
 int32_t brkga_get_best(brkga_engine* e, float* keys, int32_t* perm, float* fitness);

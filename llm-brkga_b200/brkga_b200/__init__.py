@@ -92,6 +92,8 @@ def lib():
         "brkga_synchronize": (_i32, [_vp]),
         "brkga_run": (_i32, [_vp]),
         "brkga_generation": (_i32, [_vp]),
+        "brkga_get_stream": (_i32, [_vp, C.POINTER(_vp)]),
+        "brkga_engine_info": (_i32, [_vp, _vp, _i32]),
         "brkga_get_best": (_i32, [_vp, _vp, _vp, _vp]),
         "brkga_get_fitness_history": (_i32, [_vp, _vp, _i32, C.POINTER(_i32)]),
         "brkga_get_population": (_i32, [_vp, _vp, _vp]),
@@ -275,6 +277,20 @@ class Solver:
     @property
     def generation(self):
         return lib().brkga_generation(self.h)
+
+    @property
+    def info(self):
+        """(threads per row CTA, float4 groups per thread, grid, coordinates staged)"""
+        out = np.zeros(4, np.int32)
+        check(lib().brkga_engine_info(self.h, _ptr(out), 4))
+        return tuple(int(x) for x in out)
+
+    @property
+    def stream(self):
+        """the engine's cudaStream_t as an integer handle"""
+        s = C.c_void_p()
+        check(lib().brkga_get_stream(self.h, C.byref(s)))
+        return s.value or 0
 
     def get_best_individual(self):
         keys = np.zeros(self.n, np.float32)

@@ -2,10 +2,14 @@
 // buffers, and the device-resident solver engine.
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "../../include/brkga_b200.h"
@@ -139,6 +143,77 @@ int points_of(const ProblemData& pd) { return (pd.kind == BRKGA_BITSP_COORDS) ? 
 
 bool stage_fits(const RowTile& t, int n, int pts, int kind) {
     return row_smem_bytes(t, n, pts, kind, true) <= kMaxSmem;
+}
+
+// ---------------------------------------------------------------------------------------
+// tile choice cache
+// ---------------------------------------------------------------------------------------
+static std::mutex g_tune_mu;
+static std::map<std::tuple<int, int, int, int>, RowTile> g_tune;  // (device, kind, n, rows)
+static bool g_tune_loaded = false;
+
+static int cur_device() {
+    int d = 0;
+    cudaGetDevice(&d);
+    return d;
+}
+
+static void tune_load_file() {
+    if (g_tune_loaded) return;
+    g_tune_loaded = true;
+    const char* path = std::getenv("BRKGA_TUNE_CACHE");
+    if (!path) return;
+    FILE* f = std::fopen(path, "r");
+    if (!f) return;
+    int kind, n, rows, b, g;
+    while (std::fscanf(f, "%d %d %d %d %d", &kind, &n, &rows, &b, &g) == 5)
+        g_tune[{cur_device(), kind, n, rows}] = RowTile{b, g};
+    std::fclose(f);
+}
+
+int32_t tune_lookup(int kind, int n, int rows, RowTile* t) {
+    if (const char* forced = std::getenv("BRKGA_TILE")) {
+        int b = 0, g = 0;
+        if (std::sscanf(forced, "%d,%d", &b, &g) == 2 && 4 * b * g >= n) {
+            *t = RowTile{b, g};
+            return BRKGA_OK;
+        }
+    }
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    tune_load_file();
+    auto it = g_tune.find({cur_device(), kind, n, rows});
+    if (it == g_tune.end()) return BRKGA_ERR_NOT_READY;
+    *t = it->second;
+    return BRKGA_OK;
+}
+
+void tune_store(int kind, int n, int rows, const RowTile& t) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune[{cur_device(), kind, n, rows}] = t;
+    if (const char* path = std::getenv("BRKGA_TUNE_CACHE")) {
+        if (FILE* f = std::fopen(path, "a")) {
+            std::fprintf(f, "%d %d %d %d %d\n", kind, n, rows, t.block, t.groups);
+            std::fclose(f);
+        }
+    }
+}
+
+int32_t tile_setup(const RowTile& t, int kind, int n, int pts, TunedTile* out) {
+    TunedTile tt;
+    tt.tile = t;
+    tt.stage = stage_fits(t, n, pts, kind);
+    const size_t smem = row_smem_bytes(t, n, pts, kind, tt.stage);
+    if (smem > kMaxSmem) return fail(BRKGA_ERR_UNSUPPORTED, "tile needs too much shared memory");
+    int per_sm = 0;
+    cudaError_t e = prepare_rows(t, smem, &per_sm);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return cuda_fail(e, "tile set-up");
+    }
+    if (per_sm <= 0) return fail(BRKGA_ERR_UNSUPPORTED, "tile does not fit on an SM");
+    tt.grid = per_sm * device_sm_count();
+    *out = tt;
+    return BRKGA_OK;
 }
 
 uint32_t prob_threshold(double p) {

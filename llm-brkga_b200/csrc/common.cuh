@@ -101,11 +101,23 @@ struct PopDesc {
     float* keys[2];
     float* fit[2];            // [rows][m]
     int32_t* sorted;          // rank -> row (relative to row0) of keys[cur]
+    int2* parents;            // per child row of the next generation: (elite rank, non-elite rank)
+    int32_t* done;            // completion counter of the rank kernel (last CTA flips the state)
     float* history;           // best fitness per generation
     int32_t hist_cap;
     int32_t cur;
     uint32_t gen;
-    int32_t pad_;
+    // NSGA-II state (null for single-objective populations)
+    int32_t Mn;               // fresh random offspring per generation
+    uint32_t mutT;            // per-gene reset threshold
+    int32_t div_interval;     // ensure_minimum_diversity period (0 = off)
+    int32_t domW;             // row stride (words) of the dominance matrix
+    int32_t* nrank;           // [2P] pool ranks; [0,P) the survivors'
+    float* ncd;               // [2P] crowding distances
+    int32_t* nsel;            // [P] survivor pool indices / unique list of the diversity pass
+    uint32_t* domS;           // [2P][domW] dominance rows
+    int32_t* domcnt;          // [2P] domination counts
+    int32_t* nu;              // diversity pass: unique count, P when nothing was rebuilt
 };
 
 // ---------------------------------------------------------------------------------------

@@ -33,7 +33,8 @@ int32_t make_shape(const ProblemData& pd, const brkga_params& p, Shape* s) {
         // mutant_size here is the optional count of fresh random offspring
         if (sh.k != 1) return fail(BRKGA_ERR_UNSUPPORTED, "islands are single-objective only");
         if (P < 2) return fail(BRKGA_ERR_INVALID, "NSGA-II needs population_size >= 2");
-        if (2 * P > kMaxPop) return fail(BRKGA_ERR_UNSUPPORTED, "NSGA-II pool above " + std::to_string(kMaxPop));
+        if (P > nsga_max_population())
+            return fail(BRKGA_ERR_UNSUPPORTED, "NSGA-II population above " + std::to_string(nsga_max_population()));
         sh.Pi = P;
         sh.Mn = std::max(0, std::min(P, p.mutant_size));
     } else {
@@ -74,16 +75,13 @@ int32_t Population::allocate(int device) {
     }
     if ((st = dalloc(*this, &p, (size_t)rows * 4)) != BRKGA_OK) return st;
     sorted = (int32_t*)p;
+    if ((st = dalloc(*this, &p, (size_t)rows * 8)) != BRKGA_OK) return st;
+    parents = (int2*)p;
+    if ((st = dalloc(*this, &p, (size_t)sh.k * 4)) != BRKGA_OK) return st;
+    done = (int32_t*)p;
+    cudaMemset(done, 0, (size_t)sh.k * 4);
     if ((st = dalloc(*this, &p, (size_t)sh.k * hist_cap * 4)) != BRKGA_OK) return st;
     history = (float*)p;
-    if (sh.mo) {
-        if ((st = dalloc(*this, &p, (size_t)rows * 4)) != BRKGA_OK) return st;
-        rank = (int32_t*)p;
-        if ((st = dalloc(*this, &p, (size_t)rows * 4)) != BRKGA_OK) return st;
-        cd = (float*)p;
-        if ((st = dalloc(*this, &p, (size_t)sh.Pi * 4)) != BRKGA_OK) return st;
-        sel = (int32_t*)p;
-    }
     return BRKGA_OK;
 }
 
@@ -274,6 +272,8 @@ int32_t brkga_create(brkga_problem* pbh, const brkga_params* params, brkga_engin
             d.fit[b] = e->pop.fit[b] + (size_t)i * sh.Pi * sh.m;
         }
         d.sorted = e->pop.sorted + (size_t)i * sh.Pi;
+        d.parents = sh.mo ? nullptr : e->pop.parents + (size_t)i * sh.Pi;
+        d.done = e->pop.done + i;
         d.history = e->pop.history + (size_t)i * e->pop.hist_cap;
         d.hist_cap = e->pop.hist_cap;
         d.cur = 0;
@@ -311,26 +311,38 @@ int32_t brkga_create(brkga_problem* pbh, const brkga_params* params, brkga_engin
         e->nt_gen = sh.Pi;
         e->nt_all = sh.Pi;
     }
-    // tile, staging and grid from occupancy
-    e->tile = pick_tile(sh.n);
-    const int pts = points_of(*pd);
-    e->stage = stage_fits(e->tile, sh.n, pts, pd->kind);
-    const size_t smem = row_smem_bytes(e->tile, sh.n, pts, pd->kind, e->stage);
-    int per_sm = 0;
-    err = prepare_rows(e->tile, smem, &per_sm);
-    if (err != cudaSuccess || per_sm <= 0) {
-        destroy_engine(e);
-        return err != cudaSuccess ? cuda_fail(err, "row kernel set-up")
-                                  : fail(BRKGA_ERR_UNSUPPORTED, "row kernel does not fit on an SM");
+    // tile, staging and grid: autotuned on this engine's own rows (initialisation launches)
+    {
+        const int pts = points_of(*pd);
+        auto launch = [&](const TunedTile& tt) -> cudaError_t {
+            RowLaunch L;
+            std::memset(&L, 0, sizeof(L));
+            L.descs = e->dd;
+            L.mode = MODE_INIT;
+            L.tasks = (sh.k > 1) ? e->d_tasks_all : nullptr;
+            L.ntasks = sh.mo ? sh.Pi : e->nt_all;
+            L.max_n = sh.n;
+            L.max_points = pts;
+            L.stage_xy = tt.stage ? 1 : 0;
+            return launch_rows(L, pd->kind, tt.tile, tt.grid, e->stream);
+        };
+        TunedTile tt;
+        st = autotune_tile(pd->kind, sh.n, pts, sh.mo ? sh.Pi : e->nt_all, e->stream, launch, &tt);
+        if (st != BRKGA_OK) {
+            destroy_engine(e);
+            return st;
+        }
+        e->tile = tt.tile;
+        e->grid = tt.grid;
+        e->stage = tt.stage;
     }
-    e->grid = per_sm * device_sm_count();
     err = prepare_sort(sh.mo ? 2 * sh.Pi : sh.Pi);
     if (err != cudaSuccess) {
         destroy_engine(e);
         return cuda_fail(err, "sort set-up");
     }
     if (sh.mo) {
-        st = nsga_setup(e->nsga, e->pop, e->dd, e->tile, e->grid, e->stage);
+        st = nsga_setup(e->nsga, e->pop, e->dd, e->hd[0], e->tile, e->grid, e->stage);
         if (st != BRKGA_OK) {
             destroy_engine(e);
             return st;
@@ -440,6 +452,21 @@ int32_t brkga_run(brkga_engine* e) {
 }
 
 int32_t brkga_generation(const brkga_engine* e) { return e ? (int32_t)e->gen : BRKGA_ERR_INVALID; }
+
+int32_t brkga_engine_info(brkga_engine* e, int32_t* info, int32_t cap) {
+    if (!e || !info || cap < 4) return fail(BRKGA_ERR_INVALID, "need an engine and cap >= 4");
+    info[0] = e->tile.block;
+    info[1] = e->tile.groups;
+    info[2] = e->grid;
+    info[3] = e->stage ? 1 : 0;
+    return BRKGA_OK;
+}
+
+int32_t brkga_get_stream(brkga_engine* e, void** stream) {
+    if (!e || !stream) return fail(BRKGA_ERR_INVALID, "null argument");
+    *stream = (void*)e->stream;
+    return BRKGA_OK;
+}
 
 int32_t brkga_get_population(brkga_engine* e, float* keys, float* fitness) {
     if (!e) return fail(BRKGA_ERR_INVALID, "null engine");

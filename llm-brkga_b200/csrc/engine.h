@@ -56,6 +56,22 @@ int points_of(const ProblemData& pd);
 bool stage_fits(const RowTile& t, int n, int pts, int kind);
 uint32_t prob_threshold(double p);
 
+// Tile autotuner: times every candidate tile (capacity covering n) on `launch`, which
+// must enqueue one representative row-kernel launch for the tile and grid it is given on
+// `stream`; returns the fastest with its grid.  Results are cached per (kind, n, rows) in
+// the process and, when BRKGA_TUNE_CACHE names a file, persisted there.  BRKGA_TILE=
+// "block,groups" forces a tile.
+struct TunedTile {
+    RowTile tile{};
+    int grid = 0;
+    bool stage = false;
+};
+template <typename F>
+int32_t autotune_tile(int kind, int n, int pts, int rows, cudaStream_t stream, F&& launch, TunedTile* out);
+int32_t tune_lookup(int kind, int n, int rows, RowTile* t);
+void tune_store(int kind, int n, int rows, const RowTile& t);
+int32_t tile_setup(const RowTile& t, int kind, int n, int pts, TunedTile* out);
+
 // validated, per-island GA shape
 struct Shape {
     int k = 1;        // islands
@@ -76,6 +92,8 @@ struct Population {
     float* keys[2] = {nullptr, nullptr};
     float* fit[2] = {nullptr, nullptr};
     int32_t* sorted = nullptr;
+    int2* parents = nullptr;   // next generation's parent ranks per child row
+    int32_t* done = nullptr;   // rank-kernel completion counters, one per island
     float* history = nullptr;
     int hist_cap = 0;
     // NSGA-II state
@@ -88,5 +106,40 @@ struct Population {
     int32_t allocate(int device);
     void release(int device);
 };
+
+template <typename F>
+int32_t autotune_tile(int kind, int n, int pts, int rows, cudaStream_t stream, F&& launch, TunedTile* out) {
+    RowTile forced{};
+    if (tune_lookup(kind, n, rows, &forced) == BRKGA_OK) return tile_setup(forced, kind, n, pts, out);
+    RowTile cand[16];
+    const int nc = tile_candidates(n, cand, 16);
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    float best_ms = 1e30f;
+    TunedTile best;
+    for (int c = 0; c < nc; ++c) {
+        TunedTile tt;
+        if (tile_setup(cand[c], kind, n, pts, &tt) != BRKGA_OK) continue;
+        if (launch(tt) != cudaSuccess) continue;  // warm-up
+        cudaEventRecord(a, stream);
+        for (int r = 0; r < 3; ++r) launch(tt);
+        cudaEventRecord(b, stream);
+        if (cudaEventSynchronize(b) != cudaSuccess) continue;
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, a, b);
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = tt;
+        }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaGetLastError();
+    if (best.grid <= 0) return fail(BRKGA_ERR_UNSUPPORTED, "no row-kernel tile fits this size");
+    tune_store(kind, n, rows, best.tile);
+    *out = best;
+    return BRKGA_OK;
+}
 
 }  // namespace bk

@@ -12,8 +12,8 @@
 //      shared memory (or a distance matrix), the depot tour of the bi-objective TSP,
 //      or the knapsack decoders; FP32 tour sums use one fixed order (256 virtual lanes,
 //      xor butterflies, fixed 8-way tree) that the oracle restates bit for bit.
-// The elite partition is a bitonic sort of (fitness key, row) composites in shared
-// memory, one CTA per population.
+// The elite partition ranks (fitness key, row) composites by exact counting across the
+// grid (rank_kernel below).
 #include <climits>
 #include <cstdio>
 #include <map>
@@ -36,13 +36,11 @@ struct RowSmem {
 
 __host__ __device__ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
-__host__ __device__ inline size_t cnt_words(int block, int max_n) {
-    const int kb = (max_n + block - 1) / block;
-    return (size_t)block * (kb > 0 ? kb : 1) + 1;
-}
+// bucket counters: 4 * groups * block buckets (>= n) plus a sentinel, padded to 16 bytes
+__host__ __device__ inline size_t cnt_words(int block, int groups) { return (size_t)4 * groups * block + 4; }
 
 size_t row_smem_bytes(const RowTile& t, int max_n, int max_points, int kind, bool stage_xy) {
-    size_t b = align_up(cnt_words(t.block, max_n) * 4, 16);
+    size_t b = align_up(cnt_words(t.block, t.groups) * 4, 16);
     b += align_up((size_t)max_n * 8, 16);
     b += align_up((size_t)max_n * 4, 16);
     if (stage_xy && (kind == TSP_COORDS || kind == BITSP_COORDS))
@@ -50,11 +48,11 @@ size_t row_smem_bytes(const RowTile& t, int max_n, int max_points, int kind, boo
     return b;
 }
 
-__device__ __forceinline__ RowSmem carve(unsigned char* base, int block, int max_n, int max_points) {
+__device__ __forceinline__ RowSmem carve(unsigned char* base, int block, int groups, int max_n, int max_points) {
     RowSmem s;
     size_t off = 0;
     s.cnt = reinterpret_cast<uint32_t*>(base + off);
-    off += align_up(cnt_words(block, max_n) * 4, 16);
+    off += align_up(cnt_words(block, groups) * 4, 16);
     s.sc = reinterpret_cast<unsigned long long*>(base + off);
     off += align_up((size_t)max_n * 8, 16);
     s.perm = reinterpret_cast<int32_t*>(base + off);
@@ -76,14 +74,14 @@ __device__ __forceinline__ int bucket_of(float key, float nbf, int nb) {
     return b < nb - 1 ? b : nb - 1;
 }
 
+// Counters must be zero on entry; they are left holding bucket offsets (the caller
+// re-zeroes them while it no longer needs them).  Bucket count NB = 4 * G * BLOCK >= n,
+// thread t owns the contiguous buckets [4Gt, 4Gt + 4G) for the scan.
 template <int BLOCK, int G>
 __device__ void row_argsort(const float (&k)[G][4], int n, const RowSmem& s, uint32_t* warp_tot) {
+    constexpr int KB = 4 * G, NB = KB * BLOCK;
     const int t = threadIdx.x;
-    const int KB = (n + BLOCK - 1) / BLOCK;
-    const int NB = BLOCK * KB;
     const float nbf = (float)NB;
-    for (int b = t; b <= NB; b += BLOCK) s.cnt[b] = 0u;
-    __syncthreads();
     uint32_t bs[G][4];  // (bucket << 16) | slot
 #pragma unroll
     for (int g = 0; g < G; ++g)
@@ -97,22 +95,24 @@ __device__ void row_argsort(const float (&k)[G][4], int n, const RowSmem& s, uin
             }
         }
     __syncthreads();
-    // exclusive scan over contiguous bucket ranges [t*KB, t*KB + KB)
-    uint32_t c[4 * G];
+    uint4 c[G];
     uint32_t sum = 0;
 #pragma unroll
-    for (int i = 0; i < 4 * G; ++i) {
-        c[i] = (i < KB) ? s.cnt[t * KB + i] : 0u;
-        sum += c[i];
+    for (int g = 0; g < G; ++g) {
+        c[g] = reinterpret_cast<const uint4*>(s.cnt)[t * G + g];
+        sum += c[g].x + c[g].y + c[g].z + c[g].w;
     }
-    uint32_t total;
-    uint32_t run = block_exclusive_scan<BLOCK>(sum, warp_tot, &total);
+    uint32_t run = block_exclusive_scan<BLOCK>(sum, warp_tot, nullptr);
 #pragma unroll
-    for (int i = 0; i < 4 * G; ++i)
-        if (i < KB) {
-            s.cnt[t * KB + i] = run;
-            run += c[i];
-        }
+    for (int g = 0; g < G; ++g) {
+        uint4 o;
+        o.x = run;
+        o.y = o.x + c[g].x;
+        o.z = o.y + c[g].y;
+        o.w = o.z + c[g].z;
+        run = o.w + c[g].w;
+        reinterpret_cast<uint4*>(s.cnt)[t * G + g] = o;
+    }
     if (t == 0) s.cnt[NB] = (uint32_t)n;
     __syncthreads();
     // scatter composites
@@ -143,6 +143,13 @@ __device__ void row_argsort(const float (&k)[G][4], int n, const RowSmem& s, uin
             }
         }
     __syncthreads();
+}
+
+// zero the bucket counters (4 * G * BLOCK + 1 words) with 128-bit stores
+template <int BLOCK, int G>
+__device__ __forceinline__ void zero_counters(const RowSmem& s) {
+    uint4* c = reinterpret_cast<uint4*>(s.cnt);
+    for (int i = threadIdx.x; i < G * BLOCK + 1; i += BLOCK) c[i] = make_uint4(0u, 0u, 0u, 0u);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -202,7 +209,6 @@ __device__ __forceinline__ void canon_sum(int nedges, EdgeF edge, float* red, fl
         out[o] = __fadd_rn(__fadd_rn(__fadd_rn(g[0], g[1]), __fadd_rn(g[2], g[3])),
                            __fadd_rn(__fadd_rn(g[4], g[5]), __fadd_rn(g[6], g[7])));
     }
-    __syncthreads();
 }
 
 template <int BLOCK>
@@ -295,8 +301,15 @@ __device__ __forceinline__ int tourn(int i1, int i2, const int32_t* rank, const 
     return i2;
 }
 
+// residency target: 1536 threads per SM for one float4 group per thread, 1024 otherwise
 template <int BLOCK, int G>
-__global__ void __launch_bounds__(BLOCK) row_kernel(RowLaunch L) {
+struct RowResidency {
+    static constexpr int want = (G == 1 ? 1536 : 1024) / BLOCK;
+    static constexpr int value = want < 1 ? 1 : (want > 32 ? 32 : want);
+};
+
+template <int BLOCK, int G>
+__global__ void __launch_bounds__(BLOCK, RowResidency<BLOCK, G>::value) row_kernel(RowLaunch L) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ PopDesc sd;
     __shared__ uint32_t warp_tot[32];
@@ -305,8 +318,9 @@ __global__ void __launch_bounds__(BLOCK) row_kernel(RowLaunch L) {
     __shared__ long long misc[4];
 
     const int t = threadIdx.x;
-    const RowSmem s = carve(smem_raw, BLOCK, L.max_n, L.max_points);
+    const RowSmem s = carve(smem_raw, BLOCK, G, L.max_n, L.max_points);
     int cur_pid = -1;
+    zero_counters<BLOCK, G>(s);
 
     for (int task = blockIdx.x; task < L.ntasks; task += gridDim.x) {
         int pid = 0, r = task;
@@ -341,129 +355,82 @@ __global__ void __launch_bounds__(BLOCK) row_kernel(RowLaunch L) {
         float* dfit = nullptr;
         bool eval = true, store = true;
         const uint32_t isl = sd.island << 8;
-
+        // how the row is built: BUILD_LOAD (given keys), BUILD_COPY (elite), BUILD_RANDOM
+        // (fresh keys from one stream), BUILD_CROSS (biased crossover), BUILD_NSGA
+        // (uniform crossover + per-gene reset)
+        enum { BUILD_LOAD, BUILD_COPY, BUILD_RANDOM, BUILD_CROSS, BUILD_NSGA };
+        int build = BUILD_LOAD;
+        uint32_t gdraw = 0, tag0 = 0;
+        const float* src = sd.keys[cur];
+        int pa = 0, pb = 0;
         if (L.mode == MODE_GEN) {
-            const float* src = sd.keys[cur];
             dst = sd.keys[cur ^ 1];
             dfit = sd.fit[cur ^ 1];
-            const uint32_t g = sd.gen + 1;
+            gdraw = sd.gen + 1;
             if (r < E) {
-                // elite copy (core/population.hpp:700-714), fitness kept
-                const int sr = __ldg(sd.sorted + r);
-                const float4* a = reinterpret_cast<const float4*>(src + (size_t)sr * ld);
-                float4* o = reinterpret_cast<float4*>(dst + (size_t)r * ld);
-                for (int q = t; q < ld / 4; q += BLOCK) o[q] = __ldg(a + q);
-                if (t < m) dfit[(size_t)r * m + t] = __ldg(sd.fit[cur] + (size_t)sr * m + t);
-                eval = false;
-                store = false;
+                build = BUILD_COPY;
             } else if (r < P - M) {
                 // biased crossover (core/solver.hpp:1109-1135; core/cuda_kernels.cuh:120-134)
-                const uint4 pr = draw4(sd.seed, 0u, (uint32_t)r, g, isl | TAG_PARENT);
-                const int ea = __ldg(sd.sorted + pick(pr.x, (uint32_t)E));
-                const int nb = __ldg(sd.sorted + E + pick(pr.y, (uint32_t)(P - E)));
-                const float4* A = reinterpret_cast<const float4*>(src + (size_t)ea * ld);
-                const float4* B = reinterpret_cast<const float4*>(src + (size_t)nb * ld);
-#pragma unroll
-                for (int gg = 0; gg < G; ++gg) {
-                    const int q = t + gg * BLOCK;
-                    if (4 * q < n) {
-                        const float4 a = __ldg(A + q), b = __ldg(B + q);
-                        const uint4 c = draw4(sd.seed, (uint32_t)q, (uint32_t)r, g, isl | TAG_COIN);
-                        k[gg][0] = ((c.x >> 8) < sd.rhoT) ? a.x : b.x;
-                        k[gg][1] = ((c.y >> 8) < sd.rhoT) ? a.y : b.y;
-                        k[gg][2] = ((c.z >> 8) < sd.rhoT) ? a.z : b.z;
-                        k[gg][3] = ((c.w >> 8) < sd.rhoT) ? a.w : b.w;
-                    }
+                build = BUILD_CROSS;
+                tag0 = isl | TAG_COIN;
+                int2 prk;
+                if (sd.parents) {
+                    prk = sd.parents[r];
+                } else {
+                    const uint4 pr = draw4(sd.seed, 0u, (uint32_t)r, gdraw, isl | TAG_PARENT);
+                    prk = make_int2((int)pick(pr.x, (uint32_t)E), E + (int)pick(pr.y, (uint32_t)(P - E)));
                 }
+                pa = __ldg(sd.sorted + prk.x);
+                pb = __ldg(sd.sorted + prk.y);
             } else {
-                // mutant (core/solver.hpp:1244-1258)
-#pragma unroll
-                for (int gg = 0; gg < G; ++gg) {
-                    const int q = t + gg * BLOCK;
-                    if (4 * q < n) {
-                        const uint4 c = draw4(sd.seed, (uint32_t)q, (uint32_t)r, g, isl | TAG_MUTANT);
-                        k[gg][0] = u24(c.x);
-                        k[gg][1] = u24(c.y);
-                        k[gg][2] = u24(c.z);
-                        k[gg][3] = u24(c.w);
-                    }
-                }
+                build = BUILD_RANDOM;  // mutant (core/solver.hpp:1244-1258)
+                tag0 = isl | TAG_MUTANT;
             }
         } else if (L.mode == MODE_INIT) {
             // Population::initialize keys (core/population.hpp:107-110)
             dst = sd.keys[cur];
             dfit = sd.fit[cur];
-#pragma unroll
-            for (int gg = 0; gg < G; ++gg) {
-                const int q = t + gg * BLOCK;
-                if (4 * q < n) {
-                    const uint4 c = draw4(sd.seed, (uint32_t)q, (uint32_t)r, 0u, isl | TAG_INIT);
-                    k[gg][0] = u24(c.x);
-                    k[gg][1] = u24(c.y);
-                    k[gg][2] = u24(c.z);
-                    k[gg][3] = u24(c.w);
-                }
-            }
+            build = BUILD_RANDOM;
+            tag0 = isl | TAG_INIT;
         } else if (L.mode == MODE_NSGA_OFF) {
             // NSGA-II offspring (core/solver.hpp:1019-1091): pool rows [P, 2P) of keys[cur]
-            const float* src = sd.keys[cur];
             dst = sd.keys[cur] + (size_t)P * ld;
             dfit = sd.fit[cur] + (size_t)P * m;
-            const uint32_t g = sd.gen + 1;
-            if (r >= P - L.nsga_Mn) {
-#pragma unroll
-                for (int gg = 0; gg < G; ++gg) {
-                    const int q = t + gg * BLOCK;
-                    if (4 * q < n) {
-                        const uint4 c = draw4(sd.seed, (uint32_t)q, (uint32_t)r, g, TAG_MUTANT);
-                        k[gg][0] = u24(c.x);
-                        k[gg][1] = u24(c.y);
-                        k[gg][2] = u24(c.z);
-                        k[gg][3] = u24(c.w);
-                    }
-                }
+            gdraw = sd.gen + 1;
+            if (r >= P - sd.Mn) {
+                build = BUILD_RANDOM;
+                tag0 = TAG_MUTANT;
             } else {
-                const uint4 pk = draw4(sd.seed, 0u, (uint32_t)r, g, TAG_NSGA_TOUR);
-                const int p1 = tourn(pick(pk.x, P), pick(pk.y, P), L.nsga_rank, L.nsga_cd);
-                const int p2 = tourn(pick(pk.z, P), pick(pk.w, P), L.nsga_rank, L.nsga_cd);
-                const float4* A = reinterpret_cast<const float4*>(src + (size_t)p1 * ld);
-                const float4* B = reinterpret_cast<const float4*>(src + (size_t)p2 * ld);
-#pragma unroll
-                for (int gg = 0; gg < G; ++gg) {
-                    const int q = t + gg * BLOCK;
-                    if (4 * q < n) {
-                        const float4 a = __ldg(A + q), b = __ldg(B + q);
-                        const uint4 c = draw4(sd.seed, (uint32_t)q, (uint32_t)r, g, TAG_NSGA_COIN);
-                        const uint4 mp = draw4(sd.seed, (uint32_t)q, (uint32_t)r, g, TAG_NSGA_MUTP);
-                        const uint4 mk = draw4(sd.seed, (uint32_t)q, (uint32_t)r, g, TAG_NSGA_MUTK);
-                        k[gg][0] = ((mp.x >> 8) < L.nsga_mutT) ? u24(mk.x) : (((c.x >> 8) < sd.rhoT) ? a.x : b.x);
-                        k[gg][1] = ((mp.y >> 8) < L.nsga_mutT) ? u24(mk.y) : (((c.y >> 8) < sd.rhoT) ? a.y : b.y);
-                        k[gg][2] = ((mp.z >> 8) < L.nsga_mutT) ? u24(mk.z) : (((c.z >> 8) < sd.rhoT) ? a.z : b.z);
-                        k[gg][3] = ((mp.w >> 8) < L.nsga_mutT) ? u24(mk.w) : (((c.w >> 8) < sd.rhoT) ? a.w : b.w);
-                    }
-                }
+                build = BUILD_NSGA;
+                tag0 = TAG_NSGA_COIN;
+                const uint4 pk = draw4(sd.seed, 0u, (uint32_t)r, gdraw, TAG_NSGA_TOUR);
+                pa = tourn(pick(pk.x, P), pick(pk.y, P), sd.nrank, sd.ncd);
+                pb = tourn(pick(pk.z, P), pick(pk.w, P), sd.nrank, sd.ncd);
             }
         } else if (L.mode == MODE_NSGA_REFILL) {
             // ensure_minimum_diversity refill (core/population.hpp:166-171): rows from the
             // unique count on are replaced by fresh random keys of generation sd.gen
-            if (r < __ldg(L.refill_from)) continue;
+            if (r < __ldg(sd.nu)) continue;
             dst = sd.keys[cur];
             dfit = sd.fit[cur];
-#pragma unroll
-            for (int gg = 0; gg < G; ++gg) {
-                const int q = t + gg * BLOCK;
-                if (4 * q < n) {
-                    const uint4 c = draw4(sd.seed, (uint32_t)q, (uint32_t)r, sd.gen, TAG_NSGA_REFILL);
-                    k[gg][0] = u24(c.x);
-                    k[gg][1] = u24(c.y);
-                    k[gg][2] = u24(c.z);
-                    k[gg][3] = u24(c.w);
-                }
-            }
+            gdraw = sd.gen;
+            build = BUILD_RANDOM;
+            tag0 = TAG_NSGA_REFILL;
         } else {  // MODE_EVAL: given keys
-            const float* src = sd.keys[cur];
             dfit = sd.fit[cur];
             store = false;
+        }
+
+        if (build == BUILD_COPY) {
+            // elite copy (core/population.hpp:700-714), fitness kept
+            const int sr = __ldg(sd.sorted + r);
+            const float4* a = reinterpret_cast<const float4*>(src + (size_t)sr * ld);
+            float4* o = reinterpret_cast<float4*>(dst + (size_t)r * ld);
+            for (int q = t; q < ld / 4; q += BLOCK) o[q] = __ldg(a + q);
+            if (t < m) dfit[(size_t)r * m + t] = __ldg(sd.fit[cur] + (size_t)sr * m + t);
+            eval = false;
+            store = false;
+        } else if (build == BUILD_LOAD) {
             const float* row = src + (size_t)r * ld;
             const bool vec = ((ld & 3) == 0) && ((reinterpret_cast<uintptr_t>(src) & 15) == 0);
 #pragma unroll
@@ -478,6 +445,43 @@ __global__ void __launch_bounds__(BLOCK) row_kernel(RowLaunch L) {
                 } else {
 #pragma unroll
                     for (int l = 0; l < 4; ++l) k[gg][l] = (4 * q + l < n) ? __ldg(row + 4 * q + l) : 0.0f;
+                }
+            }
+        } else {
+            const float4* A = reinterpret_cast<const float4*>(src + (size_t)pa * ld);
+            const float4* Bv = reinterpret_cast<const float4*>(src + (size_t)pb * ld);
+#pragma unroll
+            for (int gg = 0; gg < G; ++gg) {
+                const int q = t + gg * BLOCK;
+                if (4 * q < n) {
+                    float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a;
+                    if (build != BUILD_RANDOM) {
+                        a = __ldg(A + q);
+                        b = __ldg(Bv + q);
+                    }
+                    // one Philox call site per group for every way a row is built
+                    const uint4 x = draw4(sd.seed, (uint32_t)q, (uint32_t)r, gdraw, tag0);
+                    if (build == BUILD_RANDOM) {
+                        k[gg][0] = u24(x.x);
+                        k[gg][1] = u24(x.y);
+                        k[gg][2] = u24(x.z);
+                        k[gg][3] = u24(x.w);
+                    } else {
+                        const uint32_t T = sd.rhoT;
+                        k[gg][0] = ((x.x >> 8) < T) ? a.x : b.x;
+                        k[gg][1] = ((x.y >> 8) < T) ? a.y : b.y;
+                        k[gg][2] = ((x.z >> 8) < T) ? a.z : b.z;
+                        k[gg][3] = ((x.w >> 8) < T) ? a.w : b.w;
+                    }
+                    if (build == BUILD_NSGA) {
+                        const uint4 mp = draw4(sd.seed, (uint32_t)q, (uint32_t)r, gdraw, TAG_NSGA_MUTP);
+                        const uint4 mk = draw4(sd.seed, (uint32_t)q, (uint32_t)r, gdraw, TAG_NSGA_MUTK);
+                        const uint32_t T = sd.mutT;
+                        if ((mp.x >> 8) < T) k[gg][0] = u24(mk.x);
+                        if ((mp.y >> 8) < T) k[gg][1] = u24(mk.y);
+                        if ((mp.z >> 8) < T) k[gg][2] = u24(mk.z);
+                        if ((mp.w >> 8) < T) k[gg][3] = u24(mk.w);
+                    }
                 }
             }
         }
@@ -521,6 +525,7 @@ __global__ void __launch_bounds__(BLOCK) row_kernel(RowLaunch L) {
                 res[0] = (twf > sd.cap) ? __fsub_rn(tvf, __fmul_rn(__fsub_rn(twf, sd.cap), 1000.0f)) : tvf;
             } else {
                 row_argsort<BLOCK, G>(k, n, s, warp_tot);
+                zero_counters<BLOCK, G>(s);  // ready for the next row (separated by the row-end barrier)
                 const int32_t* perm = s.perm;
                 if (kind == TSP_COORDS) {
                     const float* xy = L.stage_xy ? s.xy : sd.xy;
@@ -570,27 +575,22 @@ __global__ void __launch_bounds__(BLOCK) row_kernel(RowLaunch L) {
 }
 
 // ---------------------------------------------------------------------------------------
-// elite partition: bitonic sort of (fitness key << 32 | row) in shared memory
+// elite partition by exact rank counting: the composite key (fitness key << 32 | row) is
+// unique, so rank(i) = #{j : key_j < key_i} is a permutation and sorted[rank(i)] = i is
+// the stable order.  P^2 compares spread over ceil(P / RK_CH) CTAs per population, TPE
+// threads per element (each counts a slice of j), no sort network and no atomics on the
+// ranks.  In engine mode the last CTA of a population (completion counter) swaps the
+// buffer index and advances the generation; every CTA also draws the parent ranks of its
+// slice of the next generation's child rows (they depend only on seed, row, generation).
 // ---------------------------------------------------------------------------------------
-template <int BLOCK>
-__device__ void bitonic_u64(unsigned long long* s, int P2) {
-    const int t = threadIdx.x;
-    for (int k = 2; k <= P2; k <<= 1) {
-        for (int j = k >> 1; j > 0; j >>= 1) {
-            for (int p = t; p < (P2 >> 1); p += BLOCK) {
-                const int i = ((p & ~(j - 1)) << 1) | (p & (j - 1));
-                const int ixj = i + j;
-                const bool up = (i & k) == 0;
-                const unsigned long long a = s[i], b = s[ixj];
-                if ((a > b) == up) {
-                    s[i] = b;
-                    s[ixj] = a;
-                }
-            }
-            __syncthreads();
-        }
-    }
-}
+constexpr int RK_THREADS = 256, RK_TPE = 32, RK_CH = RK_THREADS / RK_TPE;
+
+struct RankArgs {
+    PopDesc* descs;       // engine mode (nullptr: raw mode)
+    const float* fit;     // raw mode: segments of P fitness values
+    int32_t* sorted;
+    int P, maximize, flip;
+};
 
 __host__ __device__ inline int next_pow2(int x) {
     int p = 1;
@@ -598,42 +598,79 @@ __host__ __device__ inline int next_pow2(int x) {
     return p;
 }
 
-template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK) sort_raw_kernel(const float* fit, int P, int maximize, int32_t* sorted) {
-    extern __shared__ unsigned long long sk[];
-    const int seg = blockIdx.x, t = threadIdx.x;
-    const int P2 = next_pow2(P);
-    const float* f = fit + (size_t)seg * P;
-    for (int i = t; i < P2; i += BLOCK)
-        sk[i] = (i < P) ? (((unsigned long long)fitkey(__ldg(f + i), maximize) << 32) | (uint32_t)i) : ~0ull;
-    __syncthreads();
-    bitonic_u64<BLOCK>(sk, P2);
-    for (int i = t; i < P; i += BLOCK) sorted[(size_t)seg * P + i] = (int32_t)(uint32_t)sk[i];
-}
-
-template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK) sort_pops_kernel(PopDesc* descs, int flip) {
-    extern __shared__ unsigned long long sk[];
-    PopDesc& d = descs[blockIdx.x];
-    const int t = threadIdx.x;
-    const int P = d.P, m = d.m, mx = d.maximize;
-    const int buf = flip ? (d.cur ^ 1) : d.cur;
-    const float* f = d.fit[buf];
-    const int P2 = next_pow2(P);
-    for (int i = t; i < P2; i += BLOCK)
-        sk[i] = (i < P) ? (((unsigned long long)fitkey(f[(size_t)i * m], mx) << 32) | (uint32_t)i) : ~0ull;
-    __syncthreads();
-    bitonic_u64<BLOCK>(sk, P2);
-    for (int i = t; i < P; i += BLOCK) d.sorted[i] = (int32_t)(uint32_t)sk[i];
-    __syncthreads();
-    if (t == 0) {
-        uint32_t g = d.gen;
-        if (flip) {
-            d.cur = buf;
-            g = g + 1;
-            d.gen = g;
+__global__ void __launch_bounds__(RK_THREADS) rank_kernel(RankArgs a) {
+    extern __shared__ unsigned long long rk_keys[];
+    const int t = threadIdx.x, pop = blockIdx.y;
+    PopDesc* d = a.descs ? a.descs + pop : nullptr;
+    int P, mx, m, buf = 0;
+    const float* f;
+    int32_t* sorted;
+    uint32_t gen_new = 0;
+    if (d) {
+        P = d->P;
+        mx = d->maximize;
+        m = d->m;
+        buf = a.flip ? (d->cur ^ 1) : d->cur;
+        f = d->fit[buf];
+        sorted = d->sorted;
+        gen_new = a.flip ? d->gen + 1 : d->gen;
+    } else {
+        P = a.P;
+        mx = a.maximize;
+        m = 1;
+        f = a.fit + (size_t)pop * P;
+        sorted = a.sorted + (size_t)pop * P;
+    }
+    const int base = blockIdx.x * RK_CH;
+    if (base >= P) return;
+    // issue every global load of this thread before the first use (one HBM round trip)
+    constexpr int RK_BATCH = 8;
+    for (int i0 = t; i0 < P; i0 += RK_THREADS * RK_BATCH) {
+        float v[RK_BATCH];
+#pragma unroll
+        for (int u = 0; u < RK_BATCH; ++u) {
+            const int i = i0 + u * RK_THREADS;
+            v[u] = (i < P) ? __ldg(f + (size_t)i * m) : 0.0f;
         }
-        if (d.history && (int)g < d.hist_cap) d.history[g] = f[(size_t)(uint32_t)sk[0] * m];
+#pragma unroll
+        for (int u = 0; u < RK_BATCH; ++u) {
+            const int i = i0 + u * RK_THREADS;
+            if (i < P) rk_keys[i] = ((unsigned long long)fitkey(v[u], mx) << 32) | (uint32_t)i;
+        }
+    }
+    __syncthreads();
+    const int e = t / RK_TPE, part = t % RK_TPE;
+    const int i = base + e;
+    const unsigned long long me = (i < P) ? rk_keys[i] : 0ull;
+    // part p counts j = p, p + TPE, ...: the TPE parts of a warp read consecutive keys
+    int cnt = 0;
+#pragma unroll 8
+    for (int j = part; j < P; j += RK_TPE) cnt += (rk_keys[j] < me) ? 1 : 0;
+#pragma unroll
+    for (int o = RK_TPE / 2; o >= 1; o >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, o, RK_TPE);
+    if (part == 0 && i < P) {
+        sorted[cnt] = i;
+        if (cnt == 0 && d && d->history && (int)gen_new < d->hist_cap) d->history[gen_new] = f[(size_t)i * m];
+    }
+    if (d) {
+        // parent ranks of child row i of generation gen_new + 1 (core/solver.hpp:1117-1118)
+        if (part == 1 && d->parents && i >= d->E && i < P - d->M) {
+            const uint4 pr = draw4(d->seed, 0u, (uint32_t)i, gen_new + 1, (d->island << 8) | TAG_PARENT);
+            d->parents[i] = make_int2((int)pick(pr.x, (uint32_t)d->E), d->E + (int)pick(pr.y, (uint32_t)(P - d->E)));
+        }
+        if (a.flip) {
+            __syncthreads();
+            if (t == 0) {
+                __threadfence();
+                const int nblocks = (P + RK_CH - 1) / RK_CH;
+                if (atomicAdd(d->done, 1) == nblocks - 1) {
+                    d->cur = buf;
+                    d->gen = gen_new;
+                    *d->done = 0;
+                    __threadfence();
+                }
+            }
+        }
     }
 }
 
@@ -667,9 +704,22 @@ int device_sm_count() {
     return sms;
 }
 
+// default tile per size (smallest capacity 4 * block * groups that covers n); the
+// autotuner may pick any other tile whose capacity covers n
 static constexpr RowTile kTiles[] = {
     {32, 1}, {64, 1}, {128, 1}, {256, 1}, {256, 2}, {512, 2}, {512, 4}, {1024, 3}, {1024, 4},
 };
+static constexpr RowTile kAllTiles[] = {
+    {32, 1}, {64, 1}, {64, 2}, {128, 1}, {128, 2}, {128, 4}, {256, 1}, {256, 2}, {256, 4},
+    {512, 1}, {512, 2}, {512, 4}, {1024, 1}, {1024, 2}, {1024, 3}, {1024, 4},
+};
+
+int tile_candidates(int n, RowTile* out, int cap) {
+    int c = 0;
+    for (const RowTile& t : kAllTiles)
+        if (4 * t.block * t.groups >= n && 4 * t.block * t.groups <= 8 * n + 128 && c < cap) out[c++] = t;
+    return c;
+}
 
 RowTile pick_tile(int n) {
     for (const RowTile& t : kTiles)
@@ -686,11 +736,18 @@ static RowFn row_fn(const RowTile& t) {
     if (t.block == B && t.groups == G) return row_kernel<B, G>;
     BK_TILE(32, 1)
     BK_TILE(64, 1)
+    BK_TILE(64, 2)
     BK_TILE(128, 1)
+    BK_TILE(128, 2)
+    BK_TILE(128, 4)
     BK_TILE(256, 1)
     BK_TILE(256, 2)
+    BK_TILE(256, 4)
+    BK_TILE(512, 1)
     BK_TILE(512, 2)
     BK_TILE(512, 4)
+    BK_TILE(1024, 1)
+    BK_TILE(1024, 2)
     BK_TILE(1024, 3)
     BK_TILE(1024, 4)
 #undef BK_TILE
@@ -741,36 +798,23 @@ cudaError_t launch_rows_auto(const RowLaunch& L, int kind, const RowTile& tile, 
 }
 
 cudaError_t prepare_sort(int maxP) {
-    const size_t smem = (size_t)next_pow2(maxP > 0 ? maxP : 1) * 8;
-    const void* fns[] = {reinterpret_cast<const void*>(sort_pops_kernel<256>),
-                         reinterpret_cast<const void*>(sort_pops_kernel<1024>),
-                         reinterpret_cast<const void*>(sort_raw_kernel<256>),
-                         reinterpret_cast<const void*>(sort_raw_kernel<1024>)};
-    for (const void* f : fns) {
-        cudaError_t e = raise_smem_limit(f, smem);
-        if (e != cudaSuccess) return e;
-    }
-    return cudaSuccess;
+    return raise_smem_limit(reinterpret_cast<const void*>(rank_kernel), (size_t)(maxP > 0 ? maxP : 1) * 8);
 }
 
 cudaError_t launch_sort_raw(const float* fit, int P, int segments, int maximize, int32_t* sorted,
                             cudaStream_t s) {
     if (P <= 0 || segments <= 0) return cudaSuccess;
-    const size_t smem = (size_t)next_pow2(P) * 8;
-    if (P <= 512)
-        sort_raw_kernel<256><<<segments, 256, smem, s>>>(fit, P, maximize, sorted);
-    else
-        sort_raw_kernel<1024><<<segments, 1024, smem, s>>>(fit, P, maximize, sorted);
+    RankArgs a{nullptr, fit, sorted, P, maximize, 0};
+    dim3 grid((P + RK_CH - 1) / RK_CH, segments);
+    rank_kernel<<<grid, RK_THREADS, (size_t)P * 8, s>>>(a);
     return cudaGetLastError();
 }
 
 cudaError_t launch_sort_pops(PopDesc* descs, int npops, int maxP, int flip, cudaStream_t s) {
     if (npops <= 0) return cudaSuccess;
-    const size_t smem = (size_t)next_pow2(maxP) * 8;
-    if (maxP <= 512)
-        sort_pops_kernel<256><<<npops, 256, smem, s>>>(descs, flip);
-    else
-        sort_pops_kernel<1024><<<npops, 1024, smem, s>>>(descs, flip);
+    RankArgs a{descs, nullptr, nullptr, 0, 0, flip};
+    dim3 grid((maxP + RK_CH - 1) / RK_CH, npops);
+    rank_kernel<<<grid, RK_THREADS, (size_t)maxP * 8, s>>>(a);
     return cudaGetLastError();
 }
 

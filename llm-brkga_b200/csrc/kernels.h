@@ -32,15 +32,12 @@ struct RowLaunch {
     int32_t max_n;           // largest chromosome among the populations launched
     int32_t max_points;      // largest coordinate count (n, or n+1 with a depot)
     int32_t stage_xy;        // stage coordinates in shared memory
-    const int32_t* nsga_rank;  // NSGA-II offspring mode: parent ranks / crowding
-    const float* nsga_cd;
-    int32_t nsga_Mn;           // fresh random offspring count
-    uint32_t nsga_mutT;        // per-gene reset threshold
-    const int32_t* refill_from;  // NSGA-II diversity refill: rows >= *refill_from get fresh keys
 };
 
 // smallest tile whose capacity (4 * block * groups) covers n
 RowTile pick_tile(int n);
+// every compiled tile whose capacity covers n without being far larger (autotuning set)
+int tile_candidates(int n, RowTile* out, int cap);
 // shared memory bytes for one CTA of the row kernel
 size_t row_smem_bytes(const RowTile& t, int max_n, int max_points, int kind, bool stage_xy);
 // largest n the in-shared-memory row kernel supports

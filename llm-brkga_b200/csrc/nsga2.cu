@@ -4,17 +4,21 @@
 // Population::fast_non_dominated_sort / calculate_crowding_distance /
 // select_next_generation_nsga2 / ensure_minimum_diversity (core/population.hpp:130-517).
 //
-// Pareto ranks, two objectives (the bi-objective TSP): the pool is sorted by
-// (f0, f1); a point is then dominated exactly when the lexicographic minimum of (f1, f0)
-// over the points before it is below its own (f1, f0), so each front is one block-wide
-// exclusive min-scan over the points still unranked, and peeling repeats the scan on
-// the compacted remainder.  Any number of objectives: a bit-packed dominance matrix
-// (row i, bit j = "j dominates i") built 32 columns at a time with __ballot_sync,
-// domination counts and front peeling with __popc over the row & front-mask words.
-// Crowding: per objective a bitonic sort of (rank, objective, index) so each front is
-// contiguous and ordered; interior points add (next - prev) / range in the reference's
-// accumulation order.  Survivors: bitonic sort of (rank, -crowding, index), first P.
+// The reference pushes every first-front point into fronts[0] twice (once in
+// fast_non_dominated_sort, core/population.hpp:431-434, again in
+// build_fronts_from_domination, :335-340).  Its ranks therefore come from a peeling in
+// which the first front decrements twice, its crowding pass sees every first-front point
+// as two adjacent entries, and its survivor list takes first-front points twice.  All
+// three are reproduced here (ties fixed by index), bit for bit against the oracle.
+//
+// Ranks: bit-packed dominance matrix + bit-sliced front peeling (below).
+// Crowding: per objective a bitonic sort of (rank, objective, index) makes every front a
+// contiguous ordered run; each entry adds (next - prev) / range in list order.
+// Survivors: bitonic sort of the entry list (first-front points twice) by (rank, last
+// objective or -crowding for the front that is cut, index, copy); the first P entries.
+#include <algorithm>
 #include <cfloat>
+#include <map>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -27,44 +31,12 @@
 namespace bk {
 
 constexpr int kNsgaBlock = 1024;
-constexpr int kMaxPool = 8192;  // largest pool of the in-shared-memory select kernel
+constexpr int kMaxPool = 4096;  // largest pool (2P) of the in-shared-memory select kernel
 
 __host__ __device__ inline int npow2(int x) {
     int p = 1;
     while (p < x) p <<= 1;
     return p;
-}
-
-// ---------------------------------------------------------------------------------------
-// block helpers
-// ---------------------------------------------------------------------------------------
-template <int BLOCK>
-__device__ unsigned long long block_excl_min_u64(unsigned long long v, unsigned long long* wt) {
-    constexpr int NW = BLOCK / 32;
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    unsigned long long x = v;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= o) x = (y < x) ? y : x;
-    }
-    unsigned long long prev = __shfl_up_sync(0xffffffffu, x, 1);
-    if (lane == 0) prev = ~0ull;
-    if (lane == 31) wt[w] = x;
-    __syncthreads();
-    if (w == 0) {
-        unsigned long long s = (lane < NW) ? wt[lane] : ~0ull;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const unsigned long long y = __shfl_up_sync(0xffffffffu, s, o);
-            if (lane >= o) s = (y < s) ? y : s;
-        }
-        if (lane < NW) wt[lane] = s;
-    }
-    __syncthreads();
-    const unsigned long long base = (w > 0) ? wt[w - 1] : ~0ull;
-    __syncthreads();
-    return (base < prev) ? base : prev;
 }
 
 template <int BLOCK>
@@ -86,55 +58,230 @@ __device__ void bitonic_u64(unsigned long long* s, int N2) {
         }
 }
 
-template <int BLOCK>
-__device__ void bitonic_kv(unsigned long long* s, uint16_t* v, int N2) {
-    const int t = threadIdx.x;
-    for (int k = 2; k <= N2; k <<= 1)
-        for (int j = k >> 1; j > 0; j >>= 1) {
-            for (int p = t; p < (N2 >> 1); p += BLOCK) {
-                const int i = ((p & ~(j - 1)) << 1) | (p & (j - 1));
-                const int ixj = i + j;
-                const bool up = (i & k) == 0;
-                const unsigned long long a = s[i], b = s[ixj];
-                if ((a > b) == up) {
-                    s[i] = b;
-                    s[ixj] = a;
-                    const uint16_t x = v[i];
-                    v[i] = v[ixj];
-                    v[ixj] = x;
-                }
-            }
-            __syncthreads();
-        }
+constexpr int kCB = 16;  // count planes (two's complement)
+constexpr int kDB = 15;  // decrement planes
+
+__device__ __forceinline__ bool dominates_m(const float* a, const float* b, int m) {
+    bool better = false;
+    for (int o = 0; o < m; ++o) {
+        if (a[o] > b[o]) return false;
+        if (a[o] < b[o]) better = true;
+    }
+    return better;
 }
 
+struct DomArgs {
+    PopDesc* dd;          // engine mode: population blockIdx.y (objectives fit[cur], buffers)
+    int pool;             // engine mode: 1 = the 2P pool, 0 = the P population
+    int only_rebuilt;     // engine mode: skip populations whose diversity pass kept them (*nu >= P)
+    const float* obj;     // raw mode
+    int rawN, m;
+    uint32_t* S;          // raw mode: [N][Wmax]
+    int32_t* cnt;         // raw mode: [N]
+    int Wmax;
+};
+
+__global__ void dom_build_kernel(DomArgs a) {
+    const float* obj;
+    int N, m, Wmax;
+    uint32_t* S;
+    int32_t* cnt;
+    if (a.dd) {
+        const PopDesc& d = a.dd[blockIdx.y];
+        if (a.only_rebuilt && __ldg(d.nu) >= d.P) return;
+        N = a.pool ? 2 * d.P : d.P;
+        m = d.m;
+        obj = d.fit[d.cur];
+        S = d.domS;
+        cnt = d.domcnt;
+        Wmax = d.domW;
+    } else {
+        N = a.rawN;
+        m = a.m;
+        obj = a.obj;
+        S = a.S;
+        cnt = a.cnt;
+        Wmax = a.Wmax;
+    }
+    const int W = (N + 31) / 32;
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int i = warp; i < N; i += nwarps) {
+        float oi[4];
+        for (int o = 0; o < m && o < 4; ++o) oi[o] = __ldg(obj + (size_t)i * m + o);
+        int c = 0;
+        for (int w = 0; w < W; ++w) {
+            const int j = 32 * w + lane;
+            bool dij = false, dji = false;
+            if (j < N && j != i) {
+                float oj[4];
+                for (int o = 0; o < m && o < 4; ++o) oj[o] = __ldg(obj + (size_t)j * m + o);
+                dij = dominates_m(oi, oj, m);
+                dji = dominates_m(oj, oi, m);
+            }
+            const uint32_t si = __ballot_sync(0xffffffffu, dij);
+            const uint32_t di = __ballot_sync(0xffffffffu, dji);
+            if (lane == 0) S[(size_t)i * Wmax + w] = si;
+            c += __popc(di);
+        }
+        if (lane == 0) cnt[i] = c;
+    }
+}
+
+struct PeelSmem {
+    uint32_t* C;      // [kCB][W] count planes
+    uint32_t* A;      // [W] ranked
+    uint32_t* F;      // [W] current front
+    uint32_t* V;      // [W] valid points
+    uint16_t* list;   // [N] front members
+};
+
+__host__ __device__ inline size_t peel_smem_bytes(int N) {
+    const int W = (N + 31) / 32;
+    return (size_t)(kCB + 4) * W * 4 + (((size_t)N * 2 + 15) / 16) * 16;
+}
+
+__device__ inline PeelSmem peel_carve(unsigned char* base, int N) {
+    const int W = (N + 31) / 32;
+    PeelSmem p;
+    p.C = (uint32_t*)base;
+    p.A = p.C + (size_t)kCB * W;
+    p.F = p.A + W;
+    p.V = p.F + W;
+    p.list = (uint16_t*)(p.V + 2 * W);  // V[W..2W) stages the next front
+    return p;
+}
+
+// ranks of N points into rank[] (shared memory); S rows of stride Wmax, counts cnt[]
+template <int T>
+__device__ int peel_ranks(int N, const uint32_t* __restrict__ S, int Wmax, const int32_t* __restrict__ cnt,
+                          uint16_t* rank, const PeelSmem& ps, uint32_t* wt32) {
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int W = (N + 31) / 32;
+    // counts -> planes, valid mask
+    for (int w = warp; w < W; w += T / 32) {
+        const int i = 32 * w + lane;
+        const int c = (i < N) ? __ldg(cnt + i) : 0;
+#pragma unroll
+        for (int b = 0; b < kCB; ++b) {
+            const uint32_t pl = __ballot_sync(0xffffffffu, (c >> b) & 1);
+            if (lane == 0) ps.C[(size_t)b * W + w] = pl;
+        }
+        const uint32_t v = __ballot_sync(0xffffffffu, i < N);
+        if (lane == 0) ps.V[w] = v;
+    }
+    __syncthreads();
+    // first front: zero counts
+    for (int w = t; w < W; w += T) {
+        uint32_t z = ps.V[w];
+#pragma unroll
+        for (int b = 0; b < kCB; ++b) z &= ~ps.C[(size_t)b * W + w];
+        ps.F[w] = z;
+        ps.A[w] = z;
+        for (uint32_t x = z; x; x &= x - 1) rank[32 * w + __ffs(x) - 1] = 0;
+    }
+    __syncthreads();
+    // lanes per word for the column sums: a power of two, at most 32, SP * W <= T
+    int SP = 32;
+    while (SP > 1 && SP * W > T) SP >>= 1;
+    int k = 0;
+    for (; k < N; ++k) {
+        // front member list
+        const uint32_t pc = (t < W) ? __popc(ps.F[t]) : 0u;
+        uint32_t nf = 0;
+        uint32_t base = block_exclusive_scan<T>(pc, wt32, &nf);
+        if (t < W)
+            for (uint32_t x = ps.F[t]; x; x &= x - 1) ps.list[base++] = (uint16_t)(32 * t + __ffs(x) - 1);
+        __syncthreads();
+        if (nf == 0) break;
+        const int w = t / SP, sl = t % SP;
+        uint32_t acc[kDB];
+#pragma unroll
+        for (int b = 0; b < kDB; ++b) acc[b] = 0u;
+        if (w < W) {
+            for (int j = sl; j < (int)nf; j += SP) {
+                uint32_t carry = __ldg(S + (size_t)ps.list[j] * Wmax + w);
+#pragma unroll
+                for (int b = 0; b < kDB; ++b) {
+                    const uint32_t tb = acc[b] & carry;
+                    acc[b] ^= carry;
+                    carry = tb;
+                }
+            }
+        }
+        // combine the SP partial sums of a word (consecutive lanes) with full adders
+        for (int off = 1; off < SP; off <<= 1) {
+            uint32_t c = 0u;
+#pragma unroll
+            for (int b = 0; b < kDB; ++b) {
+                const uint32_t o = __shfl_xor_sync(0xffffffffu, acc[b], off);
+                const uint32_t s2 = acc[b] ^ o ^ c;
+                c = (acc[b] & o) | (c & (acc[b] ^ o));
+                acc[b] = s2;
+            }
+        }
+        if (w < W && sl == 0) {
+            // decrement: doubled for the first front
+            uint32_t dec[kCB];
+#pragma unroll
+            for (int b = 0; b < kCB; ++b) dec[b] = 0u;
+            if (k == 0) {
+#pragma unroll
+                for (int b = 1; b < kCB; ++b) dec[b] = (b - 1 < kDB) ? acc[b - 1] : 0u;
+            } else {
+#pragma unroll
+                for (int b = 0; b < kDB; ++b) dec[b] = acc[b];
+            }
+            uint32_t bor = 0u, any = 0u;
+#pragma unroll
+            for (int b = 0; b < kCB; ++b) {
+                const uint32_t x = ps.C[(size_t)b * W + w];
+                const uint32_t d = x ^ dec[b] ^ bor;
+                bor = (~x & dec[b]) | (~(x ^ dec[b]) & bor);
+                ps.C[(size_t)b * W + w] = d;
+                any |= d;
+            }
+            const uint32_t sign = ps.C[(size_t)(kCB - 1) * W + w];
+            const uint32_t nz = (sign | ~any) & ~ps.A[w] & ps.V[w];
+            ps.A[w] |= nz;
+            for (uint32_t x = nz; x; x &= x - 1) rank[32 * w + __ffs(x) - 1] = (uint16_t)(k + 1);
+            ps.V[W + w] = nz;  // next front, staged after the valid mask
+        }
+        __syncthreads();
+        if (t < W) ps.F[t] = ps.V[W + t];
+        __syncthreads();
+    }
+    return k;
+}
+
+
 // ---------------------------------------------------------------------------------------
-// shared-memory working set of the select kernel (N <= kMaxPool points, 2 objectives)
+// crowding and survivors (two objectives), one CTA per population
 // ---------------------------------------------------------------------------------------
 struct SelSmem {
-    float* obj;                // [N][2]
-    uint16_t* rank;            // [N]
-    float* cd;                 // [N]
-    unsigned long long* key;   // [N2]
-    uint16_t* sidx;            // [N2]
-    uint16_t* ra;              // [N]
-    uint16_t* rb;              // [N]
+    float* obj;                 // [N][2]
+    uint16_t* rank;             // [N]
+    float* cd;                  // [N]
+    unsigned long long* key;    // [K2]: next_pow2(2N) sort entries
+    uint16_t* fs;               // [N] first sorted position of each rank
+    uint16_t* fe;               // [N] last sorted position of each rank
+    unsigned char* peel;        // peel_smem_bytes(N)
 };
 
 __host__ __device__ inline size_t sel_smem_bytes(int N) {
-    const int N2 = npow2(N);
-    size_t b = (size_t)N * 8;           // obj
-    b += ((size_t)N * 2 + 15) / 16 * 16;  // rank
-    b += (size_t)N * 4;                 // cd
-    b = (b + 15) / 16 * 16;
-    b += (size_t)N2 * 8;                // key
-    b += (size_t)N2 * 2;                // sidx
-    b += (size_t)N * 2 * 2;             // ra, rb
+    const int K2 = npow2(2 * N);
+    size_t b = (size_t)N * 8;
+    b += ((size_t)N * 2 + 15) / 16 * 16;
+    b += ((size_t)N * 4 + 15) / 16 * 16;
+    b += (size_t)K2 * 8;
+    b += ((size_t)N * 2 + 15) / 16 * 16 * 2;
+    b += peel_smem_bytes(N);
     return (b + 15) / 16 * 16;
 }
 
 __device__ inline SelSmem sel_carve(unsigned char* base, int N) {
-    const int N2 = npow2(N);
+    const int K2 = npow2(2 * N);
     SelSmem s;
     size_t off = 0;
     s.obj = (float*)(base + off);
@@ -142,123 +289,142 @@ __device__ inline SelSmem sel_carve(unsigned char* base, int N) {
     s.rank = (uint16_t*)(base + off);
     off += ((size_t)N * 2 + 15) / 16 * 16;
     s.cd = (float*)(base + off);
-    off += (size_t)N * 4;
-    off = (off + 15) / 16 * 16;
+    off += ((size_t)N * 4 + 15) / 16 * 16;
     s.key = (unsigned long long*)(base + off);
-    off += (size_t)N2 * 8;
-    s.sidx = (uint16_t*)(base + off);
-    off += (size_t)N2 * 2;
-    s.ra = (uint16_t*)(base + off);
-    off += (size_t)N * 2;
-    s.rb = (uint16_t*)(base + off);
+    off += (size_t)K2 * 8;
+    s.fs = (uint16_t*)(base + off);
+    off += ((size_t)N * 2 + 15) / 16 * 16;
+    s.fe = (uint16_t*)(base + off);
+    off += ((size_t)N * 2 + 15) / 16 * 16;
+    s.peel = base + off;
     return s;
-}
-
-__device__ __forceinline__ unsigned long long lex10(const float* obj, int i) {
-    return ((unsigned long long)okey(obj[2 * i + 1]) << 32) | okey(obj[2 * i]);
-}
-
-// two-objective Pareto ranks by staircase peeling; returns the number of fronts
-template <int BLOCK>
-__device__ int rank2_staircase(int N, const SelSmem& s, unsigned long long* wt64, uint32_t* wt32) {
-    const int t = threadIdx.x;
-    const int N2 = npow2(N);
-    for (int i = t; i < N2; i += BLOCK) {
-        s.key[i] = (i < N) ? (((unsigned long long)okey(s.obj[2 * i]) << 32) | okey(s.obj[2 * i + 1])) : ~0ull;
-        s.sidx[i] = (uint16_t)i;
-    }
-    __syncthreads();
-    bitonic_kv<BLOCK>(s.key, s.sidx, N2);
-    // the padding (~0 keys) sorts last, so the first N entries are the points
-    for (int p = t; p < N; p += BLOCK) s.ra[p] = s.sidx[p];
-    __syncthreads();
-    uint16_t* ra = s.ra;
-    uint16_t* rb = s.rb;
-    int nr = N, k = 0;
-    while (nr > 0) {
-        const int ch = (nr + BLOCK - 1) / BLOCK;
-        const int p0 = t * ch, p1 = min(nr, p0 + ch);
-        unsigned long long lmin = ~0ull;
-        for (int p = p0; p < p1; ++p) {
-            const unsigned long long v = lex10(s.obj, ra[p]);
-            lmin = (v < lmin) ? v : lmin;
-        }
-        const unsigned long long pm0 = block_excl_min_u64<BLOCK>(lmin, wt64);
-        unsigned long long pm = pm0;
-        uint32_t kept = 0;
-        for (int p = p0; p < p1; ++p) {
-            const int i = ra[p];
-            const unsigned long long me = lex10(s.obj, i);
-            if (pm < me) ++kept;
-            else s.rank[i] = (uint16_t)k;
-            pm = (me < pm) ? me : pm;
-        }
-        uint32_t total;
-        uint32_t base = block_exclusive_scan<BLOCK>(kept, wt32, &total);
-        pm = pm0;
-        for (int p = p0; p < p1; ++p) {
-            const int i = ra[p];
-            const unsigned long long me = lex10(s.obj, i);
-            if (pm < me) rb[base++] = (uint16_t)i;
-            pm = (me < pm) ? me : pm;
-        }
-        __syncthreads();
-        uint16_t* tmp = ra;
-        ra = rb;
-        rb = tmp;
-        nr = (int)total;
-        ++k;
-    }
-    return k;
-}
-
-// crowding distance per front, objectives processed in order (core/population.hpp:453-489)
-template <int BLOCK>
-__device__ void crowding2(int N, const SelSmem& s) {
-    const int t = threadIdx.x;
-    const int N2 = npow2(N);
-    uint16_t* fs = s.ra;  // front first position, indexed by rank
-    uint16_t* fe = s.rb;  // front last position
-    for (int i = t; i < N; i += BLOCK) s.cd[i] = 0.0f;
-    for (int o = 0; o < 2; ++o) {
-        __syncthreads();
-        for (int i = t; i < N2; i += BLOCK)
-            s.key[i] = (i < N) ? (((unsigned long long)s.rank[i] << 48) |
-                                  ((unsigned long long)okey(s.obj[2 * i + o]) << 16) | (unsigned long long)i)
-                               : ~0ull;
-        __syncthreads();
-        bitonic_u64<BLOCK>(s.key, N2);
-        for (int p = t; p < N; p += BLOCK) {
-            const int r = (int)(s.key[p] >> 48);
-            if (p == 0 || (int)(s.key[p - 1] >> 48) != r) fs[r] = (uint16_t)p;
-            if (p == N - 1 || (int)(s.key[p + 1] >> 48) != r) fe[r] = (uint16_t)p;
-        }
-        __syncthreads();
-        for (int p = t; p < N; p += BLOCK) {
-            const int i = (int)(s.key[p] & 0xFFFFu);
-            const int r = (int)(s.key[p] >> 48);
-            const int f = fs[r], l = fe[r];
-            if (l - f + 1 <= 2 || p == f || p == l) {
-                s.cd[i] = INFINITY;
-            } else {
-                const float lo = s.obj[2 * (int)(s.key[f] & 0xFFFFu) + o];
-                const float hi = s.obj[2 * (int)(s.key[l] & 0xFFFFu) + o];
-                const float range = __fsub_rn(hi, lo);
-                if (range > 0.0f) {
-                    const float a = s.obj[2 * (int)(s.key[p + 1] & 0xFFFFu) + o];
-                    const float b = s.obj[2 * (int)(s.key[p - 1] & 0xFFFFu) + o];
-                    s.cd[i] = __fadd_rn(s.cd[i], __fdiv_rn(__fsub_rn(a, b), range));
-                }
-            }
-        }
-    }
-    __syncthreads();
 }
 
 __device__ __forceinline__ uint32_t cd_key(float c) {
     const uint32_t k = okey(c);
     return (k == 0xFFFFFFFFu) ? 0xFFFFFFFFu : ~k;
 }
+
+// crowding distance (core/population.hpp:453-489) over the reference's front lists:
+// rank-0 points are two adjacent entries (index, copy 0/1), other points one
+template <int T>
+__device__ void crowding_ref(int N, const SelSmem& s) {
+    const int t = threadIdx.x;
+    const int N2 = npow2(N);
+    for (int i = t; i < N; i += T) s.cd[i] = 0.0f;
+    for (int o = 0; o < 2; ++o) {
+        __syncthreads();
+        for (int i = t; i < N2; i += T)
+            s.key[i] = (i < N) ? (((unsigned long long)s.rank[i] << 48) |
+                                  ((unsigned long long)okey(s.obj[2 * i + o]) << 16) | (unsigned long long)i)
+                               : ~0ull;
+        __syncthreads();
+        bitonic_u64<T>(s.key, N2);
+        for (int p = t; p < N; p += T) {
+            const int r = (int)(s.key[p] >> 48);
+            if (p == 0 || (int)(s.key[p - 1] >> 48) != r) s.fs[r] = (uint16_t)p;
+            if (p == N - 1 || (int)(s.key[p + 1] >> 48) != r) s.fe[r] = (uint16_t)p;
+        }
+        __syncthreads();
+#define VAL(pos) s.obj[2 * (int)(s.key[pos] & 0xFFFFu) + o]
+        for (int p = t; p < N; p += T) {
+            const int i = (int)(s.key[p] & 0xFFFFu);
+            const int r = (int)(s.key[p] >> 48);
+            const int f = s.fs[r], l = s.fe[r];
+            const int size = l - f + 1;
+            if (r == 0) {
+                // entries 2(p-f) and 2(p-f)+1 of the doubled list of 2*size entries
+                if (size == 1 || p == f || p == l) {
+                    s.cd[i] = INFINITY;
+                } else {
+                    const float range = __fsub_rn(VAL(l), VAL(f));
+                    if (range > 0.0f) {
+                        const float v = VAL(p);
+                        const float da = __fdiv_rn(__fsub_rn(v, VAL(p - 1)), range);
+                        const float db = __fdiv_rn(__fsub_rn(VAL(p + 1), v), range);
+                        s.cd[i] = __fadd_rn(__fadd_rn(s.cd[i], da), db);
+                    }
+                }
+            } else {
+                if (size <= 2 || p == f || p == l) {
+                    s.cd[i] = INFINITY;
+                } else {
+                    const float range = __fsub_rn(VAL(l), VAL(f));
+                    if (range > 0.0f)
+                        s.cd[i] = __fadd_rn(s.cd[i], __fdiv_rn(__fsub_rn(VAL(p + 1), VAL(p - 1)), range));
+                }
+            }
+        }
+#undef VAL
+    }
+    __syncthreads();
+}
+
+// survivors (core/population.hpp:491-517): whole fronts while they fit, ordered by
+// (last objective, index, copy); the cut front by (-crowding, index, copy)
+template <int T>
+__device__ void select_ref(int N, int P, const SelSmem& s, int32_t* g_sel, int32_t* g_rank, float* g_cd,
+                           float* fmin_out, uint32_t* wt32) {
+    const int t = threadIdx.x;
+    const int ch = (N + T - 1) / T;
+    const int i0 = min(N, t * ch), i1 = min(N, i0 + ch);
+    __shared__ int s_cut;
+    // entries per rank (first-front points count twice), in the key buffer before the sort
+    uint32_t* cnt = reinterpret_cast<uint32_t*>(s.key);
+    for (int r = t; r < N; r += T) cnt[r] = 0u;
+    if (t == 0) s_cut = 0x7fffffff;
+    __syncthreads();
+    for (int i = t; i < N; i += T) atomicAdd(&cnt[s.rank[i]], s.rank[i] == 0 ? 2u : 1u);
+    __syncthreads();
+    // inclusive prefix over ranks; the cut is the first rank whose prefix passes P
+    uint32_t loc = 0;
+    for (int r = i0; r < i1; ++r) loc += cnt[r];
+    uint32_t run = block_exclusive_scan<T>(loc, wt32, nullptr);
+    for (int r = i0; r < i1; ++r) {
+        run += cnt[r];
+        if (run > (uint32_t)P) {
+            atomicMin(&s_cut, r);
+            break;
+        }
+    }
+    // compact the first-front points (their second entries), in index order
+    uint32_t z = 0;
+    for (int i = i0; i < i1; ++i) z += (s.rank[i] == 0) ? 1u : 0u;
+    uint32_t n0 = 0;
+    uint32_t pos = block_exclusive_scan<T>(z, wt32, &n0);
+    for (int i = i0; i < i1; ++i)
+        if (s.rank[i] == 0) s.fe[pos++] = (uint16_t)i;
+    __syncthreads();
+    const int cut = s_cut;
+    const int E = N + (int)n0;
+    const int K2 = npow2(E);
+    for (int e = t; e < K2; e += T) {
+        unsigned long long k = ~0ull;
+        if (e < E) {
+            const int i = (e < N) ? e : (int)s.fe[e - N];
+            const int c = (e < N) ? 0 : 1;
+            const int r = s.rank[i];
+            if (r <= cut) {
+                const uint32_t sec = (r == cut) ? cd_key(s.cd[i]) : okey(s.obj[2 * i + 1]);
+                k = ((unsigned long long)r << 46) | ((unsigned long long)sec << 14) | ((unsigned long long)i << 1) |
+                    (unsigned long long)c;
+            }
+        }
+        s.key[e] = k;
+    }
+    __syncthreads();
+    bitonic_u64<T>(s.key, K2);
+    float fmin = INFINITY;
+    for (int q = t; q < P; q += T) {
+        const int i = (int)((s.key[q] >> 1) & 0x1FFFu);
+        g_sel[q] = i;
+        g_rank[q] = s.rank[i];
+        g_cd[q] = s.cd[i];
+        fmin = fminf(fmin, s.obj[2 * i]);
+    }
+    *fmin_out = fmin;
+}
+
 
 __device__ float block_min_f(float v, float* red) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -272,47 +438,32 @@ __device__ float block_min_f(float v, float* red) {
     return r;
 }
 
-// mode 0: select P survivors from the 2P pool of fit[cur];
-// mode 1: ranks + crowding of the P population (initialisation);
-// mode 2: as mode 1, only when the diversity pass rebuilt the population (*nu < P)
-__global__ void __launch_bounds__(kNsgaBlock) nsga_select_kernel(PopDesc* dd, int32_t* g_rank, float* g_cd,
-                                                                 int32_t* g_sel, const int32_t* d_nu, int mode) {
+// mode 0: survivors of the 2P pool of fit[cur]; mode 1: ranks + crowding of the P
+// population (initialisation); mode 2: as mode 1, only for populations the diversity
+// pass rebuilt (*nu < P).  One CTA per population (blockIdx.x).
+__global__ void __launch_bounds__(kNsgaBlock) nsga_select_kernel(PopDesc* dd, int mode) {
     extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ unsigned long long wt64[32];
     __shared__ uint32_t wt32[32];
     __shared__ float redf[32];
     PopDesc& d = dd[blockIdx.x];
     const int t = threadIdx.x;
     const int P = d.P;
-    if (mode == 2 && __ldg(d_nu) >= P) return;
+    if (mode == 2 && __ldg(d.nu) >= P) return;
     const int N = (mode == 0) ? 2 * P : P;
     const float* f = d.fit[d.cur];
     const SelSmem s = sel_carve(smem, N);
     for (int i = t; i < 2 * N; i += kNsgaBlock) s.obj[i] = f[i];
+    const PeelSmem ps = peel_carve(s.peel, N);
+    peel_ranks<kNsgaBlock>(N, d.domS, d.domW, d.domcnt, s.rank, ps, wt32);
     __syncthreads();
-    rank2_staircase<kNsgaBlock>(N, s, wt64, wt32);
-    __syncthreads();
-    crowding2<kNsgaBlock>(N, s);
+    crowding_ref<kNsgaBlock>(N, s);
     float fmin = INFINITY;
     if (mode == 0) {
-        const int N2 = npow2(N);
-        for (int i = t; i < N2; i += kNsgaBlock)
-            s.key[i] = (i < N) ? (((unsigned long long)s.rank[i] << 48) | ((unsigned long long)cd_key(s.cd[i]) << 16) |
-                                  (unsigned long long)i)
-                               : ~0ull;
-        __syncthreads();
-        bitonic_u64<kNsgaBlock>(s.key, N2);
-        for (int q = t; q < P; q += kNsgaBlock) {
-            const int i = (int)(s.key[q] & 0xFFFFu);
-            g_sel[q] = i;
-            g_rank[q] = s.rank[i];
-            g_cd[q] = s.cd[i];
-            fmin = fminf(fmin, s.obj[2 * i]);
-        }
+        select_ref<kNsgaBlock>(N, P, s, d.nsel, d.nrank, d.ncd, &fmin, wt32);
     } else {
         for (int i = t; i < P; i += kNsgaBlock) {
-            g_rank[i] = s.rank[i];
-            g_cd[i] = s.cd[i];
+            d.nrank[i] = s.rank[i];
+            d.ncd[i] = s.cd[i];
             fmin = fminf(fmin, s.obj[2 * i]);
         }
     }
@@ -323,9 +474,32 @@ __global__ void __launch_bounds__(kNsgaBlock) nsga_select_kernel(PopDesc* dd, in
     }
 }
 
-// survivors -> the other pool buffer, rows [0, P)
-__global__ void nsga_gather_kernel(PopDesc* dd, const int32_t* sel) {
-    const PopDesc& d = dd[0];
+// ranks only (op API, any number of objectives): one CTA
+__global__ void __launch_bounds__(kNsgaBlock) peel_op_kernel(int N, const uint32_t* S, const int32_t* cnt, int Wmax,
+                                                             int32_t* rank) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ uint32_t wt32[32];
+    uint16_t* r16 = reinterpret_cast<uint16_t*>(smem);
+    const PeelSmem ps = peel_carve(smem + (((size_t)N * 2 + 15) / 16) * 16, N);
+    peel_ranks<kNsgaBlock>(N, S, Wmax, cnt, r16, ps, wt32);
+    __syncthreads();
+    for (int i = threadIdx.x; i < N; i += kNsgaBlock) rank[i] = r16[i];
+}
+
+// crowding from given ranks (op API, two objectives): one CTA
+__global__ void __launch_bounds__(kNsgaBlock) crowd_op_kernel(const float* obj, const int32_t* rank, int N, float* cd) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const SelSmem s = sel_carve(smem, N);
+    for (int i = threadIdx.x; i < 2 * N; i += kNsgaBlock) s.obj[i] = obj[i];
+    for (int i = threadIdx.x; i < N; i += kNsgaBlock) s.rank[i] = (uint16_t)rank[i];
+    __syncthreads();
+    crowding_ref<kNsgaBlock>(N, s);
+    for (int i = threadIdx.x; i < N; i += kNsgaBlock) cd[i] = s.cd[i];
+}
+
+// survivors -> the other pool buffer, rows [0, P); population blockIdx.y
+__global__ void nsga_gather_kernel(PopDesc* dd) {
+    const PopDesc& d = dd[blockIdx.y];
     const int P = d.P, ld4 = d.ld / 4, m = d.m;
     const float4* src = reinterpret_cast<const float4*>(d.keys[d.cur]);
     float4* dst = reinterpret_cast<float4*>(d.keys[d.cur ^ 1]);
@@ -334,35 +508,36 @@ __global__ void nsga_gather_kernel(PopDesc* dd, const int32_t* sel) {
     const size_t total = (size_t)P * ld4;
     for (size_t x = (size_t)blockIdx.x * blockDim.x + threadIdx.x; x < total; x += (size_t)gridDim.x * blockDim.x) {
         const int q = (int)(x / ld4), c = (int)(x % ld4);
-        const size_t sq = (size_t)__ldg(sel + q);
+        const size_t sq = (size_t)__ldg(d.nsel + q);
         dst[x] = src[sq * ld4 + c];
         if (c == 0)
             for (int o = 0; o < m; ++o) fd[(size_t)q * m + o] = fs[sq * m + o];
     }
 }
 
-__global__ void nsga_finish_kernel(PopDesc* dd) {
-    if (threadIdx.x == 0) {
-        dd[0].cur ^= 1;
-        dd[0].gen += 1;
+// one thread per population: swap the pool buffers, advance the generation
+__global__ void nsga_finish_kernel(PopDesc* dd, int npops) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < npops) {
+        dd[p].cur ^= 1;
+        dd[p].gen += 1;
     }
 }
 
 // ensure_minimum_diversity (core/population.hpp:130-182): greedy in-order dedupe in
 // objective space (distance < 0.001, float differences squared and summed in double);
 // when fewer than 70% are unique, the unique rows move to the front in order and
-// *nu < P tells the refill and re-rank launches to run.  Runs after generation g
-// when (g - 1) % interval == 0.
-__global__ void __launch_bounds__(kNsgaBlock) nsga_diversity_kernel(PopDesc* dd, int interval, int32_t* d_nu,
-                                                                    int32_t* g_uniq) {
-    PopDesc& d = dd[0];
-    const int t = threadIdx.x, P = d.P;
+// *nu < P tells the refill and re-rank launches to run.  It runs after generation g when
+// (g - 1) % interval == 0 (the reference's counter is g - 1).  One CTA per population.
+__global__ void __launch_bounds__(kNsgaBlock) nsga_diversity_kernel(PopDesc* dd) {
+    extern __shared__ float2 uobj[];  // [P]
+    PopDesc& d = dd[blockIdx.x];
+    const int t = threadIdx.x, P = d.P, interval = d.div_interval;
     const uint32_t g = d.gen;
     if (interval <= 0 || g < 1 || ((g - 1) % (uint32_t)interval) != 0) {
-        if (t == 0) *d_nu = P;
+        if (t == 0) *d.nu = P;
         return;
     }
-    extern __shared__ float2 uobj[];  // [P]
     float* f = d.fit[d.cur];
     int nu = 0;
     for (int c = 0; c < P; ++c) {
@@ -378,7 +553,7 @@ __global__ void __launch_bounds__(kNsgaBlock) nsga_diversity_kernel(PopDesc* dd,
         if (!near) {
             if (t == 0) {
                 uobj[nu] = make_float2(c0, c1);
-                g_uniq[nu] = c;
+                d.nsel[nu] = c;
             }
             ++nu;
         }
@@ -386,136 +561,110 @@ __global__ void __launch_bounds__(kNsgaBlock) nsga_diversity_kernel(PopDesc* dd,
     }
     const double ratio = (double)nu / (double)P;
     if (!(ratio < 0.70)) {
-        if (t == 0) *d_nu = P;
+        if (t == 0) *d.nu = P;
         return;
     }
     // compact the unique rows to the front, in order (sources never precede targets)
     float4* keys = reinterpret_cast<float4*>(d.keys[d.cur]);
     const int ld4 = d.ld / 4;
     for (int i = 0; i < nu; ++i) {
-        const int src = g_uniq[i];
+        const int src = d.nsel[i];
         if (src != i) {
             for (int c = t; c < ld4; c += kNsgaBlock) keys[(size_t)i * ld4 + c] = keys[(size_t)src * ld4 + c];
             if (t < 2) f[2 * i + t] = f[2 * src + t];
         }
         __syncthreads();
     }
-    if (t == 0) *d_nu = nu;
+    if (t == 0) *d.nu = nu;
 }
 
 // ---------------------------------------------------------------------------------------
-// general-m Pareto ranks: bit-packed dominance matrix
+// host
 // ---------------------------------------------------------------------------------------
-__device__ __forceinline__ bool dominates_m(const float* a, const float* b, int m) {
-    bool better = false;
-    for (int o = 0; o < m; ++o) {
-        if (a[o] > b[o]) return false;
-        if (a[o] < b[o]) better = true;
-    }
-    return better;
+int nsga_max_population() { return kMaxPool / 2; }
+
+size_t nsga_select_smem(int maxP) { return sel_smem_bytes(2 * maxP); }
+
+cudaError_t nsga_prepare(int maxP) {
+    cudaError_t e = raise_smem_limit(reinterpret_cast<const void*>(nsga_select_kernel), sel_smem_bytes(2 * maxP));
+    if (e == cudaSuccess)
+        e = raise_smem_limit(reinterpret_cast<const void*>(nsga_diversity_kernel), (size_t)maxP * 8);
+    return e;
 }
 
-// D[i][w] bit b: point j = 32w + b dominates point i
-__global__ void dom_matrix_kernel(const float* __restrict__ obj, int N, int m, int W, uint32_t* __restrict__ D) {
-    const int lane = threadIdx.x & 31;
-    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-    for (long long x = warp; x < (long long)N * W; x += nwarps) {
-        const int i = (int)(x / W), w = (int)(x % W);
-        const int j = 32 * w + lane;
-        const bool dom = (j < N && j != i) ? dominates_m(obj + (size_t)j * m, obj + (size_t)i * m, m) : false;
-        const uint32_t word = __ballot_sync(0xffffffffu, dom);
-        if (lane == 0) D[(size_t)i * W + w] = word;
-    }
+static cudaError_t launch_dom(PopDesc* dd, int npops, int maxN, int pool, int only_rebuilt, cudaStream_t st) {
+    DomArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.dd = dd;
+    a.pool = pool;
+    a.only_rebuilt = only_rebuilt;
+    dim3 grid((maxN + 7) / 8, npops);
+    dom_build_kernel<<<grid, 256, 0, st>>>(a);
+    return cudaGetLastError();
 }
 
-// domination counts and front peeling: count_i -= popc(D[i] & front) per front
-__global__ void __launch_bounds__(kNsgaBlock) dom_peel_kernel(const uint32_t* __restrict__ D, int N, int W,
-                                                             int32_t* rank) {
-    extern __shared__ uint32_t sm[];
-    int32_t* cnt = reinterpret_cast<int32_t*>(sm);  // [N], -1 once ranked
-    uint32_t* F = sm + N;                           // [W]
-    const int t = threadIdx.x;
-    for (int i = t; i < N; i += kNsgaBlock) {
-        int c = 0;
-        for (int w = 0; w < W; ++w) c += __popc(__ldg(D + (size_t)i * W + w));
-        cnt[i] = c;
-    }
-    __syncthreads();
-    for (int k = 0; k < N; ++k) {
-        for (int w = t; w < W; w += kNsgaBlock) F[w] = 0u;
-        __syncthreads();
-        int any = 0;
-        for (int i = t; i < N; i += kNsgaBlock)
-            if (cnt[i] == 0) {
-                rank[i] = k;
-                atomicOr(&F[i >> 5], 1u << (i & 31));
-                any = 1;
-            }
-        any = __syncthreads_or(any);
-        if (!any) break;
-        for (int i = t; i < N; i += kNsgaBlock) {
-            if (cnt[i] == 0) {
-                cnt[i] = -1;
-            } else if (cnt[i] > 0) {
-                int c = 0;
-                for (int w = 0; w < W; ++w)
-                    if (F[w]) c += __popc(__ldg(D + (size_t)i * W + w) & F[w]);
-                cnt[i] -= c;
-            }
-        }
-        __syncthreads();
-    }
+// ranks, crowding and (mode 0) survivors of every population of the group
+cudaError_t nsga_enqueue_select(PopDesc* dd, int npops, int maxP, int mode, cudaStream_t st) {
+    const int maxN = (mode == 0) ? 2 * maxP : maxP;
+    cudaError_t e = launch_dom(dd, npops, maxN, mode == 0 ? 1 : 0, mode == 2 ? 1 : 0, st);
+    if (e != cudaSuccess) return e;
+    nsga_select_kernel<<<npops, kNsgaBlock, sel_smem_bytes(maxN), st>>>(dd, mode);
+    return cudaGetLastError();
 }
 
-// ranks (+ crowding) of an arbitrary two-objective point set, one CTA: op API
-__global__ void __launch_bounds__(kNsgaBlock) rank2_op_kernel(const float* obj, int N, int32_t* rank, float* cd) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ unsigned long long wt64[32];
-    __shared__ uint32_t wt32[32];
-    const SelSmem s = sel_carve(smem, N);
-    for (int i = threadIdx.x; i < 2 * N; i += kNsgaBlock) s.obj[i] = obj[i];
-    __syncthreads();
-    rank2_staircase<kNsgaBlock>(N, s, wt64, wt32);
-    __syncthreads();
-    if (cd) crowding2<kNsgaBlock>(N, s);
-    for (int i = threadIdx.x; i < N; i += kNsgaBlock) {
-        if (rank) rank[i] = s.rank[i];
-        if (cd) cd[i] = s.cd[i];
-    }
+cudaError_t nsga_enqueue_gather_finish(PopDesc* dd, int npops, int maxP, int maxld, cudaStream_t st) {
+    const int blocks = std::max(1, std::min(256, (maxP * (maxld / 4) + 255) / 256));
+    nsga_gather_kernel<<<dim3(blocks, npops), 256, 0, st>>>(dd);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    nsga_finish_kernel<<<(npops + 127) / 128, 128, 0, st>>>(dd, npops);
+    return cudaGetLastError();
 }
 
-// crowding from given ranks, one CTA: op API
-__global__ void __launch_bounds__(kNsgaBlock) crowd2_op_kernel(const float* obj, const int32_t* rank, int N, float* cd) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    const SelSmem s = sel_carve(smem, N);
-    for (int i = threadIdx.x; i < 2 * N; i += kNsgaBlock) s.obj[i] = obj[i];
-    for (int i = threadIdx.x; i < N; i += kNsgaBlock) s.rank[i] = (uint16_t)rank[i];
-    __syncthreads();
-    crowding2<kNsgaBlock>(N, s);
-    for (int i = threadIdx.x; i < N; i += kNsgaBlock) cd[i] = s.cd[i];
+cudaError_t nsga_enqueue_diversity(PopDesc* dd, int npops, int maxP, cudaStream_t st) {
+    nsga_diversity_kernel<<<npops, kNsgaBlock, (size_t)maxP * 8, st>>>(dd);
+    return cudaGetLastError();
 }
 
-// ---------------------------------------------------------------------------------------
-// host: engine integration
-// ---------------------------------------------------------------------------------------
-static cudaError_t prep_select(int N) {
-    const size_t smem = sel_smem_bytes(N);
-    const void* fns[] = {reinterpret_cast<const void*>(nsga_select_kernel),
-                         reinterpret_cast<const void*>(rank2_op_kernel),
-                         reinterpret_cast<const void*>(crowd2_op_kernel)};
-    for (const void* f : fns) {
-        cudaError_t e = raise_smem_limit(f, smem);
-        if (e != cudaSuccess) return e;
-    }
-    return cudaSuccess;
+int32_t nsga_alloc(PopDesc& d, int P, double mut_rate, int div_interval, int Mn, std::vector<void*>& allocs,
+                   size_t* bytes) {
+    const int N = 2 * P;
+    const int W = (N + 31) / 32;
+    auto get = [&](size_t b, void** p) -> int32_t {
+        cudaError_t e = cudaMalloc(p, b ? b : 16);
+        if (e != cudaSuccess) return fail(BRKGA_ERR_OOM, "cudaMalloc (NSGA-II state)");
+        allocs.push_back(*p);
+        *bytes += b;
+        return BRKGA_OK;
+    };
+    void* p = nullptr;
+    int32_t st;
+    if ((st = get((size_t)N * 4, &p)) != BRKGA_OK) return st;
+    d.nrank = (int32_t*)p;
+    if ((st = get((size_t)N * 4, &p)) != BRKGA_OK) return st;
+    d.ncd = (float*)p;
+    if ((st = get((size_t)P * 4, &p)) != BRKGA_OK) return st;
+    d.nsel = (int32_t*)p;
+    if ((st = get((size_t)N * W * 4, &p)) != BRKGA_OK) return st;
+    d.domS = (uint32_t*)p;
+    if ((st = get((size_t)N * 4, &p)) != BRKGA_OK) return st;
+    d.domcnt = (int32_t*)p;
+    if ((st = get(16, &p)) != BRKGA_OK) return st;
+    d.nu = (int32_t*)p;
+    d.domW = W;
+    d.Mn = Mn;
+    d.mutT = prob_threshold(mut_rate);
+    d.div_interval = div_interval;
+    return BRKGA_OK;
 }
 
-int32_t nsga_setup(NsgaState& s, Population& pop, PopDesc* dd, const RowTile& tile, int grid, bool stage) {
+int32_t nsga_setup(NsgaState& s, Population& pop, PopDesc* dd, PopDesc& hdesc, const RowTile& tile, int grid,
+                   bool stage) {
     s.dd = dd;
     s.P = pop.sh.Pi;
     s.N = 2 * pop.sh.Pi;
-    if (s.N > kMaxPool) return fail(BRKGA_ERR_UNSUPPORTED, "NSGA-II pool above " + std::to_string(kMaxPool));
+    if (s.P > nsga_max_population())
+        return fail(BRKGA_ERR_UNSUPPORTED, "NSGA-II population above " + std::to_string(nsga_max_population()));
     s.n = pop.sh.n;
     s.ld = pop.sh.ld;
     s.kind = pop.pd->kind;
@@ -523,28 +672,14 @@ int32_t nsga_setup(NsgaState& s, Population& pop, PopDesc* dd, const RowTile& ti
     s.tile = tile;
     s.grid = grid;
     s.stage = stage;
-    for (int b = 0; b < 2; ++b) {
-        s.keys[b] = pop.keys[b];
-        s.fit[b] = pop.fit[b];
-    }
-    s.rank = pop.rank;
-    s.cd = pop.cd;
-    s.sel = pop.sel;
-    s.history = pop.history;
-    s.hist_cap = pop.hist_cap;
-    s.Mn = pop.sh.Mn;
     const double rate = (pop.prm.mutation_rate > 0.0) ? pop.prm.mutation_rate : 5.0 / (double)pop.sh.n;
-    s.mutT = prob_threshold(rate);
+    int32_t st = nsga_alloc(hdesc, s.P, rate, pop.prm.diversity_interval, pop.sh.Mn, pop.allocs, &pop.bytes);
+    if (st != BRKGA_OK) return st;
     s.div_interval = pop.prm.diversity_interval;
-    void* p = nullptr;
-    cudaError_t e = cudaMalloc(&p, 16);
-    if (e != cudaSuccess) return fail(BRKGA_ERR_OOM, "cudaMalloc nu");
-    pop.allocs.push_back(p);
-    s.d_nu = (int32_t*)p;
-    e = prep_select(s.N);
-    if (e != cudaSuccess) return cuda_fail(e, "select set-up");
-    e = raise_smem_limit(reinterpret_cast<const void*>(nsga_diversity_kernel), (size_t)s.P * 8);
-    if (e != cudaSuccess) return cuda_fail(e, "diversity set-up");
+    cudaError_t e = cudaMemcpy(dd, &hdesc, sizeof(PopDesc), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(e, "descriptor upload");
+    e = nsga_prepare(s.P);
+    if (e != cudaSuccess) return cuda_fail(e, "NSGA-II set-up");
     s.ready = true;
     return BRKGA_OK;
 }
@@ -556,7 +691,7 @@ void nsga_set_history(NsgaState& s, float* h, int cap) {
     s.hist_cap = cap;
 }
 
-static RowLaunch nsga_launch(const NsgaState& s, int mode) {
+static RowLaunch nsga_rows(const NsgaState& s, int mode) {
     RowLaunch L;
     std::memset(&L, 0, sizeof(L));
     L.descs = s.dd;
@@ -565,44 +700,27 @@ static RowLaunch nsga_launch(const NsgaState& s, int mode) {
     L.max_n = s.n;
     L.max_points = s.max_points;
     L.stage_xy = s.stage ? 1 : 0;
-    L.nsga_rank = s.rank;
-    L.nsga_cd = s.cd;
-    L.nsga_Mn = s.Mn;
-    L.nsga_mutT = s.mutT;
-    L.refill_from = s.d_nu;
     return L;
 }
 
 cudaError_t nsga_enqueue_init(NsgaState& s, cudaStream_t st) {
-    RowLaunch L = nsga_launch(s, MODE_INIT);
-    cudaError_t e = launch_rows(L, s.kind, s.tile, s.grid, st);
+    cudaError_t e = launch_rows(nsga_rows(s, MODE_INIT), s.kind, s.tile, s.grid, st);
     if (e != cudaSuccess) return e;
-    nsga_select_kernel<<<1, kNsgaBlock, sel_smem_bytes(s.P), st>>>(s.dd, s.rank, s.cd, s.sel, s.d_nu, 1);
-    return cudaGetLastError();
+    return nsga_enqueue_select(s.dd, 1, s.P, 1, st);
 }
 
 cudaError_t nsga_enqueue_generation(NsgaState& s, cudaStream_t st) {
-    // offspring into pool rows [P, 2P) (core/solver.hpp:1019-1032) + objectives
-    RowLaunch L = nsga_launch(s, MODE_NSGA_OFF);
-    cudaError_t e = launch_rows(L, s.kind, s.tile, s.grid, st);
+    // offspring into pool rows [P, 2P) (core/solver.hpp:1019-1032) + their objectives
+    cudaError_t e = launch_rows(nsga_rows(s, MODE_NSGA_OFF), s.kind, s.tile, s.grid, st);
     if (e != cudaSuccess) return e;
-    // ranks, crowding, survivors of the 2P pool (core/population.hpp:409-517)
-    nsga_select_kernel<<<1, kNsgaBlock, sel_smem_bytes(s.N), st>>>(s.dd, s.rank, s.cd, s.sel, s.d_nu, 0);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    const int sms = device_sm_count();
-    nsga_gather_kernel<<<sms * 4, 256, 0, st>>>(s.dd, s.sel);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    nsga_finish_kernel<<<1, 32, 0, st>>>(s.dd);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    // ranks, crowding and survivors of the pool (core/population.hpp:409-517)
+    if ((e = nsga_enqueue_select(s.dd, 1, s.P, 0, st)) != cudaSuccess) return e;
+    if ((e = nsga_enqueue_gather_finish(s.dd, 1, s.P, s.ld, st)) != cudaSuccess) return e;
     if (s.div_interval > 0) {
-        // the diversity pass decides on the device whether it is due and needed
-        nsga_diversity_kernel<<<1, kNsgaBlock, (size_t)s.P * 8, st>>>(s.dd, s.div_interval, s.d_nu, s.sel);
-        if ((e = cudaGetLastError()) != cudaSuccess) return e;
-        RowLaunch R = nsga_launch(s, MODE_NSGA_REFILL);
-        e = launch_rows(R, s.kind, s.tile, s.grid, st);
-        if (e != cudaSuccess) return e;
-        nsga_select_kernel<<<1, kNsgaBlock, sel_smem_bytes(s.P), st>>>(s.dd, s.rank, s.cd, s.sel, s.d_nu, 2);
-        e = cudaGetLastError();
+        // decided on the device: due this generation, and fewer than 70% unique
+        if ((e = nsga_enqueue_diversity(s.dd, 1, s.P, st)) != cudaSuccess) return e;
+        if ((e = launch_rows(nsga_rows(s, MODE_NSGA_REFILL), s.kind, s.tile, s.grid, st)) != cudaSuccess) return e;
+        e = nsga_enqueue_select(s.dd, 1, s.P, 2, st);
     }
     return e;
 }
@@ -635,27 +753,23 @@ int32_t nsga_set_population(NsgaState& s, cudaStream_t st, const float* keys) {
     for (int r = 0; r < s.P; ++r) std::memcpy(hk.data() + (size_t)r * s.ld, keys + (size_t)r * s.n, (size_t)s.n * 4);
     cudaError_t e = cudaMemcpy(d.keys[d.cur], hk.data(), hk.size() * 4, cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return cuda_fail(e, "population upload");
-    RowLaunch L = nsga_launch(s, MODE_EVAL);
-    e = launch_rows(L, s.kind, s.tile, s.grid, st);
-    if (e == cudaSuccess) {
-        nsga_select_kernel<<<1, kNsgaBlock, sel_smem_bytes(s.P), st>>>(s.dd, s.rank, s.cd, s.sel, s.d_nu, 1);
-        e = cudaGetLastError();
-    }
+    e = launch_rows(nsga_rows(s, MODE_EVAL), s.kind, s.tile, s.grid, st);
+    if (e == cudaSuccess) e = nsga_enqueue_select(s.dd, 1, s.P, 1, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return cuda_fail(e, "population evaluate");
     return BRKGA_OK;
 }
 
-// best = the front-0 member with the largest crowding distance (update_best_from_front,
-// core/population.hpp:684-698), first such index on ties
+// best = the first-front member with the largest crowding distance (update_best_from_front,
+// core/population.hpp:684-698), the first such index on ties
 int32_t nsga_get_best(NsgaState& s, cudaStream_t st, float* keys, int32_t* perm, float* obj) {
     PopDesc d;
     int32_t rc = read_desc(s, st, &d);
     if (rc != BRKGA_OK) return rc;
     std::vector<int32_t> hr(s.P);
     std::vector<float> hc(s.P), ho((size_t)s.P * 2);
-    cudaMemcpy(hr.data(), s.rank, (size_t)s.P * 4, cudaMemcpyDeviceToHost);
-    cudaMemcpy(hc.data(), s.cd, (size_t)s.P * 4, cudaMemcpyDeviceToHost);
+    cudaMemcpy(hr.data(), d.nrank, (size_t)s.P * 4, cudaMemcpyDeviceToHost);
+    cudaMemcpy(hc.data(), d.ncd, (size_t)s.P * 4, cudaMemcpyDeviceToHost);
     cudaError_t e = cudaMemcpy(ho.data(), d.fit[d.cur], ho.size() * 4, cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return cuda_fail(e, "best read-back");
     int best = -1;
@@ -672,14 +786,7 @@ int32_t nsga_get_best(NsgaState& s, cudaStream_t st, float* keys, int32_t* perm,
         if (e != cudaSuccess) return cuda_fail(e, "best keys");
     }
     if (perm) {
-        std::vector<float> k(s.n);
-        cudaMemcpy(k.data(), row, (size_t)s.n * 4, cudaMemcpyDeviceToHost);
-        // decode on the device through the evaluate entry point's kernel
-        RowLaunch L;
-        std::memset(&L, 0, sizeof(L));
-        L.single = d;
-        L.single.keys[0] = const_cast<float*>(row);
-        L.single.cur = 0;
+        // decode on the device with the row kernel (same argsort as the generation step)
         float* tmpf = nullptr;
         int32_t* tmpp = nullptr;
         e = cudaMalloc(&tmpf, 16);
@@ -688,7 +795,12 @@ int32_t nsga_get_best(NsgaState& s, cudaStream_t st, float* keys, int32_t* perm,
             cudaFree(tmpf);
             return fail(BRKGA_ERR_OOM, "decode scratch");
         }
+        RowLaunch L;
+        std::memset(&L, 0, sizeof(L));
+        L.single = d;
+        L.single.keys[0] = const_cast<float*>(row);
         L.single.fit[0] = tmpf;
+        L.single.cur = 0;
         L.ntasks = 1;
         L.mode = MODE_EVAL;
         L.perm_out = tmpp;
@@ -711,7 +823,7 @@ int32_t nsga_get_front(NsgaState& s, cudaStream_t st, float* obj, float* keys, i
     if (rc != BRKGA_OK) return rc;
     std::vector<int32_t> hr(s.P);
     std::vector<float> ho((size_t)s.P * 2), hk((size_t)s.P * s.ld);
-    cudaMemcpy(hr.data(), s.rank, (size_t)s.P * 4, cudaMemcpyDeviceToHost);
+    cudaMemcpy(hr.data(), d.nrank, (size_t)s.P * 4, cudaMemcpyDeviceToHost);
     cudaMemcpy(ho.data(), d.fit[d.cur], ho.size() * 4, cudaMemcpyDeviceToHost);
     cudaError_t e = cudaMemcpy(hk.data(), d.keys[d.cur], hk.size() * 4, cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return cuda_fail(e, "front read-back");
@@ -731,11 +843,26 @@ int32_t nsga_get_front(NsgaState& s, cudaStream_t st, float* obj, float* keys, i
     return BRKGA_OK;
 }
 
-// scratch for the dominance matrix of the op API (grow-only, per process)
-static std::mutex g_dom_mu;
-static void* g_dom_buf = nullptr;
-static size_t g_dom_cap = 0;
-static int g_dom_dev = -1;
+// scratch of the operator entry points (grow-only, per device)
+static std::mutex g_op_mu;
+static std::map<int, std::pair<void*, size_t>> g_op_buf;
+
+static int32_t op_scratch(size_t need, void** out) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    auto& b = g_op_buf[dev];
+    if (b.second < need) {
+        if (b.first) {
+            cudaDeviceSynchronize();
+            cudaFree(b.first);
+        }
+        b = {nullptr, 0};
+        if (cudaMalloc(&b.first, need) != cudaSuccess) return fail(BRKGA_ERR_OOM, "operator scratch");
+        b.second = need;
+    }
+    *out = b.first;
+    return BRKGA_OK;
+}
 
 }  // namespace bk
 
@@ -743,69 +870,52 @@ using namespace bk;
 
 extern "C" {
 
-int32_t brkga_pareto_rank(const float* d_obj, int32_t N, int32_t m, int32_t* d_rank, void* stream) {
-    if (!d_obj || !d_rank) return fail(BRKGA_ERR_INVALID, "null argument");
-    if (N < 0 || m < 1) return fail(BRKGA_ERR_INVALID, "need N >= 0 and m >= 1");
-    if (N == 0) return BRKGA_OK;
-    if (N > 65535) return fail(BRKGA_ERR_UNSUPPORTED, "more than 65535 points");
-    cudaStream_t st = (cudaStream_t)stream;
-    cudaError_t e;
-    if (m == 2 && N <= kMaxPool) {
-        if ((e = prep_select(N)) != cudaSuccess) return cuda_fail(e, "rank set-up");
-        rank2_op_kernel<<<1, kNsgaBlock, sel_smem_bytes(N), st>>>(d_obj, N, d_rank, nullptr);
-        if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "rank launch");
-        return BRKGA_OK;
-    }
-    return brkga_pareto_rank_bitmatrix(d_obj, N, m, d_rank, stream);
-}
-
 int32_t brkga_pareto_rank_bitmatrix(const float* d_obj, int32_t N, int32_t m, int32_t* d_rank, void* stream) {
     if (!d_obj || !d_rank) return fail(BRKGA_ERR_INVALID, "null argument");
-    if (N < 0 || m < 1) return fail(BRKGA_ERR_INVALID, "need N >= 0 and m >= 1");
+    if (N < 0 || m < 1 || m > 4) return fail(BRKGA_ERR_INVALID, "need N >= 0 and 1 <= m <= 4");
     if (N == 0) return BRKGA_OK;
-    const int W = (N + 31) / 32;
-    const size_t smem = (size_t)N * 4 + (size_t)W * 4;
-    if (smem > kMaxSmem) return fail(BRKGA_ERR_UNSUPPORTED, "too many points for the peeling kernel");
+    if (N > 8192) return fail(BRKGA_ERR_UNSUPPORTED, "more than 8192 points");
     cudaStream_t st = (cudaStream_t)stream;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    std::lock_guard<std::mutex> lk(g_dom_mu);
-    const size_t need = (size_t)N * W * 4;
-    cudaError_t e;
-    if (g_dom_dev != dev || g_dom_cap < need) {
-        if (g_dom_buf) {
-            cudaStreamSynchronize(st);
-            cudaFree(g_dom_buf);
-        }
-        g_dom_buf = nullptr;
-        g_dom_cap = 0;
-        if ((e = cudaMalloc(&g_dom_buf, need)) != cudaSuccess) return fail(BRKGA_ERR_OOM, "dominance matrix");
-        g_dom_cap = need;
-        g_dom_dev = dev;
-    }
-    uint32_t* D = (uint32_t*)g_dom_buf;
-    const long long warps = (long long)N * W;
-    const int blocks = (int)std::min<long long>((warps * 32 + 255) / 256, (long long)device_sm_count() * 16);
-    dom_matrix_kernel<<<blocks, 256, 0, st>>>(d_obj, N, m, W, D);
-    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "dominance launch");
-    if ((e = raise_smem_limit(reinterpret_cast<const void*>(dom_peel_kernel), smem)) != cudaSuccess)
+    const int W = (N + 31) / 32;
+    const size_t sbytes = (size_t)N * W * 4, cbytes = (size_t)N * 4;
+    std::lock_guard<std::mutex> lk(g_op_mu);
+    void* buf = nullptr;
+    int32_t rc = op_scratch(sbytes + cbytes, &buf);
+    if (rc != BRKGA_OK) return rc;
+    DomArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.obj = d_obj;
+    a.rawN = N;
+    a.m = m;
+    a.S = (uint32_t*)buf;
+    a.cnt = (int32_t*)((char*)buf + sbytes);
+    a.Wmax = W;
+    dom_build_kernel<<<(N + 7) / 8, 256, 0, st>>>(a);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "dominance launch");
+    const size_t smem = (((size_t)N * 2 + 15) / 16) * 16 + peel_smem_bytes(N);
+    if ((e = raise_smem_limit(reinterpret_cast<const void*>(peel_op_kernel), smem)) != cudaSuccess)
         return cuda_fail(e, "peel set-up");
-    dom_peel_kernel<<<1, kNsgaBlock, smem, st>>>(D, N, W, d_rank);
+    peel_op_kernel<<<1, kNsgaBlock, smem, st>>>(N, a.S, a.cnt, W, d_rank);
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "peel launch");
-    // the scratch is reused by the next call on this stream order; callers on other
-    // streams are serialised by waiting here
+    // the scratch is shared by later calls: finish before returning
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(e, "peel");
     return BRKGA_OK;
+}
+
+int32_t brkga_pareto_rank(const float* d_obj, int32_t N, int32_t m, int32_t* d_rank, void* stream) {
+    return brkga_pareto_rank_bitmatrix(d_obj, N, m, d_rank, stream);
 }
 
 int32_t brkga_crowding(const float* d_obj, const int32_t* d_rank, int32_t N, int32_t m, float* d_cd, void* stream) {
     if (!d_obj || !d_rank || !d_cd) return fail(BRKGA_ERR_INVALID, "null argument");
     if (m != 2) return fail(BRKGA_ERR_UNSUPPORTED, "crowding kernel handles two objectives");
-    if (N < 0 || N > kMaxPool) return fail(BRKGA_ERR_UNSUPPORTED, "N outside [0, 8192]");
+    if (N < 0 || N > kMaxPool) return fail(BRKGA_ERR_UNSUPPORTED, "N outside [0, 4096]");
     if (N == 0) return BRKGA_OK;
     cudaError_t e;
-    if ((e = prep_select(N)) != cudaSuccess) return cuda_fail(e, "crowding set-up");
-    crowd2_op_kernel<<<1, kNsgaBlock, sel_smem_bytes(N), (cudaStream_t)stream>>>(d_obj, d_rank, N, d_cd);
+    if ((e = raise_smem_limit(reinterpret_cast<const void*>(crowd_op_kernel), sel_smem_bytes(N))) != cudaSuccess)
+        return cuda_fail(e, "crowding set-up");
+    crowd_op_kernel<<<1, kNsgaBlock, sel_smem_bytes(N), (cudaStream_t)stream>>>(d_obj, d_rank, N, d_cd);
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "crowding launch");
     return BRKGA_OK;
 }

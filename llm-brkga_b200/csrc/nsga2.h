@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cstdint>
+#include <vector>
 #include <cuda_runtime.h>
 
 #include "kernels.h"
@@ -11,26 +12,28 @@ namespace bk {
 struct Population;
 
 struct NsgaState {
-    PopDesc* dd = nullptr;   // device descriptor of the population
+    PopDesc* dd = nullptr;   // device descriptor of the population (buffers live in it)
     int P = 0, N = 0, n = 0, ld = 0, kind = 0, max_points = 0;
     RowTile tile{};
     int grid = 0;
     bool stage = false;
-    float* keys[2] = {nullptr, nullptr};  // [2P][ld] pools
-    float* fit[2] = {nullptr, nullptr};   // [2P][2]
-    int32_t* rank = nullptr;              // [2P]
-    float* cd = nullptr;                  // [2P]
-    int32_t* sel = nullptr;               // [P]
-    int32_t* d_nu = nullptr;              // diversity: unique count (P when no rebuild)
     float* history = nullptr;
     int hist_cap = 0;
-    int Mn = 0;
-    uint32_t mutT = 0;
     int div_interval = 0;
     bool ready = false;
 };
 
-int32_t nsga_setup(NsgaState& s, Population& pop, PopDesc* dd, const RowTile& tile, int grid, bool stage);
+int32_t nsga_setup(NsgaState& s, Population& pop, PopDesc* dd, PopDesc& hdesc, const RowTile& tile, int grid,
+                   bool stage);
+// allocate one population's NSGA-II buffers and fill its descriptor fields
+int32_t nsga_alloc(PopDesc& d, int P, double mut_rate, int div_interval, int Mn, std::vector<void*>& allocs,
+                   size_t* bytes);
+int nsga_max_population();
+cudaError_t nsga_prepare(int maxP);
+// group launches over `npops` consecutive NSGA-II descriptors
+cudaError_t nsga_enqueue_select(PopDesc* dd, int npops, int maxP, int mode, cudaStream_t st);
+cudaError_t nsga_enqueue_gather_finish(PopDesc* dd, int npops, int maxP, int maxld, cudaStream_t st);
+cudaError_t nsga_enqueue_diversity(PopDesc* dd, int npops, int maxP, cudaStream_t st);
 void nsga_release(NsgaState& s);
 void nsga_set_history(NsgaState& s, float* h, int cap);
 cudaError_t nsga_enqueue_init(NsgaState& s, cudaStream_t st);
