@@ -19,6 +19,8 @@ from __future__ import annotations
 
 import argparse
 import json
+
+import numpy as np
 import os
 import re
 import statistics
@@ -284,18 +286,26 @@ def run_ours(args, rank, world):
         perm = np.zeros(N_CITIES, np.int32)
         e2e_steps = max(1, min(args.steps, 5))
         times = []
+        phases = {"create_ms": 0.0, "run_ms": 0.0, "get_best_ms": 0.0, "destroy_ms": 0.0}
         for i in range(1 + e2e_steps):
             barrier()
             t0 = time.perf_counter()
             pe = B.tsp(xy_host, device=dev)
             se = B.Solver(pe, B.params(POP, ELITE, MUTANTS, RHO, E2E_GENERATIONS, seed=100 + i, device=dev))
+            t1 = time.perf_counter()
             se.run()
+            t2 = time.perf_counter()
             k2, p2, f2 = se.get_best_individual()
+            t3 = time.perf_counter()
             se.close()
             pe.close()
             barrier()
+            t4 = time.perf_counter()
             if i > 0:
-                times.append(time.perf_counter() - t0)
+                times.append(t4 - t0)
+                for key, dt in (("create_ms", t1 - t0), ("run_ms", t2 - t1), ("get_best_ms", t3 - t2),
+                                ("destroy_ms", t4 - t3)):
+                    phases[key] += 1e3 * dt / e2e_steps
         tt = sum(times)
         if dist is not None:
             t = torch.tensor([tt], device=dev, dtype=torch.float64)
@@ -304,7 +314,8 @@ def run_ours(args, rank, world):
         e2e = {"value": world * e2e_steps * E2E_GENERATIONS / tt, "unit": "gens/s",
                "h2d_bytes_per_step": int(xy.nbytes), "d2h_bytes_per_step": int(keys.nbytes + perm.nbytes + 4),
                "step": f"one {E2E_GENERATIONS}-generation solve through brkga_problem_create / brkga_create / "
-                       f"brkga_run / brkga_get_best", "ms_per_solve": 1e3 * tt / e2e_steps}
+                       f"brkga_run / brkga_get_best", "ms_per_solve": 1e3 * tt / e2e_steps,
+               "phases": {k: round(v, 3) for k, v in phases.items()}}
 
     peak, peak_kind = measured_peak()
     alg = algorithmic_bytes_per_generation()
@@ -325,6 +336,7 @@ def run_ours(args, rank, world):
                          "frac": achieved / peak, "traffic": profile_traffic(),
                          "kernel": "bk::row_kernel<256,1> (fused crossover/mutant/decode/tour length), "
                                    "timed through brkga_generation_step",
+                         "traffic_note": "DRAM bytes per launch from profiles/row_kernel_tsp_n1000_p2048.md",
                          "engine_tile": {"threads": s_info[0], "groups": s_info[1], "grid": s_info[2],
                                          "coords_in_smem": bool(s_info[3])},
                          "algorithmic_bytes_per_launch": alg, "kernel_ms": row_ms, "peak_kind": peak_kind,
@@ -339,6 +351,222 @@ def run_ours(args, rank, world):
         dist.barrier()
         dist.destroy_process_group()
     return out
+
+
+# ---------------------------------------------------------------------------------------
+# the other workloads (one JSON line each; the default run measures the headline only)
+# ---------------------------------------------------------------------------------------
+def _events_time(fn, stream=None):
+    import torch
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record(stream)
+    fn()
+    b.record(stream)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / 1e3
+
+
+def workload_solver(args, name, problem_fn, prm_kwargs, gens, cpu_kind=None, cpu_args=None):
+    """gens/s of one device-resident solver run (population resident, L2 warm between
+    generations because the whole run is one enqueue) and the reference's CPU path"""
+    import torch
+    import brkga_b200 as B
+    pb = problem_fn()
+    s = B.Solver(pb, B.params(**prm_kwargs))
+    s.initialize()
+    s.evolve(args.warmup)
+    s.synchronize()
+    stream = torch.cuda.ExternalStream(s.stream)
+    with torch.cuda.stream(stream):
+        torch.cuda._sleep(HOLD_CYCLES_PER_STEP)
+    secs = _events_time(lambda: s.evolve(gens), stream)
+    best = s.get_best_individual()[2]
+    out = {"metric": f"gens/s {name}", "value": gens / secs, "unit": "gens/s", "generations": gens,
+           "best": np.asarray(best, np.float64).tolist(), "workload": name,
+           "engine_tile": s.info}
+    if cpu_kind is not None and not args.no_cpu:
+        out["cpu_baseline"] = cpu_reference(cpu_kind, cpu_args, seconds=10.0)
+    return out
+
+
+def cpu_reference(kind, a, seconds=10.0, max_gens=2000):
+    """the reference's own Solver on its CPU path (oracle/_ref), generations per second"""
+    code = f"""
+import json, sys, time
+sys.path[:0] = [{os.path.join(ROOT, 'oracle')!r}]
+import numpy as np
+import oracle as O
+a = {a!r}
+xy = np.random.default_rng(a['seed']).random((a['pts'], 2), dtype=np.float32) * np.float32(a.get('scale', 1.0))
+xy2 = np.random.default_rng(a['seed'] + 1).random((a['pts'], 2), dtype=np.float32)
+if not O.ref_available():
+    print(json.dumps(dict(value=None))); sys.exit(0)
+R = O.ref()
+h = R.ref_solver_create({kind}, a['n'], xy.ctypes.data, xy2.ctypes.data, None, None, 0.0, a['P'], a['E'], a['M'], 0.7)
+R.ref_solver_evolve(h, 1)
+g, t = 0, 0.0
+while t < {seconds} and g < {max_gens}:
+    t += R.ref_solver_evolve(h, 1); g += 1
+print(json.dumps(dict(value=g / t, gens=g, seconds=t)))
+"""
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES="")
+    r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=900)
+    if r.returncode != 0:
+        return {"error": r.stderr[-500:]}
+    d = json.loads(r.stdout.strip().splitlines()[-1])
+    if d.get("value") is None:
+        return None
+    return {"value": d["value"], "unit": "gens/s", "cores": 1, "kind": "reference",
+            "sample": f"{d['gens']} generations ({d['seconds']:.1f} s) of the same workload"}
+
+
+def workload_batch(args):
+    """256 TSP instances, n ~ U[100,2000], P in {256,512,1024}, 4 islands migrating the 2
+    best every 50 generations, 500 generations, in one batch; against the same instances
+    solved one after another by the plain solver (timed on a sample)"""
+    import torch
+    import brkga_b200 as B
+    rng = np.random.default_rng(4)
+    count, gens = args.instances, args.generations
+    ns = rng.integers(100, 2001, count)
+    Ps = rng.choice([256, 512, 1024], count)
+    probs, prms = [], []
+    for i in range(count):
+        xy = np.random.default_rng(1000 + i).random((int(ns[i]), 2), dtype=np.float32)
+        P = int(Ps[i])
+        probs.append(B.tsp(xy))
+        prms.append(B.params(P, int(0.15 * P), int(0.15 * P), 0.7, gens, seed=2000 + i, num_islands=4,
+                             migration_interval=50, num_migrants=2))
+    t0 = time.perf_counter()
+    batch = B.Batch(probs, prms)
+    batch.synchronize()
+    t_create = time.perf_counter() - t0
+    secs = _events_time(lambda: (batch.evolve(gens), batch.synchronize()))
+    best_b = batch.best()[:, 0]
+    batch.close()
+    # plain solver, one instance at a time, on a sample of the same instances
+    sample = list(range(0, count, max(1, count // 16)))
+    tsum = 0.0
+    same = 0
+    for i in sample:
+        s = B.Solver(probs[i], prms[i])
+        t = _events_time(lambda: (s.run(), s.synchronize()))
+        tsum += t
+        same += int(s.get_best_individual()[2] == best_b[i])
+        s.close()
+    plain_per_instance = tsum / len(sample)
+    return {"metric": "instance-generations/s batched TSP islands", "value": count * gens / secs,
+            "unit": "instance-gens/s", "instances": count, "generations": gens, "seconds": secs,
+            "create_seconds": t_create, "plain_solver_instance_gens_per_s": gens / plain_per_instance,
+            "speedup_vs_plain": (count * gens / secs) / (gens / plain_per_instance),
+            "sample_results_identical_to_plain": f"{same}/{len(sample)}",
+            "elements_per_generation": int(sum(int(p) * int(n) for p, n in zip(Ps, ns)))}
+
+
+def workload_serve(args):
+    """Poisson arrivals: 50% TSP (n ~ U[50,5000], P 512), 30% greedy knapsack (n ~
+    U[500,10000], weights/values U{1..100}, capacity half the weight, P 1024), 20%
+    bi-objective TSP NSGA-II (n 300, P 512), 500 generations each"""
+    import brkga_b200 as B
+    rng = np.random.default_rng(5)
+    rate, dur, gens = args.rate, args.duration, args.generations
+    t, arrivals = 0.0, []
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t > dur:
+            break
+        arrivals.append(t)
+    reqs = []
+    for i, at in enumerate(arrivals):
+        u = rng.random()
+        if u < 0.5:
+            n = int(rng.integers(50, 5001))
+            reqs.append((at, dict(kind=B.TSP_COORDS, n=n, coords=rng.random((n, 2), dtype=np.float32)),
+                         B.params(512, 76, 76, 0.7, gens, seed=i)))
+        elif u < 0.8:
+            n = int(rng.integers(500, 10001))
+            w = rng.integers(1, 101, n).astype(np.int32)
+            v = rng.integers(1, 101, n).astype(np.int32)
+            reqs.append((at, dict(kind=B.KNAP_GREEDY, n=n, weights=w, values=v, capacity=0.5 * float(w.sum())),
+                         B.params(1024, 153, 153, 0.7, gens, seed=i)))
+        else:
+            n = 300
+            reqs.append((at, dict(kind=B.BITSP_COORDS, n=n, coords=rng.random((n + 1, 2), dtype=np.float32),
+                                  coords2=rng.random((n + 1, 2), dtype=np.float32)),
+                         B.params(512, 0, 51, 0.7, gens, seed=i)))
+    srv = B.Server(max_active=args.max_active, generations_per_tick=args.tick)
+    ids, k = [], 0
+    t0 = time.perf_counter()
+    done = {}
+    while len(done) < len(reqs):
+        now = time.perf_counter() - t0
+        while k < len(reqs) and reqs[k][0] <= now:
+            at, kw, prm = reqs[k]
+            ids.append(srv.submit(prm=prm, **kw))
+            k += 1
+        if k < len(reqs) and srv.stats()[1] == 0 and srv.stats()[0] == 0:
+            time.sleep(max(0.0, reqs[k][0] - (time.perf_counter() - t0)))
+            continue
+        srv.step()
+        for rid in ids:
+            if rid not in done:
+                r = srv.poll(rid)
+                if r is not None:
+                    done[rid] = r
+    makespan = time.perf_counter() - t0
+    lat = np.array([done[r][3] for r in ids])
+    srv.close()
+    # plain solver: one request at a time, alone on the GPU, on a sample
+    sample = list(range(0, len(reqs), max(1, len(reqs) // 24)))
+    tsum = 0.0
+    for i in sample:
+        _, kw, prm = reqs[i]
+        kw = dict(kw)
+        kind = kw.pop("kind")
+        n = kw.pop("n")
+        pb = B.Problem(kind, n, **kw)
+        t1 = time.perf_counter()
+        s = B.Solver(pb, prm)
+        s.run()
+        s.get_best_individual()
+        s.close()
+        tsum += time.perf_counter() - t1
+    plain = len(sample) / tsum
+    return {"metric": "served solves/s mixed stream", "value": len(reqs) / makespan, "unit": "solves/s",
+            "requests": len(reqs), "arrival_rate": rate, "arrival_seconds": dur, "makespan_s": makespan,
+            "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
+            "plain_solver_solves_per_s": plain, "speedup_vs_plain": (len(reqs) / makespan) / plain,
+            "generations": gens, "max_active": args.max_active, "tick": args.tick}
+
+
+def run_workload(args):
+    import torch
+    torch.cuda.init()
+    w = args.workload
+    if w == "tsp52":
+        # n=52 coordinates uniform [0,1000)^2 from seed 1, P 256, elite 0.20, mutants 0.10
+        xy = np.random.default_rng(1).random((52, 2), dtype=np.float32) * np.float32(1000)
+        import brkga_b200 as B
+        out = workload_solver(args, "TSP n=52 pop 256", lambda: B.tsp(xy),
+                              dict(population_size=256, elite_size=51, mutant_size=25, elite_prob=0.7,
+                                   max_generations=600, seed=1), 500, 1,
+                              dict(seed=1, pts=52, n=52, P=256, E=51, M=25, scale=1000.0))
+    elif w == "nsga":
+        import brkga_b200 as B
+        a = np.random.default_rng(3).random((501, 2), dtype=np.float32)
+        b = np.random.default_rng(4).random((501, 2), dtype=np.float32)
+        out = workload_solver(args, "NSGA-II bi-TSP n=500 pop 2048", lambda: B.bitsp(a, b),
+                              dict(population_size=2048, elite_size=0, mutant_size=204, elite_prob=0.7,
+                                   max_generations=600, seed=3), args.generations, 5,
+                              dict(seed=3, pts=501, n=500, P=2048, E=0, M=0))
+    elif w == "batch":
+        out = workload_batch(args)
+    elif w == "serve":
+        out = workload_serve(args)
+    else:
+        raise SystemExit(f"unknown workload {w}")
+    print(json.dumps(out))
 
 
 def profile_op(args):
@@ -374,9 +602,19 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--profile-op", action="store_true", help="operator kernels only (profiler captures)")
+    ap.add_argument("--workload", default="tsp1000", choices=["tsp1000", "tsp52", "nsga", "batch", "serve"])
+    ap.add_argument("--generations", type=int, default=500)
+    ap.add_argument("--instances", type=int, default=256)
+    ap.add_argument("--rate", type=float, default=200.0)
+    ap.add_argument("--duration", type=float, default=10.0)
+    ap.add_argument("--max-active", type=int, default=256)
+    ap.add_argument("--tick", type=int, default=25)
     args = ap.parse_args()
     if args.profile_op:
         profile_op(args)
+        return
+    if args.workload != "tsp1000":
+        run_workload(args)
         return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -375,3 +375,105 @@ class Instance:
     weights: np.ndarray = None
     values: np.ndarray = None
     capacity: float = 0.0
+
+
+# ---------------------------------------------------------------------------------------
+# batched solving and serving
+# ---------------------------------------------------------------------------------------
+class Batch:
+    """many independent instances advanced together (brkga_batch_*)"""
+
+    def __init__(self, problems, prms):
+        self.problems, self.prms = list(problems), list(prms)
+        arr = (C.c_void_p * len(problems))(*[p.h for p in problems])
+        parr = (Params * len(prms))(*prms)
+        h = C.c_void_p()
+        check(lib().brkga_batch_create(arr, parr, len(problems), C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().brkga_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def evolve(self, generations):
+        check(lib().brkga_batch_evolve(self.h, generations))
+
+    def synchronize(self):
+        check(lib().brkga_batch_synchronize(self.h))
+
+    def best(self):
+        out = np.zeros((len(self.problems), 2), np.float32)
+        check(lib().brkga_batch_get_best(self.h, _ptr(out)))
+        return out
+
+    def best_keys(self, index):
+        keys = np.zeros(self.problems[index].n, np.float32)
+        fit = np.zeros(2, np.float32)
+        check(lib().brkga_batch_get_best_keys(self.h, index, _ptr(keys), _ptr(fit)))
+        return keys, fit
+
+
+class Server:
+    """continuous batching of solve requests (brkga_server_*)"""
+
+    def __init__(self, device=0, max_active=256, memory_budget=0, generations_per_tick=25):
+        cfg = ServerConfig(device, max_active, memory_budget, generations_per_tick)
+        h = C.c_void_p()
+        check(lib().brkga_server_create(C.byref(cfg), C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().brkga_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, kind, n, prm, stall=0, coords=None, coords2=None, matrix=None, matrix2=None, weights=None,
+               values=None, capacity=0.0):
+        keep = []
+
+        def arr(a, dt):
+            if a is None:
+                return None
+            a = np.ascontiguousarray(a, dtype=dt)
+            keep.append(a)
+            return a.ctypes.data
+
+        d = ProblemDesc(kind, n, arr(coords, np.float32), arr(coords2, np.float32), arr(matrix, np.float32),
+                        arr(matrix2, np.float32), arr(weights, np.int32), arr(values, np.int32), float(capacity))
+        rid = C.c_int64()
+        check(lib().brkga_server_submit(self.h, C.byref(d), C.byref(prm), stall, C.byref(rid)))
+        return rid.value
+
+    def step(self):
+        check(lib().brkga_server_step(self.h))
+
+    def poll(self, rid):
+        """None while pending, else (status, best[2], generations, latency seconds)"""
+        best = np.zeros(2, np.float32)
+        gens = C.c_int32()
+        lat = C.c_double()
+        code = lib().brkga_server_poll(self.h, rid, _ptr(best), C.byref(gens), C.byref(lat))
+        if code == -8:
+            return None
+        return code, best, gens.value, lat.value
+
+    def cancel(self, rid):
+        check(lib().brkga_server_cancel(self.h, rid))
+
+    def stats(self):
+        q, a, f = C.c_int32(), C.c_int32(), C.c_int32()
+        check(lib().brkga_server_stats(self.h, C.byref(q), C.byref(a), C.byref(f)))
+        return q.value, a.value, f.value

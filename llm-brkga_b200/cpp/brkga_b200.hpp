@@ -1,0 +1,468 @@
+// brkga_b200.hpp -- drop-in C++ host interface with the reference's class names and
+// signatures (hsaseendran/llm-brkga: core/individual.hpp, core/config.hpp,
+// configs/tsp_config.hpp, configs/knapsack_config.hpp, configs/multi_tsp_config.hpp,
+// core/solver.hpp), running on the B200 engine through the C ABI (include/brkga_b200.h).
+//
+// A program written against the reference switches by including this header instead of
+// "core/solver.hpp" + "configs/*.hpp" and linking libbrkga_b200.so.  Errors the reference
+// prints and swallows are thrown here as std::runtime_error with the library's message.
+//
+// Scope: the problem configs the engine implements on the GPU (TSP from a matrix or from
+// TSPLIB coordinates, 0/1 knapsack, bi-objective TSP).  A config that only supplies a
+// host std::function fitness (no GPU kernel) is rejected by Solver, because the engine
+// has no host fitness path.
+#ifndef BRKGA_B200_HPP
+#define BRKGA_B200_HPP
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <fstream>
+#include <functional>
+#include <iomanip>
+#include <iostream>
+#include <limits>
+#include <memory>
+#include <random>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/brkga_b200.h"
+
+namespace brkga_b200_detail {
+inline void check(int32_t code, const char* what) {
+    if (code != BRKGA_OK) {
+        char buf[512];
+        brkga_last_error(buf, sizeof(buf));
+        throw std::runtime_error(std::string(what) + ": " + buf);
+    }
+}
+}  // namespace brkga_b200_detail
+
+// core/individual.hpp:9-226
+template <typename T>
+class Individual {
+public:
+    std::vector<std::vector<T>> chromosomes;
+    T fitness;
+    bool evaluated;
+    std::vector<T> objectives;
+    int rank;
+    T crowding_distance;
+
+    explicit Individual(int length = 0)
+        : chromosomes(1, std::vector<T>(length)), fitness(T(0)), evaluated(false), rank(-1), crowding_distance(0) {}
+    Individual(const std::vector<int>& lens, int num_objectives = 0)
+        : fitness(T(0)), evaluated(false), rank(-1), crowding_distance(0) {
+        for (int l : lens) chromosomes.emplace_back(l);
+        if (num_objectives > 0) objectives.assign(num_objectives, T(0));
+    }
+    std::vector<T>& get_chromosome() { return chromosomes[0]; }
+    const std::vector<T>& get_chromosome() const { return chromosomes[0]; }
+    std::vector<T>& chromosome() { return chromosomes[0]; }
+    const std::vector<T>& chromosome() const { return chromosomes[0]; }
+    std::vector<T>& get_component(int i) { return chromosomes[i]; }
+    const std::vector<T>& get_component(int i) const { return chromosomes[i]; }
+    int size() const { return chromosomes.empty() ? 0 : (int)chromosomes[0].size(); }
+    int num_components() const { return (int)chromosomes.size(); }
+    T get_fitness() const { return fitness; }
+    bool is_evaluated() const { return evaluated; }
+    bool is_multi_objective() const { return !objectives.empty(); }
+    T& operator[](int i) { return chromosomes[0][i]; }
+    const T& operator[](int i) const { return chromosomes[0][i]; }
+    // minimisation dominance, core/individual.hpp:99-114
+    bool dominates(const Individual& o) const {
+        if (objectives.empty() || objectives.size() != o.objectives.size()) return false;
+        bool better = false;
+        for (size_t i = 0; i < objectives.size(); ++i) {
+            if (objectives[i] > o.objectives[i]) return false;
+            if (objectives[i] < o.objectives[i]) better = true;
+        }
+        return better;
+    }
+    std::vector<T> flatten() const {
+        std::vector<T> f;
+        for (const auto& c : chromosomes) f.insert(f.end(), c.begin(), c.end());
+        return f;
+    }
+};
+
+// core/config.hpp:14-229
+template <typename T>
+class BRKGAConfig {
+public:
+    std::vector<int> component_lengths;
+    int num_components;
+    int population_size;
+    int elite_size;
+    int mutant_size;
+    double elite_prob;
+    int max_generations;
+    int threads_per_block;
+    int blocks_per_grid;
+    std::function<T(const Individual<T>&)> fitness_function;
+    std::function<std::vector<std::vector<T>>(const Individual<T>&)> decoder;
+    std::function<bool(T, T)> comparator;
+    int num_objectives;
+    std::vector<std::function<T(const Individual<T>&)>> objective_functions;
+    // engine extras (not in the reference): Philox seed, islands, device
+    uint64_t seed = 1;
+    int num_islands = 1;
+    int migration_interval = 0;
+    int num_migrants = 0;
+    int device = 0;
+
+    explicit BRKGAConfig(int chrom_len) : BRKGAConfig(std::vector<int>{chrom_len}) {}
+    explicit BRKGAConfig(const std::vector<int>& lens, int n_objectives = 1)
+        : component_lengths(lens), num_components((int)lens.size()), population_size(100), elite_size(20),
+          mutant_size(10), elite_prob(0.7), max_generations(1000), threads_per_block(256), blocks_per_grid(32),
+          num_objectives(n_objectives) {
+        objective_functions.resize(n_objectives > 1 ? n_objectives : 0);
+    }
+    virtual ~BRKGAConfig() = default;
+
+    // the device instance this config evaluates on (nullptr: no GPU evaluation)
+    virtual brkga_problem* problem_handle() { return nullptr; }
+
+    virtual bool has_gpu_evaluation() const { return false; }
+    // core/config.hpp:50-53: d_population [pop_size][chrom_len], d_fitness [pop_size]
+    virtual void evaluate_population_gpu(T* d_population, T* d_fitness, int pop_size, int chrom_len) {
+        brkga_problem* pb = problem_handle();
+        if (!pb) return;
+        brkga_b200_detail::check(
+            brkga_evaluate_population_sync(pb, d_population, d_fitness, pop_size, chrom_len), "evaluate_population_gpu");
+    }
+    virtual bool has_local_search() const { return false; }
+    virtual void print_solution(const Individual<T>& ind) {
+        std::cout << "Best fitness: " << ind.fitness << std::endl;
+    }
+    virtual bool validate_solution(const Individual<T>&) { return true; }
+    // core/config.hpp:159-179
+    virtual bool is_valid() const {
+        bool ok = !component_lengths.empty() &&
+                  std::all_of(component_lengths.begin(), component_lengths.end(), [](int l) { return l > 0; }) &&
+                  population_size > 0 && elite_prob >= 0.0 && elite_prob <= 1.0 && max_generations > 0 &&
+                  num_objectives > 0;
+        if (!ok) return false;
+        if (num_objectives == 1) return elite_size > 0 && mutant_size >= 0 && elite_size + mutant_size <= population_size;
+        return true;
+    }
+    int get_total_chromosome_length() const {
+        int t = 0;
+        for (int l : component_lengths) t += l;
+        return t;
+    }
+    int chromosome_length() const { return get_total_chromosome_length(); }
+    int get_offspring_size() const { return population_size - elite_size - mutant_size; }
+    void update_cuda_grid_size() { blocks_per_grid = (population_size + threads_per_block - 1) / threads_per_block; }
+    bool is_multi_objective() const { return num_objectives > 1; }
+};
+
+// a config backed by a device instance
+template <typename T>
+class DeviceProblemConfig : public BRKGAConfig<T> {
+public:
+    using BRKGAConfig<T>::BRKGAConfig;
+    ~DeviceProblemConfig() override {
+        if (pb_) brkga_problem_destroy(pb_);
+    }
+    brkga_problem* problem_handle() override { return pb_; }
+    bool has_gpu_evaluation() const override { return pb_ != nullptr; }
+
+protected:
+    void create(const brkga_problem_desc& d) {
+        brkga_b200_detail::check(brkga_problem_create(&d, this->device, &pb_), "problem upload");
+    }
+    brkga_problem* pb_ = nullptr;
+};
+
+// configs/tsp_config.hpp:24-381
+template <typename T>
+class TSPConfig : public DeviceProblemConfig<T> {
+public:
+    // TSPConfig(distances, name): explicit N x N matrix
+    TSPConfig(const std::vector<std::vector<T>>& distances, const std::string& name = "TSP")
+        : DeviceProblemConfig<T>((int)distances.size()), num_cities_((int)distances.size()), name_(name) {
+        std::vector<float> flat((size_t)num_cities_ * num_cities_);
+        for (int i = 0; i < num_cities_; ++i)
+            for (int j = 0; j < num_cities_; ++j) flat[(size_t)i * num_cities_ + j] = (float)distances[i][j];
+        brkga_problem_desc d{};
+        d.kind = BRKGA_TSP_MATRIX;
+        d.n = num_cities_;
+        d.matrix = flat.data();
+        this->create(d);
+        setup();
+    }
+    // engine-native: Euclidean distances from [n][2] coordinates, computed on the device
+    // exactly as the reference builds its matrix (configs/tsp_config.hpp:361-370)
+    static std::unique_ptr<TSPConfig<T>> from_coordinates(const std::vector<std::pair<T, T>>& xy,
+                                                          const std::string& name = "TSP") {
+        return std::unique_ptr<TSPConfig<T>>(new TSPConfig<T>(xy, name, 0));
+    }
+    // configs/tsp_config.hpp:260-265, 301-380 (TSPLIB NODE_COORD_SECTION)
+    static std::unique_ptr<TSPConfig<T>> load_from_file(const std::string& filename) {
+        std::ifstream f(filename);
+        if (!f) throw std::runtime_error("File does not exist: " + filename);
+        std::string line, name;
+        int n = 0;
+        bool reading = false;
+        std::vector<std::pair<T, T>> xy;
+        while (std::getline(f, line)) {
+            if (line.empty()) continue;
+            if (line.find("NAME") != std::string::npos && line.find(':') != std::string::npos) {
+                name = line.substr(line.find(':') + 1);
+                name.erase(0, name.find_first_not_of(" \t"));
+                name.erase(name.find_last_not_of(" \t\r") + 1);
+            } else if (line.find("DIMENSION") != std::string::npos) {
+                std::istringstream is(line);
+                std::string tok;
+                while (is >> tok)
+                    if (std::isdigit((unsigned char)tok[0])) {
+                        n = std::stoi(tok);
+                        break;
+                    }
+                xy.assign(n, {T(0), T(0)});
+            } else if (line.find("NODE_COORD_SECTION") != std::string::npos) {
+                reading = true;
+            } else if (line.find("EOF") != std::string::npos) {
+                break;
+            } else if (reading) {
+                std::istringstream is(line);
+                int id;
+                T x, y;
+                if (is >> id >> x >> y && id > 0 && id <= n) xy[id - 1] = {x, y};
+            }
+        }
+        if (xy.empty()) throw std::runtime_error("No coordinates found in TSPLIB file");
+        if (name.empty()) name = filename;
+        return from_coordinates(xy, name);
+    }
+    // configs/tsp_config.hpp:267-286
+    static void configure_for_size(TSPConfig<T>* c, int n) {
+        if (n <= 20) {
+            c->population_size = 200, c->elite_size = 40, c->mutant_size = 20, c->max_generations = 100;
+        } else if (n <= 50) {
+            c->population_size = 1000, c->elite_size = 800, c->mutant_size = 400, c->max_generations = 2000;
+        } else {
+            c->population_size = 8000, c->elite_size = 1600, c->mutant_size = 800, c->max_generations = 5000;
+        }
+        c->elite_prob = 0.7;
+        c->update_cuda_grid_size();
+    }
+    int get_num_cities() const { return num_cities_; }
+    const std::string& get_instance_name() const { return name_; }
+    bool is_gpu_available() const { return this->pb_ != nullptr; }
+
+private:
+    TSPConfig(const std::vector<std::pair<T, T>>& xy, const std::string& name, int)
+        : DeviceProblemConfig<T>((int)xy.size()), num_cities_((int)xy.size()), name_(name) {
+        std::vector<float> flat(2 * xy.size());
+        for (size_t i = 0; i < xy.size(); ++i) {
+            flat[2 * i] = (float)xy[i].first;
+            flat[2 * i + 1] = (float)xy[i].second;
+        }
+        brkga_problem_desc d{};
+        d.kind = BRKGA_TSP_COORDS;
+        d.n = num_cities_;
+        d.coords = flat.data();
+        this->create(d);
+        setup();
+    }
+    void setup() {
+        this->comparator = [](T a, T b) { return a < b; };
+        this->update_cuda_grid_size();
+    }
+    int num_cities_;
+    std::string name_;
+};
+
+// configs/knapsack_config.hpp:11-62 (threshold decode, penalty x1000, maximise); greedy
+// key-order decoding is the engine's addition (greedy = true)
+template <typename T>
+class KnapsackConfig : public DeviceProblemConfig<T> {
+public:
+    KnapsackConfig(const std::vector<T>& w, const std::vector<T>& v, T cap, const std::string& name = "Knapsack",
+                   bool greedy = false)
+        : DeviceProblemConfig<T>((int)w.size()), weights_(w), values_(v), capacity_(cap), name_(name) {
+        if (w.size() != v.size()) throw std::invalid_argument("Weights and values must have same size");
+        std::vector<int32_t> wi(w.size()), vi(v.size());
+        for (size_t i = 0; i < w.size(); ++i) {
+            if (w[i] != std::floor(w[i]) || v[i] != std::floor(v[i]))
+                throw std::invalid_argument("the GPU knapsack takes integer weights and values");
+            wi[i] = (int32_t)w[i];
+            vi[i] = (int32_t)v[i];
+        }
+        brkga_problem_desc d{};
+        d.kind = greedy ? BRKGA_KNAP_GREEDY : BRKGA_KNAP_THRESHOLD;
+        d.n = (int)w.size();
+        d.weights = wi.data();
+        d.values = vi.data();
+        d.capacity = (float)cap;
+        this->create(d);
+        this->comparator = [](T a, T b) { return a > b; };
+        this->update_cuda_grid_size();
+    }
+    // configs/knapsack_config.hpp:307-331
+    static void configure_for_size(KnapsackConfig<T>* c, int n) {
+        if (n <= 50) {
+            c->population_size = 200, c->elite_size = 40, c->mutant_size = 20, c->max_generations = 300;
+        } else if (n <= 100) {
+            c->population_size = 400, c->elite_size = 80, c->mutant_size = 40, c->max_generations = 500;
+        } else if (n <= 500) {
+            c->population_size = 800, c->elite_size = 160, c->mutant_size = 80, c->max_generations = 1000;
+        } else {
+            c->population_size = 1200, c->elite_size = 240, c->mutant_size = 120, c->max_generations = 1500;
+        }
+        c->elite_prob = 0.7;
+        c->update_cuda_grid_size();
+    }
+    const std::vector<T>& get_weights() const { return weights_; }
+    const std::vector<T>& get_values() const { return values_; }
+    T get_capacity() const { return capacity_; }
+
+private:
+    std::vector<T> weights_, values_;
+    T capacity_;
+    std::string name_;
+};
+
+// configs/multi_tsp_config.hpp:16-296 (depot 0, two objectives)
+template <typename T>
+class MultiTSPConfig : public DeviceProblemConfig<T> {
+public:
+    MultiTSPConfig(const std::vector<std::vector<T>>& distances, const std::vector<std::vector<T>>& times,
+                   const std::string& name = "MultiTSP")
+        : DeviceProblemConfig<T>(std::vector<int>{(int)distances.size() - 1}, 2), name_(name) {
+        const int dim = (int)distances.size();
+        std::vector<float> a((size_t)dim * dim), b((size_t)dim * dim);
+        for (int i = 0; i < dim; ++i)
+            for (int j = 0; j < dim; ++j) {
+                a[(size_t)i * dim + j] = (float)distances[i][j];
+                b[(size_t)i * dim + j] = (float)times[i][j];
+            }
+        brkga_problem_desc d{};
+        d.kind = BRKGA_BITSP_MATRIX;
+        d.n = dim - 1;
+        d.matrix = a.data();
+        d.matrix2 = b.data();
+        this->create(d);
+        // core/config.hpp defaults as MultiTSPConfig sets them (multi_tsp_config.hpp:34-39)
+        this->population_size = 100;
+        this->elite_size = 0;
+        this->mutant_size = 0;
+        this->max_generations = 500;
+        this->elite_prob = 0.7;
+        this->update_cuda_grid_size();
+    }
+    int get_num_cities() const { return this->component_lengths[0]; }
+
+private:
+    std::string name_;
+};
+
+// core/solver.hpp:44-1726: device-resident population, one CUDA graph per chunk of
+// generations; run / initialize / evolve_generation / get_best_individual /
+// get_pareto_front / get_fitness_history / get_config / export_pareto_front
+template <typename T>
+class Solver {
+public:
+    Solver(std::unique_ptr<BRKGAConfig<T>> cfg, bool verbose = true, int print_freq = 50)
+        : config_(std::move(cfg)), verbose_(verbose), print_freq_(print_freq) {
+        if (!config_->is_valid()) throw std::runtime_error("Invalid configuration");
+        brkga_problem* pb = config_->problem_handle();
+        if (!pb) throw std::runtime_error("this config has no device problem; the engine has no host fitness path");
+        brkga_params p;
+        brkga_params_default(&p);
+        p.population_size = config_->population_size;
+        p.elite_size = config_->elite_size;
+        p.mutant_size = config_->mutant_size;
+        p.elite_prob = config_->elite_prob;
+        p.max_generations = config_->max_generations;
+        p.seed = config_->seed;
+        p.num_islands = config_->num_islands;
+        p.migration_interval = config_->migration_interval;
+        p.num_migrants = config_->num_migrants;
+        p.device = config_->device;
+        brkga_b200_detail::check(brkga_create(pb, &p, &e_), "Solver");
+        n_ = config_->get_total_chromosome_length();
+        best_ = Individual<T>(config_->component_lengths, config_->num_objectives > 1 ? config_->num_objectives : 0);
+    }
+    ~Solver() {
+        if (e_) brkga_destroy(e_);
+    }
+    Solver(const Solver&) = delete;
+    Solver& operator=(const Solver&) = delete;
+
+    void initialize() { brkga_b200_detail::check(brkga_initialize(e_), "initialize"); }
+    void evolve_generation() { brkga_b200_detail::check(brkga_evolve(e_, 1), "evolve_generation"); }
+    void evolve(int generations) { brkga_b200_detail::check(brkga_evolve(e_, generations), "evolve"); }
+    void run() {
+        brkga_b200_detail::check(brkga_run(e_), "run");
+        if (verbose_) {
+            const auto& b = get_best_individual();
+            std::cout << "Evolution completed: " << brkga_generation(e_) << " generations, best fitness "
+                      << std::setprecision(6) << b.fitness << std::endl;
+        }
+    }
+    const Individual<T>& get_best_individual() {
+        std::vector<float> k(n_), f(2);
+        brkga_b200_detail::check(brkga_get_best(e_, k.data(), nullptr, f.data()), "get_best_individual");
+        best_.chromosomes[0].assign(k.begin(), k.end());
+        best_.fitness = f[0];
+        if (config_->num_objectives > 1) best_.objectives = {(T)f[0], (T)f[1]};
+        best_.evaluated = true;
+        return best_;
+    }
+    // the decoded tour / selection order of the best individual
+    std::vector<int> get_best_permutation() {
+        std::vector<int32_t> p(n_);
+        brkga_b200_detail::check(brkga_get_best(e_, nullptr, p.data(), nullptr), "get_best_permutation");
+        return std::vector<int>(p.begin(), p.end());
+    }
+    std::vector<Individual<T>> get_pareto_front() {
+        std::vector<Individual<T>> out;
+        if (config_->num_objectives < 2) return out;
+        const int cap = config_->population_size;
+        std::vector<float> obj((size_t)cap * 2), keys((size_t)cap * n_);
+        int32_t cnt = 0;
+        brkga_b200_detail::check(brkga_get_pareto_front(e_, obj.data(), keys.data(), cap, &cnt), "get_pareto_front");
+        for (int i = 0; i < std::min<int>(cnt, cap); ++i) {
+            Individual<T> ind(config_->component_lengths, 2);
+            ind.chromosomes[0].assign(keys.begin() + (size_t)i * n_, keys.begin() + (size_t)(i + 1) * n_);
+            ind.objectives = {(T)obj[2 * i], (T)obj[2 * i + 1]};
+            ind.fitness = ind.objectives[0];
+            ind.rank = 0;
+            ind.evaluated = true;
+            out.push_back(ind);
+        }
+        return out;
+    }
+    const std::vector<T>& get_fitness_history() {
+        const int len = brkga_generation(e_) + 1;
+        std::vector<float> h(len);
+        int32_t got = 0;
+        brkga_b200_detail::check(brkga_get_fitness_history(e_, h.data(), len, &got), "get_fitness_history");
+        history_.assign(h.begin(), h.begin() + got);
+        return history_;
+    }
+    BRKGAConfig<T>* get_config() { return config_.get(); }
+    void export_pareto_front(const std::string& filename) {
+        auto front = get_pareto_front();
+        std::ofstream f(filename);
+        f << "# Pareto Front\n# Objectives: " << config_->num_objectives << "\n# Solutions: " << front.size() << "\n";
+        for (const auto& ind : front) f << ind.objectives[0] << " " << ind.objectives[1] << "\n";
+    }
+
+private:
+    std::unique_ptr<BRKGAConfig<T>> config_;
+    bool verbose_;
+    int print_freq_;
+    brkga_engine* e_ = nullptr;
+    int n_ = 0;
+    Individual<T> best_;
+    std::vector<T> history_;
+};
+
+#endif  // BRKGA_B200_HPP

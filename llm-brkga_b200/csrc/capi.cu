@@ -43,15 +43,15 @@ DeviceGuard::~DeviceGuard() { cudaSetDevice(prev_); }
 // ---------------------------------------------------------------------------------------
 ProblemData::~ProblemData() {
     DeviceGuard g(device);
-    for (void* p : allocs) cudaFree(p);
+    for (void* p : allocs) dev_free(p, nullptr);
 }
 
 static int32_t upload(ProblemData& pd, const void* host, size_t bytes, void** dev) {
     if (!host) return fail(BRKGA_ERR_INVALID, "missing instance array");
-    cudaError_t e = cudaMalloc(dev, bytes ? bytes : 4);
-    if (e != cudaSuccess) return fail(BRKGA_ERR_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    int32_t st = dev_alloc(dev, bytes ? bytes : 4, nullptr);
+    if (st != BRKGA_OK) return st;
     pd.allocs.push_back(*dev);
-    e = cudaMemcpy(*dev, host, bytes, cudaMemcpyHostToDevice);
+    cudaError_t e = cudaMemcpy(*dev, host, bytes, cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpy instance");
     pd.bytes += bytes;
     return BRKGA_OK;

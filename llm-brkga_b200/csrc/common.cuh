@@ -118,7 +118,13 @@ struct PopDesc {
     uint32_t* domS;           // [2P][domW] dominance rows
     int32_t* domcnt;          // [2P] domination counts
     int32_t* nu;              // diversity pass: unique count, P when nothing was rebuilt
+    // shared launches: a population whose generation has reached gen_limit (> 0) is left
+    // unchanged by every kernel; `advanced` records whether the last generation ran
+    uint32_t gen_limit;
+    int32_t advanced;
 };
+
+__host__ __device__ __forceinline__ bool at_limit(const PopDesc& d) { return d.gen_limit != 0u && d.gen >= d.gen_limit; }
 
 // ---------------------------------------------------------------------------------------
 // block collectives

@@ -53,8 +53,8 @@ int32_t make_shape(const ProblemData& pd, const brkga_params& p, Shape* s) {
 }
 
 static int32_t dalloc(Population& p, void** ptr, size_t bytes) {
-    cudaError_t e = cudaMalloc(ptr, bytes ? bytes : 16);
-    if (e != cudaSuccess) return fail(BRKGA_ERR_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    int32_t st = dev_alloc(ptr, bytes ? bytes : 16, p.stream);
+    if (st != BRKGA_OK) return st;
     p.allocs.push_back(*ptr);
     p.bytes += bytes;
     return BRKGA_OK;
@@ -69,7 +69,7 @@ int32_t Population::allocate(int device) {
     for (int b = 0; b < 2; ++b) {
         if ((st = dalloc(*this, &p, (size_t)rows * sh.ld * 4)) != BRKGA_OK) return st;
         keys[b] = (float*)p;
-        cudaMemset(p, 0, (size_t)rows * sh.ld * 4);
+        cudaMemsetAsync(p, 0, (size_t)rows * sh.ld * 4, stream);
         if ((st = dalloc(*this, &p, (size_t)rows * sh.m * 4)) != BRKGA_OK) return st;
         fit[b] = (float*)p;
     }
@@ -79,7 +79,7 @@ int32_t Population::allocate(int device) {
     parents = (int2*)p;
     if ((st = dalloc(*this, &p, (size_t)sh.k * 4)) != BRKGA_OK) return st;
     done = (int32_t*)p;
-    cudaMemset(done, 0, (size_t)sh.k * 4);
+    cudaMemsetAsync(done, 0, (size_t)sh.k * 4, stream);
     if ((st = dalloc(*this, &p, (size_t)sh.k * hist_cap * 4)) != BRKGA_OK) return st;
     history = (float*)p;
     return BRKGA_OK;
@@ -87,7 +87,7 @@ int32_t Population::allocate(int device) {
 
 void Population::release(int device) {
     DeviceGuard g(device);
-    for (void* a : allocs) cudaFree(a);
+    for (void* a : allocs) dev_free(a, stream);
     allocs.clear();
 }
 
@@ -189,6 +189,7 @@ static int32_t grow_history(brkga_engine* e, int need) {
     while (cap < need) cap *= 2;
     void* nh = nullptr;
     if ((st = dalloc(p, &nh, (size_t)p.sh.k * cap * 4)) != BRKGA_OK) return st;
+    cudaStreamSynchronize(e->stream);
     for (int i = 0; i < p.sh.k; ++i) {
         cudaError_t err = cudaMemcpy((float*)nh + (size_t)i * cap, p.history + (size_t)i * p.hist_cap,
                                      (size_t)p.hist_cap * 4, cudaMemcpyDeviceToDevice);
@@ -239,6 +240,7 @@ int32_t brkga_create(brkga_problem* pbh, const brkga_params* params, brkga_engin
         delete e;
         return cuda_fail(err, "stream");
     }
+    e->pop.stream = e->stream;
     if ((st = e->pop.allocate(e->device)) != BRKGA_OK) {
         destroy_engine(e);
         return st;
@@ -279,7 +281,10 @@ int32_t brkga_create(brkga_problem* pbh, const brkga_params* params, brkga_engin
         d.cur = 0;
         d.gen = 0;
     }
-    err = cudaMemcpy(e->dd, e->hd.data(), sizeof(PopDesc) * sh.k, cudaMemcpyHostToDevice);
+    // pool allocations and clears are ordered on the engine stream: complete them before
+    // the synchronous uploads below touch the memory
+    err = cudaStreamSynchronize(e->stream);
+    if (err == cudaSuccess) err = cudaMemcpy(e->dd, e->hd.data(), sizeof(PopDesc) * sh.k, cudaMemcpyHostToDevice);
     if (err != cudaSuccess) {
         destroy_engine(e);
         return cuda_fail(err, "descriptor upload");

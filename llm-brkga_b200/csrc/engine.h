@@ -18,6 +18,10 @@ constexpr size_t kMaxSmem = 227 * 1024;  // opt-in dynamic shared memory per CTA
 constexpr int kMaxPop = 16384;           // largest population the in-shared-memory sort handles
 
 int32_t fail(int32_t code, const std::string& msg);
+// stream-ordered device memory from the library's pool (memory.cu)
+int32_t dev_alloc(void** p, size_t bytes, cudaStream_t st);
+void dev_free(void* p, cudaStream_t st);
+size_t pool_reserved(int dev);
 int32_t cuda_fail(cudaError_t e, const char* what);
 
 class DeviceGuard {
@@ -103,6 +107,8 @@ struct Population {
     float* nsga_hist = nullptr;
     std::vector<void*> allocs;
     size_t bytes = 0;
+    cudaStream_t stream = nullptr;  // allocations are ordered on the owner's stream
+    std::vector<PopDesc> hd_template;  // descriptors (live state copied back before plan rebuilds)
     int32_t allocate(int device);
     void release(int device);
 };
@@ -116,23 +122,35 @@ int32_t autotune_tile(int kind, int n, int pts, int rows, cudaStream_t stream, F
     cudaEvent_t a, b;
     cudaEventCreate(&a);
     cudaEventCreate(&b);
-    float best_ms = 1e30f;
-    TunedTile best;
+    // each candidate: one warm-up, then the best of three separately timed launches; the
+    // default tile (smallest that covers n) is kept unless another is 5% faster
+    const RowTile def = pick_tile(n);
+    float best_ms = 1e30f, def_ms = 1e30f;
+    TunedTile best, deft;
     for (int c = 0; c < nc; ++c) {
         TunedTile tt;
         if (tile_setup(cand[c], kind, n, pts, &tt) != BRKGA_OK) continue;
         if (launch(tt) != cudaSuccess) continue;  // warm-up
-        cudaEventRecord(a, stream);
-        for (int r = 0; r < 3; ++r) launch(tt);
-        cudaEventRecord(b, stream);
-        if (cudaEventSynchronize(b) != cudaSuccess) continue;
-        float ms = 0.0f;
-        cudaEventElapsedTime(&ms, a, b);
+        float ms = 1e30f;
+        for (int r = 0; r < 3; ++r) {
+            cudaEventRecord(a, stream);
+            launch(tt);
+            cudaEventRecord(b, stream);
+            if (cudaEventSynchronize(b) != cudaSuccess) break;
+            float x = 0.0f;
+            cudaEventElapsedTime(&x, a, b);
+            ms = x < ms ? x : ms;
+        }
         if (ms < best_ms) {
             best_ms = ms;
             best = tt;
         }
+        if (cand[c].block == def.block && cand[c].groups == def.groups) {
+            def_ms = ms;
+            deft = tt;
+        }
     }
+    if (deft.grid > 0 && best_ms > 0.95f * def_ms) best = deft;
     cudaEventDestroy(a);
     cudaEventDestroy(b);
     cudaGetLastError();

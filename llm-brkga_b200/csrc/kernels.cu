@@ -348,6 +348,8 @@ __global__ void __launch_bounds__(BLOCK, RowResidency<BLOCK, G>::value) row_kern
         }
         const int n = sd.n, ld = sd.ld, P = sd.P, E = sd.E, M = sd.M, m = sd.m;
         const int cur = sd.cur;
+        if ((L.mode == MODE_GEN || L.mode == MODE_NSGA_OFF) && at_limit(sd)) continue;
+        if (L.mode == MODE_NSGA_REFILL && !sd.advanced) continue;
         if (!L.tasks && L.mode == MODE_GEN) r = (task < P - E) ? E + task : task - (P - E);
 
         float k[G][4];
@@ -607,6 +609,7 @@ __global__ void __launch_bounds__(RK_THREADS) rank_kernel(RankArgs a) {
     int32_t* sorted;
     uint32_t gen_new = 0;
     if (d) {
+        if (a.flip && at_limit(*d)) return;
         P = d->P;
         mx = d->maximize;
         m = d->m;

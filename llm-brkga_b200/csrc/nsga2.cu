@@ -88,7 +88,8 @@ __global__ void dom_build_kernel(DomArgs a) {
     int32_t* cnt;
     if (a.dd) {
         const PopDesc& d = a.dd[blockIdx.y];
-        if (a.only_rebuilt && __ldg(d.nu) >= d.P) return;
+        if (a.pool && at_limit(d)) return;
+        if (a.only_rebuilt && (!d.advanced || __ldg(d.nu) >= d.P)) return;
         N = a.pool ? 2 * d.P : d.P;
         m = d.m;
         obj = d.fit[d.cur];
@@ -448,7 +449,8 @@ __global__ void __launch_bounds__(kNsgaBlock) nsga_select_kernel(PopDesc* dd, in
     PopDesc& d = dd[blockIdx.x];
     const int t = threadIdx.x;
     const int P = d.P;
-    if (mode == 2 && __ldg(d.nu) >= P) return;
+    if (mode == 0 && at_limit(d)) return;
+    if (mode == 2 && (!d.advanced || __ldg(d.nu) >= P)) return;
     const int N = (mode == 0) ? 2 * P : P;
     const float* f = d.fit[d.cur];
     const SelSmem s = sel_carve(smem, N);
@@ -500,6 +502,7 @@ __global__ void __launch_bounds__(kNsgaBlock) crowd_op_kernel(const float* obj, 
 // survivors -> the other pool buffer, rows [0, P); population blockIdx.y
 __global__ void nsga_gather_kernel(PopDesc* dd) {
     const PopDesc& d = dd[blockIdx.y];
+    if (at_limit(d)) return;
     const int P = d.P, ld4 = d.ld / 4, m = d.m;
     const float4* src = reinterpret_cast<const float4*>(d.keys[d.cur]);
     float4* dst = reinterpret_cast<float4*>(d.keys[d.cur ^ 1]);
@@ -519,8 +522,13 @@ __global__ void nsga_gather_kernel(PopDesc* dd) {
 __global__ void nsga_finish_kernel(PopDesc* dd, int npops) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p < npops) {
+        if (at_limit(dd[p])) {
+            dd[p].advanced = 0;
+            return;
+        }
         dd[p].cur ^= 1;
         dd[p].gen += 1;
+        dd[p].advanced = 1;
     }
 }
 
@@ -534,7 +542,7 @@ __global__ void __launch_bounds__(kNsgaBlock) nsga_diversity_kernel(PopDesc* dd)
     PopDesc& d = dd[blockIdx.x];
     const int t = threadIdx.x, P = d.P, interval = d.div_interval;
     const uint32_t g = d.gen;
-    if (interval <= 0 || g < 1 || ((g - 1) % (uint32_t)interval) != 0) {
+    if (!d.advanced || interval <= 0 || g < 1 || ((g - 1) % (uint32_t)interval) != 0) {
         if (t == 0) *d.nu = P;
         return;
     }
@@ -627,12 +635,12 @@ cudaError_t nsga_enqueue_diversity(PopDesc* dd, int npops, int maxP, cudaStream_
 }
 
 int32_t nsga_alloc(PopDesc& d, int P, double mut_rate, int div_interval, int Mn, std::vector<void*>& allocs,
-                   size_t* bytes) {
+                   size_t* bytes, cudaStream_t stream) {
     const int N = 2 * P;
     const int W = (N + 31) / 32;
     auto get = [&](size_t b, void** p) -> int32_t {
-        cudaError_t e = cudaMalloc(p, b ? b : 16);
-        if (e != cudaSuccess) return fail(BRKGA_ERR_OOM, "cudaMalloc (NSGA-II state)");
+        int32_t rc = dev_alloc(p, b ? b : 16, stream);
+        if (rc != BRKGA_OK) return rc;
         allocs.push_back(*p);
         *bytes += b;
         return BRKGA_OK;
@@ -673,10 +681,12 @@ int32_t nsga_setup(NsgaState& s, Population& pop, PopDesc* dd, PopDesc& hdesc, c
     s.grid = grid;
     s.stage = stage;
     const double rate = (pop.prm.mutation_rate > 0.0) ? pop.prm.mutation_rate : 5.0 / (double)pop.sh.n;
-    int32_t st = nsga_alloc(hdesc, s.P, rate, pop.prm.diversity_interval, pop.sh.Mn, pop.allocs, &pop.bytes);
+    int32_t st = nsga_alloc(hdesc, s.P, rate, pop.prm.diversity_interval, pop.sh.Mn, pop.allocs, &pop.bytes,
+                            pop.stream);
     if (st != BRKGA_OK) return st;
     s.div_interval = pop.prm.diversity_interval;
-    cudaError_t e = cudaMemcpy(dd, &hdesc, sizeof(PopDesc), cudaMemcpyHostToDevice);
+    cudaError_t e = cudaStreamSynchronize(pop.stream);
+    if (e == cudaSuccess) e = cudaMemcpy(dd, &hdesc, sizeof(PopDesc), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return cuda_fail(e, "descriptor upload");
     e = nsga_prepare(s.P);
     if (e != cudaSuccess) return cuda_fail(e, "NSGA-II set-up");
@@ -789,10 +799,8 @@ int32_t nsga_get_best(NsgaState& s, cudaStream_t st, float* keys, int32_t* perm,
         // decode on the device with the row kernel (same argsort as the generation step)
         float* tmpf = nullptr;
         int32_t* tmpp = nullptr;
-        e = cudaMalloc(&tmpf, 16);
-        if (e == cudaSuccess) e = cudaMalloc(&tmpp, (size_t)s.n * 4);
-        if (e != cudaSuccess) {
-            cudaFree(tmpf);
+        if (dev_alloc((void**)&tmpf, 16, st) != BRKGA_OK || dev_alloc((void**)&tmpp, (size_t)s.n * 4, st) != BRKGA_OK) {
+            dev_free(tmpf, st);
             return fail(BRKGA_ERR_OOM, "decode scratch");
         }
         RowLaunch L;
@@ -810,8 +818,8 @@ int32_t nsga_get_best(NsgaState& s, cudaStream_t st, float* keys, int32_t* perm,
         e = launch_rows(L, s.kind, s.tile, 1, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e == cudaSuccess) e = cudaMemcpy(perm, tmpp, (size_t)s.n * 4, cudaMemcpyDeviceToHost);
-        cudaFree(tmpf);
-        cudaFree(tmpp);
+        dev_free(tmpf, st);
+        dev_free(tmpp, st);
         if (e != cudaSuccess) return cuda_fail(e, "best decode");
     }
     return BRKGA_OK;

@@ -27,7 +27,7 @@ int32_t nsga_setup(NsgaState& s, Population& pop, PopDesc* dd, PopDesc& hdesc, c
                    bool stage);
 // allocate one population's NSGA-II buffers and fill its descriptor fields
 int32_t nsga_alloc(PopDesc& d, int P, double mut_rate, int div_interval, int Mn, std::vector<void*>& allocs,
-                   size_t* bytes);
+                   size_t* bytes, cudaStream_t stream);
 int nsga_max_population();
 cudaError_t nsga_prepare(int maxP);
 // group launches over `npops` consecutive NSGA-II descriptors

@@ -177,3 +177,27 @@ def test_invalid_params_rejected(cuda):
         with pytest.raises(B().BrkgaError) as ei:
             B().Solver(pb, bad)
         assert ei.value.code == -1
+
+
+def test_cpp_dropin_program(cuda, tmp_path):
+    """the reference-style C++ program (TSPLIB file -> TSPConfig::load_from_file -> Solver)
+    gives the same best tour as the Python binding on the same coordinates and seed"""
+    import json
+    import os
+    import subprocess
+    exe = os.path.join(os.path.dirname(B().LIB_PATH), "..", "build", "solve_tsp")
+    path = str(tmp_path / "inst.tsp")
+    r = subprocess.run([exe, path, "52", "1", "256", "51", "25", "60"], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    out = json.loads(r.stdout.strip().splitlines()[-1])
+    assert sorted(out["tour"]) == list(range(52)) and out["history"] == 61
+    xy = []
+    for line in open(path):
+        parts = line.split()
+        if len(parts) == 3 and parts[0].isdigit():
+            xy.append((float(parts[1]), float(parts[2])))
+    s = B().Solver(B().tsp(np.array(xy, np.float32)), B().params(256, 51, 25, 0.7, 60, seed=7))
+    s.run()
+    _, perm, fit = s.get_best_individual()
+    assert np.float32(out["best"]) == fit
+    assert out["tour"] == perm.tolist()
