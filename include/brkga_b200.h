@@ -140,6 +140,18 @@ int32_t brkga_pareto_rank(const float* d_obj, int32_t N, int32_t m, int32_t* d_r
  * front peeling by __popc of row & front-mask words.  Uses an internal device scratch of
  * N*ceil(N/32)*4 bytes and returns after the ranks are written. */
 int32_t brkga_pareto_rank_bitmatrix(const float* d_obj, int32_t N, int32_t m, int32_t* d_rank, void* stream);
+/* Pareto ranks exactly like brkga_pareto_rank, but the call allocates no device memory:
+ * for callers that cannot call cudaMalloc -- code running under a framework whose
+ * allocator owns all device memory, or a serving loop that must not allocate once
+ * started (cudaMalloc can synchronise the device).  No counterpart in the reference.
+ * The dominance rows and counts live in a fixed device array inside the library (532 KiB
+ * on every GPU that loads it, held until the process exits), so N is limited to 2048
+ * points (larger N returns BRKGA_ERR_UNSUPPORTED); 1 <= m <= 4.  The first call on a
+ * device looks up that array's address and raises a kernel's shared-memory limit; make
+ * that first call before any stream capture.  Asynchronous on `stream`.  Every call uses
+ * the same array: calls whose work overlaps on the GPU (different streams, or another
+ * thread) race and must be ordered by the caller. */
+int32_t brkga_pareto_rank_noalloc(const float* d_obj, int32_t N, int32_t m, int32_t* d_rank, void* stream);
 /* Crowding distance per front (core/population.hpp:453-489), fronts from d_rank. */
 int32_t brkga_crowding(const float* d_obj, const int32_t* d_rank, int32_t N, int32_t m, float* d_cd,
                        void* stream);

@@ -84,6 +84,7 @@ def lib():
         "brkga_init_population": (_i32, [_vp, _vp, _vp, _i32, _i32, _u64, _i32, _vp]),
         "brkga_pareto_rank": (_i32, [_vp, _i32, _i32, _vp, _vp]),
         "brkga_pareto_rank_bitmatrix": (_i32, [_vp, _i32, _i32, _vp, _vp]),
+        "brkga_pareto_rank_noalloc": (_i32, [_vp, _i32, _i32, _vp, _vp]),
         "brkga_crowding": (_i32, [_vp, _vp, _i32, _i32, _vp, _vp]),
         "brkga_create": (_i32, [_vp, C.POINTER(Params), C.POINTER(_vp)]),
         "brkga_destroy": (_i32, [_vp]),

@@ -851,6 +851,43 @@ int32_t nsga_get_front(NsgaState& s, cudaStream_t st, float* obj, float* keys, i
     return BRKGA_OK;
 }
 
+// ---------------------------------------------------------------------------------------
+// Pareto ranks for callers that cannot allocate device memory.  The dominance rows and
+// counts live in a file-scope device array of fixed size (every GPU that loads the
+// library holds it until the process exits); host code finds its device address with
+// cudaGetSymbolAddress once per device, with that device current.
+// ---------------------------------------------------------------------------------------
+constexpr int kStaticMaxN = 2048;                       // largest point count it accepts
+constexpr int kStaticW = (kStaticMaxN + 31) / 32;       // dominance row words
+constexpr size_t kStaticWords = (size_t)kStaticMaxN * kStaticW + kStaticMaxN;  // rows + counts (532 KiB)
+static __device__ __align__(256) uint32_t g_static_scratch[kStaticWords];
+
+static std::mutex g_static_mu;
+static std::map<int, uint32_t*> g_static_addr;  // device -> address of g_static_scratch
+
+// per-device set-up on first use: the array's device address and the peel kernel's
+// shared-memory limit (neither allocates device memory)
+static int32_t static_scratch(uint32_t** out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    std::lock_guard<std::mutex> lk(g_static_mu);
+    auto it = g_static_addr.find(dev);
+    if (it != g_static_addr.end()) {
+        *out = it->second;
+        return BRKGA_OK;
+    }
+    void* ptr = nullptr;
+    e = cudaGetSymbolAddress(&ptr, g_static_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress (static scratch)");
+    const size_t smem = (((size_t)kStaticMaxN * 2 + 15) / 16) * 16 + peel_smem_bytes(kStaticMaxN);
+    e = raise_smem_limit(reinterpret_cast<const void*>(peel_op_kernel), smem);
+    if (e != cudaSuccess) return cuda_fail(e, "peel set-up");
+    g_static_addr[dev] = (uint32_t*)ptr;
+    *out = (uint32_t*)ptr;
+    return BRKGA_OK;
+}
+
 // scratch of the operator entry points (grow-only, per device)
 static std::mutex g_op_mu;
 static std::map<int, std::pair<void*, size_t>> g_op_buf;
@@ -908,6 +945,35 @@ int32_t brkga_pareto_rank_bitmatrix(const float* d_obj, int32_t N, int32_t m, in
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "peel launch");
     // the scratch is shared by later calls: finish before returning
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(e, "peel");
+    return BRKGA_OK;
+}
+
+int32_t brkga_pareto_rank_noalloc(const float* d_obj, int32_t N, int32_t m, int32_t* d_rank, void* stream) {
+    if (!d_obj || !d_rank) return fail(BRKGA_ERR_INVALID, "null argument");
+    if (N < 0 || m < 1 || m > 4) return fail(BRKGA_ERR_INVALID, "need N >= 0 and 1 <= m <= 4");
+    if (N > kStaticMaxN)
+        return fail(BRKGA_ERR_UNSUPPORTED, "brkga_pareto_rank_noalloc takes at most " + std::to_string(kStaticMaxN) +
+                                               " points (got " + std::to_string(N) + "); use brkga_pareto_rank");
+    if (N == 0) return BRKGA_OK;
+    uint32_t* base = nullptr;
+    int32_t rc = static_scratch(&base);
+    if (rc != BRKGA_OK) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    const int W = (N + 31) / 32;
+    DomArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.obj = d_obj;
+    a.rawN = N;
+    a.m = m;
+    a.S = base;                                        // rows [N][W]: every word is written
+    a.cnt = (int32_t*)(base + (size_t)kStaticMaxN * kStaticW);  // counts [N]: every entry is written
+    a.Wmax = W;
+    dom_build_kernel<<<(N + 7) / 8, 256, 0, st>>>(a);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "dominance launch");
+    const size_t smem = (((size_t)N * 2 + 15) / 16) * 16 + peel_smem_bytes(N);
+    peel_op_kernel<<<1, kNsgaBlock, smem, st>>>(N, a.S, a.cnt, W, d_rank);
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "peel launch");
     return BRKGA_OK;
 }
 
