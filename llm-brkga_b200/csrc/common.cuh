@@ -118,6 +118,7 @@ struct PopDesc {
     uint32_t* domS;           // [2P][domW] dominance rows
     int32_t* domcnt;          // [2P] domination counts
     int32_t* nu;              // diversity pass: unique count, P when nothing was rebuilt
+    int32_t* nord;            // [2][2P] pool points in (rank, objective o, index) order
     // shared launches: a population whose generation has reached gen_limit (> 0) is left
     // unchanged by every kernel; `advanced` records whether the last generation ran
     uint32_t gen_limit;

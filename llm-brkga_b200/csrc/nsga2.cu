@@ -130,6 +130,80 @@ __global__ void dom_build_kernel(DomArgs a) {
     }
 }
 
+// Two objectives (every NSGA-II problem of the engine): the objectives are staged in
+// shared memory and each warp tests four rows against 32 columns per step.  The four
+// comparisons of a pair give both directions: i dominates j iff !(a0 > b0) && !(a1 > b1)
+// && (a0 < b0 || a1 < b1), the reference's Individual::dominates (core/individual.hpp:99-114)
+// with its NaN behaviour; padding columns are NaN, which dominates nothing either way.
+constexpr int kDom2Rows = 4;     // rows per warp
+constexpr int kDom2Warps = 4;    // warps per CTA
+
+__global__ void __launch_bounds__(kDom2Warps * 32) dom2_build_kernel(DomArgs a) {
+    extern __shared__ float2 so[];  // [32 * ceil(N / 32)] objectives
+    const float* obj;
+    int N, Wmax;
+    uint32_t* S;
+    int32_t* cnt;
+    if (a.dd) {
+        const PopDesc& d = a.dd[blockIdx.y];
+        if (a.pool && at_limit(d)) return;
+        if (a.only_rebuilt && (!d.advanced || __ldg(d.nu) >= d.P)) return;
+        N = a.pool ? 2 * d.P : d.P;
+        obj = d.fit[d.cur];
+        S = d.domS;
+        cnt = d.domcnt;
+        Wmax = d.domW;
+    } else {
+        N = a.rawN;
+        obj = a.obj;
+        S = a.S;
+        cnt = a.cnt;
+        Wmax = a.Wmax;
+    }
+    constexpr int RPC = kDom2Rows * kDom2Warps;  // rows per CTA
+    const int row0 = blockIdx.x * RPC;
+    if (row0 >= N) return;
+    const int W = (N + 31) / 32;
+    const float2* o2 = reinterpret_cast<const float2*>(obj);
+    for (int j = threadIdx.x; j < 32 * W; j += blockDim.x) so[j] = (j < N) ? __ldg(o2 + j) : make_float2(NAN, NAN);
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int i0 = row0 + warp * kDom2Rows;
+    float2 oi[kDom2Rows];
+    int c[kDom2Rows];
+    uint32_t buf[kDom2Rows];
+#pragma unroll
+    for (int r = 0; r < kDom2Rows; ++r) {
+        oi[r] = so[min(i0 + r, N - 1)];
+        c[r] = 0;
+        buf[r] = 0u;
+    }
+    for (int w = 0; w < W; ++w) {
+        const float2 oj = so[32 * w + lane];
+#pragma unroll
+        for (int r = 0; r < kDom2Rows; ++r) {
+            const bool gt0 = oi[r].x > oj.x, gt1 = oi[r].y > oj.y;
+            const bool lt0 = oi[r].x < oj.x, lt1 = oi[r].y < oj.y;
+            const uint32_t si = __ballot_sync(0xffffffffu, !gt0 && !gt1 && (lt0 || lt1));
+            const uint32_t di = __ballot_sync(0xffffffffu, !lt0 && !lt1 && (gt0 || gt1));
+            c[r] += __popc(di);
+            if (lane == (w & 31)) buf[r] = si;
+        }
+        if ((w & 31) == 31 || w == W - 1) {
+            // lane l holds word (w & ~31) + l of each row: one coalesced store per row
+            const int wl = (w & ~31) + lane;
+#pragma unroll
+            for (int r = 0; r < kDom2Rows; ++r)
+                if (i0 + r < N && wl <= w) S[(size_t)(i0 + r) * Wmax + wl] = buf[r];
+        }
+    }
+    if (lane == 0) {
+#pragma unroll
+        for (int r = 0; r < kDom2Rows; ++r)
+            if (i0 + r < N) cnt[i0 + r] = c[r];
+    }
+}
+
 struct PeelSmem {
     uint32_t* C;      // [kCB][W] count planes
     uint32_t* A;      // [W] ranked
@@ -201,13 +275,41 @@ __device__ int peel_ranks(int N, const uint32_t* __restrict__ S, int Wmax, const
 #pragma unroll
         for (int b = 0; b < kDB; ++b) acc[b] = 0u;
         if (w < W) {
-            for (int j = sl; j < (int)nf; j += SP) {
-                uint32_t carry = __ldg(S + (size_t)ps.list[j] * Wmax + w);
+            // bit-sliced column sums: the member rows' words are loaded eight at a time
+            // (eight L2 requests in flight per lane), counted in a 4-plane counter and
+            // added into the kDB-plane accumulator once per batch
+            constexpr int kBatch = 8;
+            for (int j0 = sl; j0 < (int)nf; j0 += kBatch * SP) {
+                uint32_t xs[kBatch];
 #pragma unroll
-                for (int b = 0; b < kDB; ++b) {
-                    const uint32_t tb = acc[b] & carry;
-                    acc[b] ^= carry;
-                    carry = tb;
+                for (int u = 0; u < kBatch; ++u) {
+                    const int j = j0 + u * SP;
+                    xs[u] = (j < (int)nf) ? __ldg(S + (size_t)ps.list[j] * Wmax + w) : 0u;
+                }
+                uint32_t s0 = 0u, s1 = 0u, s2 = 0u, s3 = 0u;
+#pragma unroll
+                for (int u = 0; u < kBatch; ++u) {
+                    const uint32_t c0 = s0 & xs[u];
+                    s0 ^= xs[u];
+                    const uint32_t c1 = s1 & c0;
+                    s1 ^= c0;
+                    const uint32_t c2 = s2 & c1;
+                    s2 ^= c1;
+                    s3 ^= c2;
+                }
+                uint32_t cy = 0u;
+                const uint32_t sv[4] = {s0, s1, s2, s3};
+#pragma unroll
+                for (int b = 0; b < 4; ++b) {
+                    const uint32_t x = acc[b], y = sv[b];
+                    acc[b] = x ^ y ^ cy;
+                    cy = (x & y) | (cy & (x ^ y));
+                }
+#pragma unroll
+                for (int b = 4; b < kDB; ++b) {
+                    const uint32_t x = acc[b];
+                    acc[b] = x ^ cy;
+                    cy = x & cy;
                 }
             }
         }
@@ -267,6 +369,7 @@ struct SelSmem {
     unsigned long long* key;    // [K2]: next_pow2(2N) sort entries
     uint16_t* fs;               // [N] first sorted position of each rank
     uint16_t* fe;               // [N] last sorted position of each rank
+    uint32_t* rb;               // [N + 1] survivor entries before each rank
     unsigned char* peel;        // peel_smem_bytes(N)
 };
 
@@ -277,6 +380,7 @@ __host__ __device__ inline size_t sel_smem_bytes(int N) {
     b += ((size_t)N * 4 + 15) / 16 * 16;
     b += (size_t)K2 * 8;
     b += ((size_t)N * 2 + 15) / 16 * 16 * 2;
+    b += ((size_t)(N + 1) * 4 + 15) / 16 * 16;
     b += peel_smem_bytes(N);
     return (b + 15) / 16 * 16;
 }
@@ -297,6 +401,8 @@ __device__ inline SelSmem sel_carve(unsigned char* base, int N) {
     off += ((size_t)N * 2 + 15) / 16 * 16;
     s.fe = (uint16_t*)(base + off);
     off += ((size_t)N * 2 + 15) / 16 * 16;
+    s.rb = (uint32_t*)(base + off);
+    off += ((size_t)(N + 1) * 4 + 15) / 16 * 16;
     s.peel = base + off;
     return s;
 }
@@ -306,8 +412,58 @@ __device__ __forceinline__ uint32_t cd_key(float c) {
     return (k == 0xFFFFFFFFu) ? 0xFFFFFFFFu : ~k;
 }
 
-// crowding distance (core/population.hpp:453-489) over the reference's front lists:
-// rank-0 points are two adjacent entries (index, copy 0/1), other points one
+// front bounds of the (rank, objective, index) order held in s.key[0, N)
+template <int T>
+__device__ void front_bounds(int N, const SelSmem& s) {
+    for (int p = threadIdx.x; p < N; p += T) {
+        const int r = (int)(s.key[p] >> 48);
+        if (p == 0 || (int)(s.key[p - 1] >> 48) != r) s.fs[r] = (uint16_t)p;
+        if (p == N - 1 || (int)(s.key[p + 1] >> 48) != r) s.fe[r] = (uint16_t)p;
+    }
+}
+
+// one objective's contribution to the crowding distance (core/population.hpp:453-489) over
+// the reference's front lists, s.key[0, N) in (rank, objective o, index) order: rank-0
+// points are two adjacent entries (index, copy 0/1), other points one
+template <int T>
+__device__ void crowding_pass(int N, int o, const SelSmem& s) {
+#define VAL(pos) s.obj[2 * (int)(s.key[pos] & 0xFFFFu) + o]
+    for (int p = threadIdx.x; p < N; p += T) {
+        const int i = (int)(s.key[p] & 0xFFFFu);
+        const int r = (int)(s.key[p] >> 48);
+        const int f = s.fs[r], l = s.fe[r];
+        const int size = l - f + 1;
+        if (r == 0) {
+            // entries 2(p-f) and 2(p-f)+1 of the doubled list of 2*size entries
+            if (size == 1 || p == f || p == l) {
+                s.cd[i] = INFINITY;
+            } else {
+                const float range = __fsub_rn(VAL(l), VAL(f));
+                if (range > 0.0f) {
+                    const float v = VAL(p);
+                    const float da = __fdiv_rn(__fsub_rn(v, VAL(p - 1)), range);
+                    const float db = __fdiv_rn(__fsub_rn(VAL(p + 1), v), range);
+                    s.cd[i] = __fadd_rn(__fadd_rn(s.cd[i], da), db);
+                }
+            }
+        } else {
+            if (size <= 2 || p == f || p == l) {
+                s.cd[i] = INFINITY;
+            } else {
+                const float range = __fsub_rn(VAL(l), VAL(f));
+                if (range > 0.0f)
+                    s.cd[i] = __fadd_rn(s.cd[i], __fdiv_rn(__fsub_rn(VAL(p + 1), VAL(p - 1)), range));
+            }
+        }
+    }
+#undef VAL
+}
+
+__device__ __forceinline__ unsigned long long order_key(int rank, float v, int i) {
+    return ((unsigned long long)rank << 48) | ((unsigned long long)okey(v) << 16) | (unsigned long long)i;
+}
+
+// crowding with an in-CTA bitonic sort per objective (operator entry point)
 template <int T>
 __device__ void crowding_ref(int N, const SelSmem& s) {
     const int t = threadIdx.x;
@@ -315,117 +471,107 @@ __device__ void crowding_ref(int N, const SelSmem& s) {
     for (int i = t; i < N; i += T) s.cd[i] = 0.0f;
     for (int o = 0; o < 2; ++o) {
         __syncthreads();
-        for (int i = t; i < N2; i += T)
-            s.key[i] = (i < N) ? (((unsigned long long)s.rank[i] << 48) |
-                                  ((unsigned long long)okey(s.obj[2 * i + o]) << 16) | (unsigned long long)i)
-                               : ~0ull;
+        for (int i = t; i < N2; i += T) s.key[i] = (i < N) ? order_key(s.rank[i], s.obj[2 * i + o], i) : ~0ull;
         __syncthreads();
         bitonic_u64<T>(s.key, N2);
+        front_bounds<T>(N, s);
+        __syncthreads();
+        crowding_pass<T>(N, o, s);
+    }
+    __syncthreads();
+}
+
+// crowding from the orders nsga_order_kernel computed (ord[o * ostride + position]); leaves
+// s.key holding the objective-1 order and s.fs / s.fe its front bounds
+template <int T>
+__device__ void crowding_given(int N, const SelSmem& s, const int32_t* __restrict__ ord, int ostride) {
+    const int t = threadIdx.x;
+    for (int i = t; i < N; i += T) s.cd[i] = 0.0f;
+    for (int o = 0; o < 2; ++o) {
+        __syncthreads();
         for (int p = t; p < N; p += T) {
-            const int r = (int)(s.key[p] >> 48);
-            if (p == 0 || (int)(s.key[p - 1] >> 48) != r) s.fs[r] = (uint16_t)p;
-            if (p == N - 1 || (int)(s.key[p + 1] >> 48) != r) s.fe[r] = (uint16_t)p;
+            const int i = __ldg(ord + (size_t)o * ostride + p);
+            s.key[p] = order_key(s.rank[i], s.obj[2 * i + o], i);
         }
         __syncthreads();
-#define VAL(pos) s.obj[2 * (int)(s.key[pos] & 0xFFFFu) + o]
-        for (int p = t; p < N; p += T) {
-            const int i = (int)(s.key[p] & 0xFFFFu);
-            const int r = (int)(s.key[p] >> 48);
-            const int f = s.fs[r], l = s.fe[r];
-            const int size = l - f + 1;
-            if (r == 0) {
-                // entries 2(p-f) and 2(p-f)+1 of the doubled list of 2*size entries
-                if (size == 1 || p == f || p == l) {
-                    s.cd[i] = INFINITY;
-                } else {
-                    const float range = __fsub_rn(VAL(l), VAL(f));
-                    if (range > 0.0f) {
-                        const float v = VAL(p);
-                        const float da = __fdiv_rn(__fsub_rn(v, VAL(p - 1)), range);
-                        const float db = __fdiv_rn(__fsub_rn(VAL(p + 1), v), range);
-                        s.cd[i] = __fadd_rn(__fadd_rn(s.cd[i], da), db);
-                    }
-                }
-            } else {
-                if (size <= 2 || p == f || p == l) {
-                    s.cd[i] = INFINITY;
-                } else {
-                    const float range = __fsub_rn(VAL(l), VAL(f));
-                    if (range > 0.0f)
-                        s.cd[i] = __fadd_rn(s.cd[i], __fdiv_rn(__fsub_rn(VAL(p + 1), VAL(p - 1)), range));
-                }
-            }
-        }
-#undef VAL
+        front_bounds<T>(N, s);
+        __syncthreads();
+        crowding_pass<T>(N, o, s);
     }
     __syncthreads();
 }
 
 // survivors (core/population.hpp:491-517): whole fronts while they fit, ordered by
-// (last objective, index, copy); the cut front by (-crowding, index, copy)
+// (last objective, index, copy) -- the objective-1 order in s.key with every rank-0 point
+// taken twice -- then the cut front by (-crowding, index, copy), sorted alone
 template <int T>
-__device__ void select_ref(int N, int P, const SelSmem& s, int32_t* g_sel, int32_t* g_rank, float* g_cd,
-                           float* fmin_out, uint32_t* wt32) {
+__device__ void select_given(int N, int P, const SelSmem& s, int32_t* g_sel, int32_t* g_rank, float* g_cd,
+                             float* fmin_out, uint32_t* wt32) {
     const int t = threadIdx.x;
-    const int ch = (N + T - 1) / T;
-    const int i0 = min(N, t * ch), i1 = min(N, i0 + ch);
     __shared__ int s_cut;
-    // entries per rank (first-front points count twice), in the key buffer before the sort
-    uint32_t* cnt = reinterpret_cast<uint32_t*>(s.key);
-    for (int r = t; r < N; r += T) cnt[r] = 0u;
-    if (t == 0) s_cut = 0x7fffffff;
-    __syncthreads();
-    for (int i = t; i < N; i += T) atomicAdd(&cnt[s.rank[i]], s.rank[i] == 0 ? 2u : 1u);
-    __syncthreads();
-    // inclusive prefix over ranks; the cut is the first rank whose prefix passes P
+    const int R = (int)(s.key[N - 1] >> 48) + 1;  // ranks 0 .. R-1 all occur
+    // survivor entries of each rank (rank 0 counts twice), prefix over ranks
+    const int ch = (R + T - 1) / T;
+    const int r0 = min(R, t * ch), r1 = min(R, r0 + ch);
     uint32_t loc = 0;
-    for (int r = i0; r < i1; ++r) loc += cnt[r];
+    for (int r = r0; r < r1; ++r) loc += (uint32_t)(s.fe[r] - s.fs[r] + 1) * (r == 0 ? 2u : 1u);
+    if (t == 0) s_cut = R;
     uint32_t run = block_exclusive_scan<T>(loc, wt32, nullptr);
-    for (int r = i0; r < i1; ++r) {
-        run += cnt[r];
-        if (run > (uint32_t)P) {
-            atomicMin(&s_cut, r);
-            break;
-        }
+    for (int r = r0; r < r1; ++r) {
+        s.rb[r] = run;
+        run += (uint32_t)(s.fe[r] - s.fs[r] + 1) * (r == 0 ? 2u : 1u);
+        if (run > (uint32_t)P && s.rb[r] <= (uint32_t)P) s_cut = r;  // exactly one rank crosses P
     }
-    // compact the first-front points (their second entries), in index order
-    uint32_t z = 0;
-    for (int i = i0; i < i1; ++i) z += (s.rank[i] == 0) ? 1u : 0u;
-    uint32_t n0 = 0;
-    uint32_t pos = block_exclusive_scan<T>(z, wt32, &n0);
-    for (int i = i0; i < i1; ++i)
-        if (s.rank[i] == 0) s.fe[pos++] = (uint16_t)i;
     __syncthreads();
     const int cut = s_cut;
-    const int E = N + (int)n0;
-    const int K2 = npow2(E);
-    for (int e = t; e < K2; e += T) {
-        unsigned long long k = ~0ull;
-        if (e < E) {
-            const int i = (e < N) ? e : (int)s.fe[e - N];
-            const int c = (e < N) ? 0 : 1;
-            const int r = s.rank[i];
-            if (r <= cut) {
-                const uint32_t sec = (r == cut) ? cd_key(s.cd[i]) : okey(s.obj[2 * i + 1]);
-                k = ((unsigned long long)r << 46) | ((unsigned long long)sec << 14) | ((unsigned long long)i << 1) |
-                    (unsigned long long)c;
-            }
-        }
-        s.key[e] = k;
-    }
-    __syncthreads();
-    bitonic_u64<T>(s.key, K2);
     float fmin = INFINITY;
-    for (int q = t; q < P; q += T) {
-        const int i = (int)((s.key[q] >> 1) & 0x1FFFu);
-        g_sel[q] = i;
-        g_rank[q] = s.rank[i];
-        g_cd[q] = s.cd[i];
+    // whole fronts before the cut
+    for (int p = t; p < N; p += T) {
+        const int r = (int)(s.key[p] >> 48);
+        if (r >= cut) continue;
+        const int i = (int)(s.key[p] & 0xFFFFu);
+        const int k = p - s.fs[r];
+        const int q = (int)s.rb[r] + (r == 0 ? 2 * k : k);
+        for (int c = 0; c < (r == 0 ? 2 : 1); ++c) {
+            g_sel[q + c] = i;
+            g_rank[q + c] = r;
+            g_cd[q + c] = s.cd[i];
+        }
         fmin = fminf(fmin, s.obj[2 * i]);
+    }
+    const int f = (cut < R) ? s.fs[cut] : 0;
+    const int nc = (cut < R) ? s.fe[cut] - f + 1 : 0;
+    __syncthreads();
+    if (cut < R) {
+        // the cut front's points, in order, into s.fs; then its entries sorted by
+        // (cd descending, index, copy) in s.key (sized for 2N entries)
+        for (int k = t; k < nc; k += T) s.fs[k] = (uint16_t)(s.key[f + k] & 0xFFFFu);
+        __syncthreads();
+        const int mult = (cut == 0) ? 2 : 1;
+        const int E = nc * mult, K2 = npow2(E);
+        const int take = P - (int)s.rb[cut];
+        for (int e = t; e < K2; e += T) {
+            unsigned long long kk = ~0ull;
+            if (e < E) {
+                const int i = s.fs[e / mult];
+                kk = ((unsigned long long)cd_key(s.cd[i]) << 32) | ((unsigned long long)i << 1) |
+                     (unsigned long long)(e % mult);
+            }
+            s.key[e] = kk;
+        }
+        __syncthreads();
+        bitonic_u64<T>(s.key, K2);
+        for (int k = t; k < take; k += T) {
+            const int i = (int)((s.key[k] >> 1) & 0x7FFFu);
+            const int q = (int)s.rb[cut] + k;
+            g_sel[q] = i;
+            g_rank[q] = cut;
+            g_cd[q] = s.cd[i];
+            fmin = fminf(fmin, s.obj[2 * i]);
+        }
     }
     *fmin_out = fmin;
 }
-
 
 __device__ float block_min_f(float v, float* red) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -439,29 +585,73 @@ __device__ float block_min_f(float v, float* red) {
     return r;
 }
 
-// mode 0: survivors of the 2P pool of fit[cur]; mode 1: ranks + crowding of the P
-// population (initialisation); mode 2: as mode 1, only for populations the diversity
-// pass rebuilt (*nu < P).  One CTA per population (blockIdx.x).
+// Selection launches (core/population.hpp:409-517): mode 0 works on the 2P pool of fit[cur]
+// and picks the survivors; mode 1 ranks the P population (initialisation); mode 2 does
+// the same only for populations the diversity pass rebuilt (*nu < P).
+__device__ __forceinline__ bool select_active(const PopDesc& d, int mode) {
+    if (mode == 0) return !at_limit(d);
+    if (mode == 2) return d.advanced && __ldg(d.nu) < d.P;
+    return true;
+}
+
+// ranks by bit-sliced peeling, one CTA per population; ranks -> domcnt[0, N)
+__global__ void __launch_bounds__(kNsgaBlock) nsga_peel_kernel(PopDesc* dd, int mode) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ uint32_t wt32[32];
+    PopDesc& d = dd[blockIdx.x];
+    if (!select_active(d, mode)) return;
+    const int N = (mode == 0) ? 2 * d.P : d.P;
+    uint16_t* r16 = reinterpret_cast<uint16_t*>(smem);
+    const PeelSmem ps = peel_carve(smem + (((size_t)N * 2 + 15) / 16) * 16, N);
+    peel_ranks<kNsgaBlock>(N, d.domS, d.domW, d.domcnt, r16, ps, wt32);
+    __syncthreads();
+    for (int i = threadIdx.x; i < N; i += kNsgaBlock) d.domcnt[i] = r16[i];
+}
+
+// The pool ordered by (rank, objective o, index) for o = blockIdx.y, by exact counting:
+// position(i) = #{j : key_j < key_i} over unique composite keys.  N^2 compares per
+// objective spread over the grid; one warp per point.
+constexpr int kOrdThreads = 1024, kOrdPerCta = kOrdThreads / 32;
+
+__global__ void __launch_bounds__(kOrdThreads) nsga_order_kernel(PopDesc* dd, int mode) {
+    extern __shared__ unsigned long long okeys[];  // [N]
+    const PopDesc& d = dd[blockIdx.z];
+    if (!select_active(d, mode)) return;
+    const int N = (mode == 0) ? 2 * d.P : d.P;
+    const int base = blockIdx.x * kOrdPerCta;
+    if (base >= N) return;
+    const int o = blockIdx.y, t = threadIdx.x;
+    const float* f = d.fit[d.cur];
+    for (int i = t; i < N; i += kOrdThreads) okeys[i] = order_key(__ldg(d.domcnt + i), __ldg(f + 2 * i + o), i);
+    __syncthreads();
+    const int lane = t & 31, i = base + (t >> 5);
+    const unsigned long long me = (i < N) ? okeys[i] : 0ull;
+    int cnt = 0;
+#pragma unroll 8
+    for (int j = lane; j < N; j += 32) cnt += (okeys[j] < me) ? 1 : 0;
+#pragma unroll
+    for (int off = 16; off >= 1; off >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, off);
+    if (lane == 0 && i < N) d.nord[(size_t)o * 2 * d.P + cnt] = i;
+}
+
+// crowding and (mode 0) survivors from the ranks and orders above; one CTA per population
 __global__ void __launch_bounds__(kNsgaBlock) nsga_select_kernel(PopDesc* dd, int mode) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ uint32_t wt32[32];
     __shared__ float redf[32];
     PopDesc& d = dd[blockIdx.x];
+    if (!select_active(d, mode)) return;
     const int t = threadIdx.x;
     const int P = d.P;
-    if (mode == 0 && at_limit(d)) return;
-    if (mode == 2 && (!d.advanced || __ldg(d.nu) >= P)) return;
     const int N = (mode == 0) ? 2 * P : P;
     const float* f = d.fit[d.cur];
     const SelSmem s = sel_carve(smem, N);
     for (int i = t; i < 2 * N; i += kNsgaBlock) s.obj[i] = f[i];
-    const PeelSmem ps = peel_carve(s.peel, N);
-    peel_ranks<kNsgaBlock>(N, d.domS, d.domW, d.domcnt, s.rank, ps, wt32);
-    __syncthreads();
-    crowding_ref<kNsgaBlock>(N, s);
+    for (int i = t; i < N; i += kNsgaBlock) s.rank[i] = (uint16_t)__ldg(d.domcnt + i);
+    crowding_given<kNsgaBlock>(N, s, d.nord, 2 * P);
     float fmin = INFINITY;
     if (mode == 0) {
-        select_ref<kNsgaBlock>(N, P, s, d.nsel, d.nrank, d.ncd, &fmin, wt32);
+        select_given<kNsgaBlock>(N, P, s, d.nsel, d.nrank, d.ncd, &fmin, wt32);
     } else {
         for (int i = t; i < P; i += kNsgaBlock) {
             d.nrank[i] = s.rank[i];
@@ -532,58 +722,128 @@ __global__ void nsga_finish_kernel(PopDesc* dd, int npops) {
     }
 }
 
-// ensure_minimum_diversity (core/population.hpp:130-182): greedy in-order dedupe in
-// objective space (distance < 0.001, float differences squared and summed in double);
-// when fewer than 70% are unique, the unique rows move to the front in order and
-// *nu < P tells the refill and re-rank launches to run.  It runs after generation g when
-// (g - 1) % interval == 0 (the reference's counter is g - 1).  One CTA per population.
+// ensure_minimum_diversity (core/population.hpp:130-182) runs after generation g when
+// (g - 1) % interval == 0 (the reference's counter is g - 1).
+__device__ __forceinline__ bool div_due(const PopDesc& d) {
+    return d.advanced && d.div_interval > 0 && d.gen >= 1u && ((d.gen - 1u) % (uint32_t)d.div_interval) == 0u;
+}
+
+// The reference keeps a point when no earlier KEPT point is within distance 0.001 in
+// objective space (float differences, squared and summed in double).  near_build_kernel
+// records, per point c, which earlier points u < c are that close (bit u of row c of the
+// dominance scratch); nsga_diversity_kernel then settles keep / drop in rounds: c is
+// dropped as soon as a kept point is near it, kept once every near earlier point is
+// settled as dropped.  The result is the reference's greedy in-order pass.
+constexpr int kNearWarps = 4, kNearRows = 4;
+
+__global__ void __launch_bounds__(kNearWarps * 32) near_build_kernel(PopDesc* dd) {
+    extern __shared__ float2 so[];  // [32 * ceil(P / 32)]
+    const PopDesc& d = dd[blockIdx.y];
+    if (!div_due(d)) return;
+    const int P = d.P, W = (P + 31) / 32;
+    const int row0 = blockIdx.x * kNearWarps * kNearRows;
+    if (row0 >= P) return;
+    const float2* o2 = reinterpret_cast<const float2*>(d.fit[d.cur]);
+    for (int j = threadIdx.x; j < 32 * W; j += blockDim.x) so[j] = (j < P) ? o2[j] : make_float2(0.0f, 0.0f);
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int r = 0; r < kNearRows; ++r) {
+        const int c = row0 + warp * kNearRows + r;
+        if (c >= P) break;
+        const float2 pc = so[c];
+        uint32_t* row = d.domS + (size_t)c * d.domW;
+        for (int w = 0; w <= c / 32; ++w) {
+            const int u = 32 * w + lane;
+            bool near = false;
+            if (u < c) {
+                const float2 pu = so[u];
+                const double d0 = (double)__fsub_rn(pc.x, pu.x);
+                const double d1 = (double)__fsub_rn(pc.y, pu.y);
+                near = __dsqrt_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1))) < 0.001;
+            }
+            const uint32_t bits = __ballot_sync(0xffffffffu, near);
+            if (lane == 0) row[w] = bits;
+        }
+    }
+}
+
+// Settles the pass (one CTA per population).  When fewer than 70% are kept, the kept rows
+// are gathered in order into the other key buffer, which becomes the current one, and
+// *nu < P tells the refill and re-rank launches to run; otherwise *nu = P.
 __global__ void __launch_bounds__(kNsgaBlock) nsga_diversity_kernel(PopDesc* dd) {
-    extern __shared__ float2 uobj[];  // [P]
+    constexpr int WP = kMaxPool / 2 / 32;
+    __shared__ uint32_t U[WP], D[WP], Un[WP], Dn[WP];
+    __shared__ uint32_t wt32[32];
     PopDesc& d = dd[blockIdx.x];
-    const int t = threadIdx.x, P = d.P, interval = d.div_interval;
-    const uint32_t g = d.gen;
-    if (!d.advanced || interval <= 0 || g < 1 || ((g - 1) % (uint32_t)interval) != 0) {
+    const int t = threadIdx.x, P = d.P, W = (P + 31) / 32;
+    if (!div_due(d)) {
         if (t == 0) *d.nu = P;
         return;
     }
-    float* f = d.fit[d.cur];
-    int nu = 0;
-    for (int c = 0; c < P; ++c) {
-        const float c0 = f[2 * c], c1 = f[2 * c + 1];
-        int near = 0;
-        for (int u = t; u < nu; u += kNsgaBlock) {
-            const double d0 = (double)__fsub_rn(c0, uobj[u].x);
-            const double d1 = (double)__fsub_rn(c1, uobj[u].y);
-            const double dist = __dsqrt_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)));
-            near |= (dist < 0.001) ? 1 : 0;
-        }
-        near = __syncthreads_or(near);
-        if (!near) {
-            if (t == 0) {
-                uobj[nu] = make_float2(c0, c1);
-                d.nsel[nu] = c;
+    for (int w = t; w < W; w += kNsgaBlock) U[w] = D[w] = Un[w] = Dn[w] = 0u;
+    __syncthreads();
+    // every round settles at least the lowest unsettled point, so P rounds suffice
+    for (int round = 0; round <= P; ++round) {
+        int open = 0;
+        for (int c = t; c < P; c += kNsgaBlock) {
+            if ((D[c >> 5] >> (c & 31)) & 1u) continue;
+            const uint32_t* row = d.domS + (size_t)c * d.domW;
+            const int last = c >> 5;
+            bool kept_near = false, unsettled = false;
+            for (int w = 0; w <= last; ++w) {
+                uint32_t nb = __ldg(row + w);
+                if (w == last) nb &= (1u << (c & 31)) - 1u;
+                kept_near |= (nb & U[w]) != 0u;
+                unsettled |= (nb & ~D[w]) != 0u;
             }
-            ++nu;
+            if (kept_near) {
+                atomicOr(&Dn[c >> 5], 1u << (c & 31));
+            } else if (!unsettled) {
+                atomicOr(&Un[c >> 5], 1u << (c & 31));
+                atomicOr(&Dn[c >> 5], 1u << (c & 31));
+            } else {
+                open = 1;
+            }
         }
         __syncthreads();
+        for (int w = t; w < W; w += kNsgaBlock) {
+            U[w] |= Un[w];
+            D[w] |= Dn[w];
+        }
+        if (!__syncthreads_or(open)) break;
     }
+    // kept points in index order -> nsel[0, nu)
+    const int pc = (t < W) ? __popc(U[t]) : 0;
+    uint32_t nu = 0;
+    uint32_t pos = block_exclusive_scan<kNsgaBlock>((uint32_t)pc, wt32, &nu);
+    if (t < W)
+        for (uint32_t x = U[t]; x; x &= x - 1) d.nsel[pos++] = 32 * t + __ffs(x) - 1;
+    __syncthreads();
     const double ratio = (double)nu / (double)P;
     if (!(ratio < 0.70)) {
         if (t == 0) *d.nu = P;
         return;
     }
-    // compact the unique rows to the front, in order (sources never precede targets)
-    float4* keys = reinterpret_cast<float4*>(d.keys[d.cur]);
-    const int ld4 = d.ld / 4;
-    for (int i = 0; i < nu; ++i) {
-        const int src = d.nsel[i];
-        if (src != i) {
-            for (int c = t; c < ld4; c += kNsgaBlock) keys[(size_t)i * ld4 + c] = keys[(size_t)src * ld4 + c];
-            if (t < 2) f[2 * i + t] = f[2 * src + t];
-        }
-        __syncthreads();
+    // gather the kept rows, in order, into the other buffer and make it current
+    const int cur = d.cur, ld4 = d.ld / 4;
+    const float4* src = reinterpret_cast<const float4*>(d.keys[cur]);
+    float4* dst = reinterpret_cast<float4*>(d.keys[cur ^ 1]);
+    const float* fs = d.fit[cur];
+    float* fd = d.fit[cur ^ 1];
+    const size_t total = (size_t)nu * ld4;
+    for (size_t x = t; x < total; x += kNsgaBlock) {
+        const int q = (int)(x / ld4), col = (int)(x % ld4);
+        dst[x] = src[(size_t)d.nsel[q] * ld4 + col];
     }
-    if (t == 0) *d.nu = nu;
+    for (int q = t; q < (int)nu; q += kNsgaBlock) {
+        fd[2 * q] = fs[2 * d.nsel[q]];
+        fd[2 * q + 1] = fs[2 * d.nsel[q] + 1];
+    }
+    __syncthreads();
+    if (t == 0) {
+        d.cur = cur ^ 1;
+        *d.nu = (int)nu;
+    }
 }
 
 // ---------------------------------------------------------------------------------------
@@ -593,11 +853,27 @@ int nsga_max_population() { return kMaxPool / 2; }
 
 size_t nsga_select_smem(int maxP) { return sel_smem_bytes(2 * maxP); }
 
+static size_t peel_kernel_smem(int N) { return (((size_t)N * 2 + 15) / 16) * 16 + peel_smem_bytes(N); }
+
 cudaError_t nsga_prepare(int maxP) {
     cudaError_t e = raise_smem_limit(reinterpret_cast<const void*>(nsga_select_kernel), sel_smem_bytes(2 * maxP));
     if (e == cudaSuccess)
-        e = raise_smem_limit(reinterpret_cast<const void*>(nsga_diversity_kernel), (size_t)maxP * 8);
+        e = raise_smem_limit(reinterpret_cast<const void*>(nsga_peel_kernel), peel_kernel_smem(2 * maxP));
+    if (e == cudaSuccess)
+        e = raise_smem_limit(reinterpret_cast<const void*>(nsga_order_kernel), (size_t)2 * maxP * 8);
+    if (e == cudaSuccess)
+        e = raise_smem_limit(reinterpret_cast<const void*>(near_build_kernel), (size_t)((maxP + 31) / 32) * 32 * 8);
     return e;
+}
+
+// two-objective dominance rows of up to maxN points per population (grid.y)
+static cudaError_t launch_dom2(const DomArgs& a, int maxN, int npops, cudaStream_t st) {
+    constexpr int RPC = kDom2Rows * kDom2Warps;
+    const size_t smem = (size_t)((maxN + 31) / 32) * 32 * sizeof(float2);
+    cudaError_t e = raise_smem_limit(reinterpret_cast<const void*>(dom2_build_kernel), smem);
+    if (e != cudaSuccess) return e;
+    dom2_build_kernel<<<dim3((maxN + RPC - 1) / RPC, npops), kDom2Warps * 32, smem, st>>>(a);
+    return cudaGetLastError();
 }
 
 static cudaError_t launch_dom(PopDesc* dd, int npops, int maxN, int pool, int only_rebuilt, cudaStream_t st) {
@@ -606,9 +882,7 @@ static cudaError_t launch_dom(PopDesc* dd, int npops, int maxN, int pool, int on
     a.dd = dd;
     a.pool = pool;
     a.only_rebuilt = only_rebuilt;
-    dim3 grid((maxN + 7) / 8, npops);
-    dom_build_kernel<<<grid, 256, 0, st>>>(a);
-    return cudaGetLastError();
+    return launch_dom2(a, maxN, npops, st);
 }
 
 // ranks, crowding and (mode 0) survivors of every population of the group
@@ -616,6 +890,11 @@ cudaError_t nsga_enqueue_select(PopDesc* dd, int npops, int maxP, int mode, cuda
     const int maxN = (mode == 0) ? 2 * maxP : maxP;
     cudaError_t e = launch_dom(dd, npops, maxN, mode == 0 ? 1 : 0, mode == 2 ? 1 : 0, st);
     if (e != cudaSuccess) return e;
+    nsga_peel_kernel<<<npops, kNsgaBlock, peel_kernel_smem(maxN), st>>>(dd, mode);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    nsga_order_kernel<<<dim3((maxN + kOrdPerCta - 1) / kOrdPerCta, 2, npops), kOrdThreads, (size_t)maxN * 8, st>>>(
+        dd, mode);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
     nsga_select_kernel<<<npops, kNsgaBlock, sel_smem_bytes(maxN), st>>>(dd, mode);
     return cudaGetLastError();
 }
@@ -630,7 +909,12 @@ cudaError_t nsga_enqueue_gather_finish(PopDesc* dd, int npops, int maxP, int max
 }
 
 cudaError_t nsga_enqueue_diversity(PopDesc* dd, int npops, int maxP, cudaStream_t st) {
-    nsga_diversity_kernel<<<npops, kNsgaBlock, (size_t)maxP * 8, st>>>(dd);
+    constexpr int RPC = kNearWarps * kNearRows;
+    const size_t smem = (size_t)((maxP + 31) / 32) * 32 * sizeof(float2);
+    near_build_kernel<<<dim3((maxP + RPC - 1) / RPC, npops), kNearWarps * 32, smem, st>>>(dd);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    nsga_diversity_kernel<<<npops, kNsgaBlock, 0, st>>>(dd);
     return cudaGetLastError();
 }
 
@@ -659,6 +943,8 @@ int32_t nsga_alloc(PopDesc& d, int P, double mut_rate, int div_interval, int Mn,
     d.domcnt = (int32_t*)p;
     if ((st = get(16, &p)) != BRKGA_OK) return st;
     d.nu = (int32_t*)p;
+    if ((st = get((size_t)2 * N * 4, &p)) != BRKGA_OK) return st;
+    d.nord = (int32_t*)p;
     d.domW = W;
     d.Mn = Mn;
     d.mutT = prob_threshold(mut_rate);
@@ -935,8 +1221,13 @@ int32_t brkga_pareto_rank_bitmatrix(const float* d_obj, int32_t N, int32_t m, in
     a.S = (uint32_t*)buf;
     a.cnt = (int32_t*)((char*)buf + sbytes);
     a.Wmax = W;
-    dom_build_kernel<<<(N + 7) / 8, 256, 0, st>>>(a);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e;
+    if (m == 2) {
+        e = launch_dom2(a, N, 1, st);
+    } else {
+        dom_build_kernel<<<(N + 7) / 8, 256, 0, st>>>(a);
+        e = cudaGetLastError();
+    }
     if (e != cudaSuccess) return cuda_fail(e, "dominance launch");
     const size_t smem = (((size_t)N * 2 + 15) / 16) * 16 + peel_smem_bytes(N);
     if ((e = raise_smem_limit(reinterpret_cast<const void*>(peel_op_kernel), smem)) != cudaSuccess)
