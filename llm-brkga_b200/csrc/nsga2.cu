@@ -25,6 +25,8 @@
 #include <string>
 #include <vector>
 
+#include <cooperative_groups.h>
+
 #include "engine.h"
 #include "nsga2.h"
 
@@ -594,18 +596,178 @@ __device__ __forceinline__ bool select_active(const PopDesc& d, int mode) {
     return true;
 }
 
-// ranks by bit-sliced peeling, one CTA per population; ranks -> domcnt[0, N)
-__global__ void __launch_bounds__(kNsgaBlock) nsga_peel_kernel(PopDesc* dd, int mode) {
-    extern __shared__ __align__(16) unsigned char smem[];
+// Ranks by bit-sliced peeling on a cluster of kPeelCluster CTAs per population.  CTA c
+// owns columns [512c, 512c + 512) (16 words): their count planes, and for every front the
+// sum of the member rows' words over those columns.  The front masks are exchanged through
+// distributed shared memory with one cluster barrier per front, so the dominance rows are
+// read by eight SMs instead of one.  Ranks -> domcnt[0, N).
+constexpr int kPeelCluster = 8, kPeelWords = 16, kPeelThreads = 256;
+constexpr int kPeelSlices = kPeelThreads / kPeelWords, kPeelWarps = kPeelThreads / 32;
+
+__global__ void __cluster_dims__(kPeelCluster, 1, 1) __launch_bounds__(kPeelThreads)
+    nsga_peel_cluster_kernel(PopDesc* dd, int mode) {
+    namespace cg = cooperative_groups;
+    __shared__ uint32_t C[kCB][kPeelWords];  // count planes of the own words (two's complement)
+    __shared__ uint32_t A[kPeelWords], V[kPeelWords];
+    __shared__ uint32_t Floc[2][kPeelWords];  // own words of the next front, by front parity
+    __shared__ uint32_t Ffull[kPeelCluster * kPeelWords];
+    __shared__ uint16_t list[kMaxPool];
+    __shared__ uint32_t part[kPeelWarps][kDB][kPeelWords];
+    __shared__ uint16_t r16[kPeelWords * 32];
     __shared__ uint32_t wt32[32];
-    PopDesc& d = dd[blockIdx.x];
-    if (!select_active(d, mode)) return;
+    cg::cluster_group cluster = cg::this_cluster();
+    const int crank = (int)cluster.block_rank();
+    PopDesc& d = dd[blockIdx.x / kPeelCluster];
+    if (!select_active(d, mode)) return;  // the same decision in every CTA of the cluster
     const int N = (mode == 0) ? 2 * d.P : d.P;
-    uint16_t* r16 = reinterpret_cast<uint16_t*>(smem);
-    const PeelSmem ps = peel_carve(smem + (((size_t)N * 2 + 15) / 16) * 16, N);
-    peel_ranks<kNsgaBlock>(N, d.domS, d.domW, d.domcnt, r16, ps, wt32);
+    const int W = (N + 31) / 32;
+    const uint32_t* __restrict__ S = d.domS;
+    const int Wmax = d.domW;
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int w0 = crank * kPeelWords;
+    // domination counts of the own columns -> count planes
+    for (int wl = warp; wl < kPeelWords; wl += kPeelWarps) {
+        const int w = w0 + wl, i = 32 * w + lane;
+        const int c = (w < W && i < N) ? __ldg(d.domcnt + i) : 0;
+#pragma unroll
+        for (int b = 0; b < kCB; ++b) {
+            const uint32_t pl = __ballot_sync(0xffffffffu, (c >> b) & 1);
+            if (lane == 0) C[b][wl] = pl;
+        }
+        const uint32_t v = __ballot_sync(0xffffffffu, w < W && i < N);
+        if (lane == 0) V[wl] = v;
+    }
     __syncthreads();
-    for (int i = threadIdx.x; i < N; i += kNsgaBlock) d.domcnt[i] = r16[i];
+    // first front: zero counts
+    if (t < kPeelWords) {
+        uint32_t z = V[t];
+#pragma unroll
+        for (int b = 0; b < kCB; ++b) z &= ~C[b][t];
+        A[t] = z;
+        Floc[0][t] = z;
+        for (uint32_t x = z; x; x &= x - 1) r16[32 * t + __ffs(x) - 1] = 0;
+    }
+    cluster.sync();
+    constexpr int NW = kPeelCluster * kPeelWords;
+    for (int k = 0; k < N; ++k) {
+        // the whole front k, gathered from every CTA of the cluster
+        if (t < NW) {
+            const uint32_t* rem = cluster.map_shared_rank(&Floc[k & 1][0], t / kPeelWords);
+            Ffull[t] = rem[t % kPeelWords];
+        }
+        __syncthreads();
+        const uint32_t pc = (t < NW) ? __popc(Ffull[t]) : 0u;
+        uint32_t nf = 0;
+        uint32_t base = block_exclusive_scan<kPeelThreads>(pc, wt32, &nf);
+        if (t < NW)
+            for (uint32_t x = Ffull[t]; x; x &= x - 1) list[base++] = (uint16_t)(32 * t + __ffs(x) - 1);
+        __syncthreads();
+        if (nf == 0) break;  // every CTA sees the same front
+        // column sums over the front's rows: thread (word t % 16, slice t / 16); the member
+        // rows' words are loaded eight at a time into 4-plane counters
+        const int wl = t % kPeelWords, sl = t / kPeelWords, w = w0 + wl;
+        uint32_t acc[kDB];
+#pragma unroll
+        for (int b = 0; b < kDB; ++b) acc[b] = 0u;
+        if (w < W) {
+            constexpr int kBatch = 8;
+            for (int j0 = sl; j0 < (int)nf; j0 += kBatch * kPeelSlices) {
+                uint32_t xs[kBatch];
+#pragma unroll
+                for (int u = 0; u < kBatch; ++u) {
+                    const int j = j0 + u * kPeelSlices;
+                    xs[u] = (j < (int)nf) ? __ldg(S + (size_t)list[j] * Wmax + w) : 0u;
+                }
+                uint32_t s0 = 0u, s1 = 0u, s2 = 0u, s3 = 0u;
+#pragma unroll
+                for (int u = 0; u < kBatch; ++u) {
+                    const uint32_t c0 = s0 & xs[u];
+                    s0 ^= xs[u];
+                    const uint32_t c1 = s1 & c0;
+                    s1 ^= c0;
+                    const uint32_t c2 = s2 & c1;
+                    s2 ^= c1;
+                    s3 ^= c2;
+                }
+                uint32_t cy = 0u;
+                const uint32_t sv[4] = {s0, s1, s2, s3};
+#pragma unroll
+                for (int b = 0; b < 4; ++b) {
+                    const uint32_t x = acc[b], y = sv[b];
+                    acc[b] = x ^ y ^ cy;
+                    cy = (x & y) | (cy & (x ^ y));
+                }
+#pragma unroll
+                for (int b = 4; b < kDB; ++b) {
+                    const uint32_t x = acc[b];
+                    acc[b] = x ^ cy;
+                    cy = x & cy;
+                }
+            }
+        }
+        {  // the two slices of a warp (lanes l and l ^ 16 share a word)
+            uint32_t cy = 0u;
+#pragma unroll
+            for (int b = 0; b < kDB; ++b) {
+                const uint32_t o = __shfl_xor_sync(0xffffffffu, acc[b], 16);
+                const uint32_t s2 = acc[b] ^ o ^ cy;
+                cy = (acc[b] & o) | (cy & (acc[b] ^ o));
+                acc[b] = s2;
+            }
+        }
+        if (lane < kPeelWords)
+#pragma unroll
+            for (int b = 0; b < kDB; ++b) part[warp][b][wl] = acc[b];
+        __syncthreads();
+        if (t < kPeelWords) {
+            uint32_t nz = 0u;
+            if (w0 + t < W) {
+                uint32_t sum[kDB];
+#pragma unroll
+                for (int b = 0; b < kDB; ++b) sum[b] = part[0][b][t];
+                for (int wp = 1; wp < kPeelWarps; ++wp) {
+                    uint32_t cy = 0u;
+#pragma unroll
+                    for (int b = 0; b < kDB; ++b) {
+                        const uint32_t x = sum[b], y = part[wp][b][t];
+                        sum[b] = x ^ y ^ cy;
+                        cy = (x & y) | (cy & (x ^ y));
+                    }
+                }
+                // decrement: doubled for the first front (its points are listed twice)
+                uint32_t dec[kCB];
+#pragma unroll
+                for (int b = 0; b < kCB; ++b) dec[b] = 0u;
+                if (k == 0) {
+#pragma unroll
+                    for (int b = 1; b < kCB; ++b) dec[b] = (b - 1 < kDB) ? sum[b - 1] : 0u;
+                } else {
+#pragma unroll
+                    for (int b = 0; b < kDB; ++b) dec[b] = sum[b];
+                }
+                uint32_t bor = 0u, any = 0u;
+#pragma unroll
+                for (int b = 0; b < kCB; ++b) {
+                    const uint32_t x = C[b][t];
+                    const uint32_t dd2 = x ^ dec[b] ^ bor;
+                    bor = (~x & dec[b]) | (~(x ^ dec[b]) & bor);
+                    C[b][t] = dd2;
+                    any |= dd2;
+                }
+                const uint32_t sign = C[kCB - 1][t];
+                nz = (sign | ~any) & ~A[t] & V[t];
+                A[t] |= nz;
+                for (uint32_t x = nz; x; x &= x - 1) r16[32 * t + __ffs(x) - 1] = (uint16_t)(k + 1);
+            }
+            Floc[(k + 1) & 1][t] = nz;
+        }
+        cluster.sync();
+    }
+    cluster.sync();  // no CTA leaves while another may still read its front words
+    for (int x = t; x < kPeelWords * 32; x += kPeelThreads) {
+        const int i = 32 * w0 + x;
+        if (i < N) d.domcnt[i] = r16[x];
+    }
 }
 
 // The pool ordered by (rank, objective o, index) for o = blockIdx.y, by exact counting:
@@ -853,12 +1015,8 @@ int nsga_max_population() { return kMaxPool / 2; }
 
 size_t nsga_select_smem(int maxP) { return sel_smem_bytes(2 * maxP); }
 
-static size_t peel_kernel_smem(int N) { return (((size_t)N * 2 + 15) / 16) * 16 + peel_smem_bytes(N); }
-
 cudaError_t nsga_prepare(int maxP) {
     cudaError_t e = raise_smem_limit(reinterpret_cast<const void*>(nsga_select_kernel), sel_smem_bytes(2 * maxP));
-    if (e == cudaSuccess)
-        e = raise_smem_limit(reinterpret_cast<const void*>(nsga_peel_kernel), peel_kernel_smem(2 * maxP));
     if (e == cudaSuccess)
         e = raise_smem_limit(reinterpret_cast<const void*>(nsga_order_kernel), (size_t)2 * maxP * 8);
     if (e == cudaSuccess)
@@ -890,7 +1048,7 @@ cudaError_t nsga_enqueue_select(PopDesc* dd, int npops, int maxP, int mode, cuda
     const int maxN = (mode == 0) ? 2 * maxP : maxP;
     cudaError_t e = launch_dom(dd, npops, maxN, mode == 0 ? 1 : 0, mode == 2 ? 1 : 0, st);
     if (e != cudaSuccess) return e;
-    nsga_peel_kernel<<<npops, kNsgaBlock, peel_kernel_smem(maxN), st>>>(dd, mode);
+    nsga_peel_cluster_kernel<<<npops * kPeelCluster, kPeelThreads, 0, st>>>(dd, mode);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     nsga_order_kernel<<<dim3((maxN + kOrdPerCta - 1) / kOrdPerCta, 2, npops), kOrdThreads, (size_t)maxN * 8, st>>>(
         dd, mode);
