@@ -179,22 +179,19 @@ def run_ours(args, rank, world):
 
     import brkga_b200 as B
 
+    from brkga_b200.replicas import Replicas, whole_job_rate
+
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(dev)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    reps = Replicas(backend="nccl")
 
     def barrier():
-        if dist is not None:
-            dist.barrier()
+        reps.barrier()
         torch.cuda.synchronize()
 
     xy = instance()
     pb = B.tsp(xy, device=dev)
-    prm = B.params(POP, ELITE, MUTANTS, RHO, E2E_GENERATIONS, seed=SEED_GA + rank, device=dev)
+    prm = B.params(POP, ELITE, MUTANTS, RHO, E2E_GENERATIONS, seed=reps.seed(SEED_GA), device=dev)
     s = B.Solver(pb, prm)
     s_info = s.info
     s.initialize()
@@ -224,12 +221,8 @@ def run_ours(args, rank, world):
                 ends[i].record(stream)
         s.synchronize()
         barrier()
-    ms = sum(a.elapsed_time(b) for a, b in zip(starts, ends))
-    if dist is not None:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * args.steps / (ms / 1e3)
+    ms = reps.max(sum(a.elapsed_time(b) for a, b in zip(starts, ends)))
+    value = whole_job_rate(world, args.steps, ms / 1e3)
     best = float(s.get_best_individual()[2])
 
     # --- dominant kernel alone: the fused row kernel through the generation-step entry point
@@ -306,12 +299,8 @@ def run_ours(args, rank, world):
                 for key, dt in (("create_ms", t1 - t0), ("run_ms", t2 - t1), ("get_best_ms", t3 - t2),
                                 ("destroy_ms", t4 - t3)):
                     phases[key] += 1e3 * dt / e2e_steps
-        tt = sum(times)
-        if dist is not None:
-            t = torch.tensor([tt], device=dev, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            tt = float(t.item())
-        e2e = {"value": world * e2e_steps * E2E_GENERATIONS / tt, "unit": "gens/s",
+        tt = reps.max(sum(times))
+        e2e = {"value": whole_job_rate(world, e2e_steps * E2E_GENERATIONS, tt), "unit": "gens/s",
                "h2d_bytes_per_step": int(xy.nbytes), "d2h_bytes_per_step": int(keys.nbytes + perm.nbytes + 4),
                "step": f"one {E2E_GENERATIONS}-generation solve through brkga_problem_create / brkga_create / "
                        f"brkga_run / brkga_get_best", "ms_per_solve": 1e3 * tt / e2e_steps,
@@ -347,9 +336,7 @@ def run_ours(args, rank, world):
             "l2_warm_back_to_back_gens_per_s": warm_gens_per_s,
         }
     s.close()
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    reps.close()
     return out
 
 
@@ -540,6 +527,81 @@ def workload_serve(args):
             "generations": gens, "max_active": args.max_active, "tick": args.tick}
 
 
+def reference_quality(xy, runs, gens):
+    """best tour length of `runs` runs of the reference's own Solver on its CPU path
+    (oracle/_ref, CUDA hidden); the reference seeds each run from the clock"""
+    code = f"""
+import json, sys
+sys.path[:0] = [{os.path.join(ROOT, 'oracle')!r}]
+import numpy as np
+import oracle as O
+if not O.ref_available():
+    print(json.dumps(None)); sys.exit(0)
+R = O.ref()
+xy = np.array({xy.tolist()!r}, dtype=np.float32)
+out = []
+for r in range({runs}):
+    h = R.ref_solver_create(1, {len(xy)}, xy.ctypes.data, None, None, None, 0.0, 256, 51, 25, 0.7)
+    R.ref_solver_evolve(h, {gens})
+    out.append(R.ref_solver_best(h))
+    R.ref_solver_destroy(h)
+print(json.dumps(out))
+"""
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES="")
+    r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=1800)
+    if r.returncode != 0:
+        return {"error": r.stderr[-500:]}
+    return json.loads(r.stdout.strip().splitlines()[-1])
+
+
+def _stats(v):
+    v = np.asarray(v, np.float64)
+    return {"mean": float(v.mean()), "std": float(v.std()), "min": float(v.min()), "max": float(v.max())}
+
+
+def workload_quality(args):
+    """Best tour over 32 seeds on the n=52 configuration (coordinates uniform in
+    [0,1000)^2 from seed 1, population 256, elite 51, mutants 25, rho 0.7, 500
+    generations): this engine (the 32 seeds as one batch, spot-checked against the plain
+    solver) beside the reference's own solver on its CPU path (32 runs)"""
+    import brkga_b200 as B
+    xy = np.random.default_rng(1).random((52, 2), dtype=np.float32) * np.float32(1000)
+    runs, gens = 32, args.generations
+    pb = B.tsp(xy)
+    prms = [B.params(256, 51, 25, 0.7, gens, seed=sd) for sd in range(1, runs + 1)]
+    t0 = time.perf_counter()
+    batch = B.Batch([pb] * runs, prms)
+    batch.evolve(gens)
+    batch.synchronize()
+    secs = time.perf_counter() - t0
+    ours = batch.best()[:, 0].astype(np.float64)
+    rel = []
+    for i in range(runs):
+        keys, _ = batch.best_keys(i)
+        pts = xy[np.argsort(keys, kind="stable")].astype(np.float64)
+        f64 = float(np.sum(np.sqrt(np.sum((pts - np.roll(pts, -1, axis=0)) ** 2, axis=1))))
+        rel.append(abs(ours[i] - f64) / f64)
+    batch.close()
+    same = 0
+    for i in range(0, runs, 8):
+        s = B.Solver(pb, prms[i])
+        s.run()
+        same += int(np.float32(s.get_best_individual()[2]) == np.float32(ours[i]))
+        s.close()
+    out = {"metric": "best tour over 32 seeds, TSP n=52 pop 256, 500 generations", "unit": "tour length",
+           "ours": _stats(ours), "ours_seconds_32_runs": secs, "ours_fp32_vs_fp64_max_rel": max(rel),
+           "plain_solver_identical": f"{same}/{len(range(0, runs, 8))}", "generations": gens}
+    if not args.no_cpu:
+        ref = reference_quality(xy, runs, gens)
+        if isinstance(ref, list):
+            out["reference"] = _stats(ref)
+            out["mean_ours_minus_reference_rel"] = (out["ours"]["mean"] - out["reference"]["mean"]) / \
+                out["reference"]["mean"]
+        else:
+            out["reference"] = ref
+    return out
+
+
 def run_workload(args):
     import torch
     torch.cuda.init()
@@ -564,6 +626,8 @@ def run_workload(args):
         out = workload_batch(args)
     elif w == "serve":
         out = workload_serve(args)
+    elif w == "quality":
+        out = workload_quality(args)
     else:
         raise SystemExit(f"unknown workload {w}")
     print(json.dumps(out))
@@ -602,7 +666,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--profile-op", action="store_true", help="operator kernels only (profiler captures)")
-    ap.add_argument("--workload", default="tsp1000", choices=["tsp1000", "tsp52", "nsga", "batch", "serve"])
+    ap.add_argument("--workload", default="tsp1000", choices=["tsp1000", "tsp52", "nsga", "batch", "serve", "quality"])
     ap.add_argument("--generations", type=int, default=500)
     ap.add_argument("--instances", type=int, default=256)
     ap.add_argument("--rate", type=float, default=200.0)

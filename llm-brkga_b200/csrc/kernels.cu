@@ -322,7 +322,12 @@ __global__ void __launch_bounds__(BLOCK, RowResidency<BLOCK, G>::value) row_kern
     int cur_pid = -1;
     zero_counters<BLOCK, G>(s);
 
-    for (int task = blockIdx.x; task < L.ntasks; task += gridDim.x) {
+    // tasks are dealt to CTAs in groups of K consecutive tasks, round robin: neighbouring
+    // rows of one population stay in one CTA (its descriptor and coordinates are staged
+    // once per group) while every CTA still gets a mix of the whole list
+    const int K = L.task_group > 1 ? L.task_group : 1;
+    for (int g0 = blockIdx.x * K; g0 < L.ntasks; g0 += gridDim.x * K)
+    for (int task = g0; task < min(L.ntasks, g0 + K); ++task) {
         int pid = 0, r = task;
         if (L.tasks) {
             const Task tk = L.tasks[task];

@@ -32,6 +32,7 @@ struct RowLaunch {
     int32_t max_n;           // largest chromosome among the populations launched
     int32_t max_points;      // largest coordinate count (n, or n+1 with a depot)
     int32_t stage_xy;        // stage coordinates in shared memory
+    int32_t task_group;      // tasks dealt to CTAs in groups of this many consecutive tasks (0, 1: one)
 };
 
 // smallest tile whose capacity (4 * block * groups) covers n
