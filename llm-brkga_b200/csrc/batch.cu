@@ -333,6 +333,9 @@ static int32_t make_member(std::shared_ptr<ProblemData> pd, const brkga_params& 
     Shape sh;
     int32_t st = make_shape(*pd, prm, &sh);
     if (st != BRKGA_OK) return st;
+    if (row_needs_global(pd->n, points_of(*pd), pd->kind))
+        return fail(BRKGA_ERR_UNSUPPORTED, "batched and served rows must fit the shared-memory row kernel (n = " +
+                                               std::to_string(pd->n) + " does not); solve it with brkga_create");
     auto* m = new Member;
     m->pd = pd;
     m->prm = prm;
@@ -790,6 +793,12 @@ int32_t brkga_server_submit(brkga_server* s, const brkga_problem_desc* desc, con
     if (params->max_generations <= 0) return fail(BRKGA_ERR_INVALID, "max_generations must be > 0");
     if (params->num_islands > 1) return fail(BRKGA_ERR_UNSUPPORTED, "served requests run one population each");
     if (desc->n < 1 || desc->n > row_max_n()) return fail(BRKGA_ERR_UNSUPPORTED, "chromosome length out of range");
+    {
+        const int pts = (desc->kind == BRKGA_BITSP_COORDS) ? desc->n + 1 : desc->n;
+        if (row_needs_global(desc->n, pts, desc->kind))
+            return fail(BRKGA_ERR_UNSUPPORTED, "served rows must fit the shared-memory row kernel (n = " +
+                                                   std::to_string(desc->n) + " does not)");
+    }
     auto* r = new Request;
     int32_t st = server_copy_desc(r, desc);
     if (st != BRKGA_OK) {

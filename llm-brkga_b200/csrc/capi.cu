@@ -61,9 +61,9 @@ int32_t make_problem(const brkga_problem_desc* d, int device, std::shared_ptr<Pr
     if (!d) return fail(BRKGA_ERR_INVALID, "null problem description");
     const int n = d->n;
     if (n < 1) return fail(BRKGA_ERR_INVALID, "chromosome length must be >= 1");
-    if (n > row_max_n())
+    if (n > row_max_n_global())
         return fail(BRKGA_ERR_UNSUPPORTED, "chromosome length " + std::to_string(n) + " exceeds " +
-                                               std::to_string(row_max_n()));
+                                               std::to_string(row_max_n_global()));
     auto pd = std::make_shared<ProblemData>();
     pd->device = device;
     pd->kind = d->kind;
@@ -279,6 +279,31 @@ int32_t brkga_problem_destroy(brkga_problem* pb) {
 int32_t brkga_problem_num_objectives(const brkga_problem* pb) { return pb ? pb->d->m : BRKGA_ERR_INVALID; }
 int32_t brkga_problem_maximize(const brkga_problem* pb) { return pb ? pb->d->maximize : BRKGA_ERR_INVALID; }
 
+}  // extern "C"
+
+namespace bk {
+// One row launch for an operator entry point: the in-shared-memory kernel, or, for rows
+// whose sort does not fit there, the global-scratch kernel with scratch taken from the
+// stream-ordered pool and returned to it behind the launch.
+static cudaError_t launch_op_rows(RowLaunch& L, const ProblemData& pd, cudaStream_t st) {
+    if (!row_needs_global(pd.n, points_of(pd), pd.kind)) {
+        const RowTile tile = pick_tile(pd.n);
+        L.stage_xy = stage_fits(tile, pd.n, L.max_points, pd.kind) ? 1 : 0;
+        return launch_rows_auto(L, pd.kind, tile, st);
+    }
+    const int grid = row_global_grid(L.ntasks, pd.n);
+    L.gstride = row_global_stride(pd.n);
+    void* p = nullptr;
+    if (dev_alloc(&p, L.gstride * grid, st) != BRKGA_OK) return cudaErrorMemoryAllocation;
+    L.gscratch = p;
+    const cudaError_t e = launch_rows(L, pd.kind, kGlobalTile, grid, st);
+    dev_free(p, st);
+    return e;
+}
+}  // namespace bk
+
+extern "C" {
+
 int32_t brkga_evaluate_population(brkga_problem* pb, const float* d_population, float* d_fitness,
                                   int32_t pop_size, int32_t chrom_len, int32_t ld, int32_t* d_perm,
                                   void* stream) {
@@ -304,9 +329,7 @@ int32_t brkga_evaluate_population(brkga_problem* pb, const float* d_population, 
     L.perm_out = d_perm;
     L.max_n = pd.n;
     L.max_points = points_of(pd);
-    const RowTile tile = pick_tile(pd.n);
-    L.stage_xy = stage_fits(tile, pd.n, L.max_points, pd.kind) ? 1 : 0;
-    cudaError_t e = launch_rows_auto(L, pd.kind, tile, (cudaStream_t)stream);
+    cudaError_t e = launch_op_rows(L, pd, (cudaStream_t)stream);
     if (e != cudaSuccess) return cuda_fail(e, "evaluate launch");
     return BRKGA_OK;
 }
@@ -369,10 +392,8 @@ int32_t brkga_generation_step(brkga_problem* pb, const float* d_pop, const float
     L.mode = MODE_GEN;
     L.max_n = pd.n;
     L.max_points = points_of(pd);
-    const RowTile tile = pick_tile(pd.n);
-    L.stage_xy = stage_fits(tile, pd.n, L.max_points, pd.kind) ? 1 : 0;
     DeviceGuard g(pd.device);
-    cudaError_t e = launch_rows_auto(L, pd.kind, tile, (cudaStream_t)stream);
+    cudaError_t e = launch_op_rows(L, pd, (cudaStream_t)stream);
     if (e != cudaSuccess) return cuda_fail(e, "generation launch");
     return BRKGA_OK;
 }
@@ -398,10 +419,8 @@ int32_t brkga_init_population(brkga_problem* pb, float* d_pop, float* d_fitness,
     L.mode = MODE_INIT;
     L.max_n = pd.n;
     L.max_points = points_of(pd);
-    const RowTile tile = pick_tile(pd.n);
-    L.stage_xy = stage_fits(tile, pd.n, L.max_points, pd.kind) ? 1 : 0;
     DeviceGuard g(pd.device);
-    cudaError_t e = launch_rows_auto(L, pd.kind, tile, (cudaStream_t)stream);
+    cudaError_t e = launch_op_rows(L, pd, (cudaStream_t)stream);
     if (e != cudaSuccess) return cuda_fail(e, "init launch");
     return BRKGA_OK;
 }

@@ -115,6 +115,8 @@ struct brkga_engine {
     int32_t* d_perm = nullptr;
     float* d_tmpfit = nullptr;
     NsgaState nsga;
+    void* gscratch = nullptr;  // sort scratch of the global-memory row kernel (rows beyond shared memory)
+    size_t gstride = 0;
 };
 
 static RowLaunch base_launch(brkga_engine* e, int mode) {
@@ -125,6 +127,8 @@ static RowLaunch base_launch(brkga_engine* e, int mode) {
     L.max_n = e->pop.sh.n;
     L.max_points = points_of(*e->pop.pd);
     L.stage_xy = e->stage ? 1 : 0;
+    L.gscratch = e->gscratch;
+    L.gstride = e->gstride;
     return L;
 }
 
@@ -331,15 +335,28 @@ int32_t brkga_create(brkga_problem* pbh, const brkga_params* params, brkga_engin
             L.stage_xy = tt.stage ? 1 : 0;
             return launch_rows(L, pd->kind, tt.tile, tt.grid, e->stream);
         };
-        TunedTile tt;
-        st = autotune_tile(pd->kind, sh.n, pts, sh.mo ? sh.Pi : e->nt_all, e->stream, launch, &tt);
-        if (st != BRKGA_OK) {
-            destroy_engine(e);
-            return st;
+        const int rows = sh.mo ? sh.Pi : e->nt_all;
+        if (row_needs_global(sh.n, pts, pd->kind)) {
+            // the row's sort does not fit in shared memory: global-scratch kernel
+            e->tile = kGlobalTile;
+            e->grid = row_global_grid(rows, sh.n);
+            e->stage = false;
+            e->gstride = row_global_stride(sh.n);
+            if ((st = dalloc(e->pop, &e->gscratch, e->gstride * e->grid)) != BRKGA_OK) {
+                destroy_engine(e);
+                return st;
+            }
+        } else {
+            TunedTile tt;
+            st = autotune_tile(pd->kind, sh.n, pts, rows, e->stream, launch, &tt);
+            if (st != BRKGA_OK) {
+                destroy_engine(e);
+                return st;
+            }
+            e->tile = tt.tile;
+            e->grid = tt.grid;
+            e->stage = tt.stage;
         }
-        e->tile = tt.tile;
-        e->grid = tt.grid;
-        e->stage = tt.stage;
     }
     err = prepare_sort(sh.mo ? 2 * sh.Pi : sh.Pi);
     if (err != cudaSuccess) {
@@ -352,6 +369,8 @@ int32_t brkga_create(brkga_problem* pbh, const brkga_params* params, brkga_engin
             destroy_engine(e);
             return st;
         }
+        e->nsga.gscratch = e->gscratch;
+        e->nsga.gstride = e->gstride;
     }
     *out = e;
     return BRKGA_OK;
@@ -578,6 +597,8 @@ int32_t brkga_get_best(brkga_engine* e, float* keys, int32_t* perm, float* fitne
         L.max_n = sh.n;
         L.max_points = points_of(pd);
         L.stage_xy = e->stage ? 1 : 0;
+        L.gscratch = e->gscratch;
+        L.gstride = e->gstride;
         cudaError_t err = launch_rows(L, pd.kind, e->tile, 1, e->stream);
         if (err == cudaSuccess) err = cudaStreamSynchronize(e->stream);
         if (err == cudaSuccess) err = cudaMemcpy(perm, e->d_perm, (size_t)sh.n * 4, cudaMemcpyDeviceToHost);

@@ -39,6 +39,8 @@ __host__ __device__ inline size_t align_up(size_t x, size_t a) { return (x + a -
 // bucket counters: 4 * groups * block buckets (>= n) plus a sentinel, padded to 16 bytes
 __host__ __device__ inline size_t cnt_words(int block, int groups) { return (size_t)4 * groups * block + 4; }
 
+constexpr size_t kRowSmemCap = 227 * 1024;  // opt-in dynamic shared memory per CTA
+
 size_t row_smem_bytes(const RowTile& t, int max_n, int max_points, int kind, bool stage_xy) {
     size_t b = align_up(cnt_words(t.block, t.groups) * 4, 16);
     b += align_up((size_t)max_n * 8, 16);
@@ -242,20 +244,20 @@ __device__ __forceinline__ long long block_excl_scan_ll(long long v, long long* 
 // knapsack greedy in key order: prefix of the sorted items that fits, then a
 // first-fit scan of the rest by warp 0 (weights must be >= 0)
 template <int BLOCK>
-__device__ float knap_greedy(const RowSmem& s, int n, const int32_t* __restrict__ w,
+__device__ float knap_greedy(const int32_t* perm, int n, const int32_t* __restrict__ w,
                              const int32_t* __restrict__ v, long long C, long long* red,
                              long long* shared_misc) {
     const int t = threadIdx.x;
     const int ch = (n + BLOCK - 1) / BLOCK;
     const int p0 = t * ch, p1 = min(n, p0 + ch);
     long long ws = 0;
-    for (int p = p0; p < p1; ++p) ws += __ldg(w + s.perm[p]);
+    for (int p = p0; p < p1; ++p) ws += __ldg(w + perm[p]);
     long long tot;
     const long long base = block_excl_scan_ll<BLOCK>(ws, red, &tot);
     // positions whose inclusive prefix weight stays <= C
     long long S = base, cnt = 0, val = 0, lastS = -1;
     for (int p = p0; p < p1; ++p) {
-        const int it = s.perm[p];
+        const int it = perm[p];
         S += __ldg(w + it);
         if (S <= C) {
             ++cnt;
@@ -273,8 +275,8 @@ __device__ float knap_greedy(const RowSmem& s, int n, const int32_t* __restrict_
         long long r = C - shared_misc[0];
         for (int b = (int)f + 1; b < n; b += 32) {
             const int pos = b + t;
-            const long long wl = (pos < n) ? (long long)__ldg(w + s.perm[pos]) : LLONG_MAX;
-            const long long vl = (pos < n) ? (long long)__ldg(v + s.perm[pos]) : 0ll;
+            const long long wl = (pos < n) ? (long long)__ldg(w + perm[pos]) : LLONG_MAX;
+            const long long vl = (pos < n) ? (long long)__ldg(v + perm[pos]) : 0ll;
             int cur = 0;
             for (;;) {
                 const unsigned mask = __ballot_sync(0xffffffffu, pos < n && t >= cur && wl <= r);
@@ -567,7 +569,7 @@ __global__ void __launch_bounds__(BLOCK, RowResidency<BLOCK, G>::value) row_kern
                         d[1] = __ldg(m1 + (size_t)a * np1 + b);
                     }, red_f, res);
                 } else if (kind == KNAP_GREEDY) {
-                    res[0] = knap_greedy<BLOCK>(s, n, sd.w, sd.v, sd.capi, red_ll, misc);
+                    res[0] = knap_greedy<BLOCK>(s.perm, n, sd.w, sd.v, sd.capi, red_ll, misc);
                 }
                 if (L.perm_out) {
                     int32_t* po = L.perm_out + (size_t)r * n;
@@ -577,6 +579,268 @@ __global__ void __launch_bounds__(BLOCK, RowResidency<BLOCK, G>::value) row_kern
             if (t == 0) dfit[(size_t)r * m] = res[0];
             if (t == 1 && m > 1) dfit[(size_t)r * m + 1] = res[1];
         }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// rows beyond shared memory: the same build, bucket argsort and canonical sums, with the
+// sort's counters, composites and permutation in a per-CTA slice of global scratch
+// (L2-resident at these sizes) and the keys re-read from the row between passes.  One CTA
+// of 1024 threads per row; results equal the in-shared-memory kernel's bit for bit (the
+// sort order and the summation order do not depend on the tile).
+// ---------------------------------------------------------------------------------------
+constexpr int kBigBlock = 1024;
+
+__host__ __device__ inline size_t big_cnt_bytes(int max_n) {
+    return align_up((size_t)(round_up(max_n, kBigBlock) + 1) * 4, 256);
+}
+__host__ __device__ inline size_t big_perm_bytes(int max_n) { return align_up((size_t)max_n * 4, 256); }
+
+size_t row_global_stride(int max_n) { return big_cnt_bytes(max_n) + big_perm_bytes(max_n) + align_up((size_t)max_n * 8, 256); }
+
+__global__ void __launch_bounds__(kBigBlock) row_kernel_big(RowLaunch L) {
+    constexpr int BLOCK = kBigBlock;
+    __shared__ PopDesc sd;
+    __shared__ uint32_t warp_tot[32];
+    __shared__ long long red_ll[32];
+    __shared__ float red_f[16];
+    __shared__ long long misc[4];
+    const int t = threadIdx.x;
+    unsigned char* base = static_cast<unsigned char*>(L.gscratch) + (size_t)blockIdx.x * L.gstride;
+    uint32_t* cnt = reinterpret_cast<uint32_t*>(base);                               // [NB + 1]
+    int32_t* perm = reinterpret_cast<int32_t*>(base + big_cnt_bytes(L.max_n));       // slots, then the permutation
+    unsigned long long* sc =
+        reinterpret_cast<unsigned long long*>(base + big_cnt_bytes(L.max_n) + big_perm_bytes(L.max_n));
+    const int NBmax = round_up(L.max_n, BLOCK);
+    for (int j = t; j <= NBmax; j += BLOCK) cnt[j] = 0u;
+    __syncthreads();
+    int cur_pid = -1;
+
+    for (int task = blockIdx.x; task < L.ntasks; task += gridDim.x) {
+        int pid = 0, r = task;
+        if (L.tasks) {
+            const Task tk = L.tasks[task];
+            pid = tk.pid;
+            r = tk.row;
+        }
+        if (pid != cur_pid) {
+            __syncthreads();
+            if (t == 0) sd = L.descs ? L.descs[pid] : L.single;
+            __syncthreads();
+            cur_pid = pid;
+        }
+        const int n = sd.n, ld = sd.ld, P = sd.P, E = sd.E, M = sd.M, m = sd.m;
+        const int cur = sd.cur;
+        if ((L.mode == MODE_GEN || L.mode == MODE_NSGA_OFF) && at_limit(sd)) continue;
+        if (L.mode == MODE_NSGA_REFILL && !sd.advanced) continue;
+        if (!L.tasks && L.mode == MODE_GEN) r = (task < P - E) ? E + task : task - (P - E);
+
+        enum { BUILD_LOAD, BUILD_COPY, BUILD_RANDOM, BUILD_CROSS, BUILD_NSGA };
+        int build = BUILD_LOAD;
+        float* dst = nullptr;
+        float* dfit = nullptr;
+        bool store = true;
+        const uint32_t isl = sd.island << 8;
+        uint32_t gdraw = 0, tag0 = 0;
+        const float* src = sd.keys[cur];
+        int pa = 0, pb = 0;
+        if (L.mode == MODE_GEN) {
+            dst = sd.keys[cur ^ 1];
+            dfit = sd.fit[cur ^ 1];
+            gdraw = sd.gen + 1;
+            if (r < E) {
+                build = BUILD_COPY;
+            } else if (r < P - M) {
+                build = BUILD_CROSS;  // core/solver.hpp:1109-1135
+                tag0 = isl | TAG_COIN;
+                int2 prk;
+                if (sd.parents) {
+                    prk = sd.parents[r];
+                } else {
+                    const uint4 pr = draw4(sd.seed, 0u, (uint32_t)r, gdraw, isl | TAG_PARENT);
+                    prk = make_int2((int)pick(pr.x, (uint32_t)E), E + (int)pick(pr.y, (uint32_t)(P - E)));
+                }
+                pa = __ldg(sd.sorted + prk.x);
+                pb = __ldg(sd.sorted + prk.y);
+            } else {
+                build = BUILD_RANDOM;  // core/solver.hpp:1244-1258
+                tag0 = isl | TAG_MUTANT;
+            }
+        } else if (L.mode == MODE_INIT) {
+            dst = sd.keys[cur];
+            dfit = sd.fit[cur];
+            build = BUILD_RANDOM;
+            tag0 = isl | TAG_INIT;
+        } else if (L.mode == MODE_NSGA_OFF) {
+            dst = sd.keys[cur] + (size_t)P * ld;
+            dfit = sd.fit[cur] + (size_t)P * m;
+            gdraw = sd.gen + 1;
+            if (r >= P - sd.Mn) {
+                build = BUILD_RANDOM;
+                tag0 = TAG_MUTANT;
+            } else {
+                build = BUILD_NSGA;
+                tag0 = TAG_NSGA_COIN;
+                const uint4 pk = draw4(sd.seed, 0u, (uint32_t)r, gdraw, TAG_NSGA_TOUR);
+                pa = tourn(pick(pk.x, P), pick(pk.y, P), sd.nrank, sd.ncd);
+                pb = tourn(pick(pk.z, P), pick(pk.w, P), sd.nrank, sd.ncd);
+            }
+        } else if (L.mode == MODE_NSGA_REFILL) {
+            if (r < __ldg(sd.nu)) continue;
+            dst = sd.keys[cur];
+            dfit = sd.fit[cur];
+            gdraw = sd.gen;
+            build = BUILD_RANDOM;
+            tag0 = TAG_NSGA_REFILL;
+        } else {
+            dfit = sd.fit[cur];
+            store = false;
+        }
+
+        if (build == BUILD_COPY) {
+            const int sr = __ldg(sd.sorted + r);
+            const float4* a = reinterpret_cast<const float4*>(src + (size_t)sr * ld);
+            float4* o = reinterpret_cast<float4*>(dst + (size_t)r * ld);
+            for (int q = t; q < ld / 4; q += BLOCK) o[q] = __ldg(a + q);
+            if (t < m) dfit[(size_t)r * m + t] = __ldg(sd.fit[cur] + (size_t)sr * m + t);
+            __syncthreads();
+            continue;
+        }
+        const float* row = src + (size_t)r * ld;
+        if (store) {
+            const float4* A = reinterpret_cast<const float4*>(src + (size_t)pa * ld);
+            const float4* Bv = reinterpret_cast<const float4*>(src + (size_t)pb * ld);
+            float4* o = reinterpret_cast<float4*>(dst + (size_t)r * ld);
+            for (int q = t; q < ld / 4; q += BLOCK) {
+                float k[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+                if (4 * q < n) {
+                    float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a;
+                    if (build != BUILD_RANDOM) {
+                        a = __ldg(A + q);
+                        b = __ldg(Bv + q);
+                    }
+                    const uint4 x = draw4(sd.seed, (uint32_t)q, (uint32_t)r, gdraw, tag0);
+                    if (build == BUILD_RANDOM) {
+                        k[0] = u24(x.x);
+                        k[1] = u24(x.y);
+                        k[2] = u24(x.z);
+                        k[3] = u24(x.w);
+                    } else {
+                        const uint32_t T = sd.rhoT;
+                        k[0] = ((x.x >> 8) < T) ? a.x : b.x;
+                        k[1] = ((x.y >> 8) < T) ? a.y : b.y;
+                        k[2] = ((x.z >> 8) < T) ? a.z : b.z;
+                        k[3] = ((x.w >> 8) < T) ? a.w : b.w;
+                    }
+                    if (build == BUILD_NSGA) {
+                        const uint4 mp = draw4(sd.seed, (uint32_t)q, (uint32_t)r, gdraw, TAG_NSGA_MUTP);
+                        const uint4 mk = draw4(sd.seed, (uint32_t)q, (uint32_t)r, gdraw, TAG_NSGA_MUTK);
+                        const uint32_t T = sd.mutT;
+                        if ((mp.x >> 8) < T) k[0] = u24(mk.x);
+                        if ((mp.y >> 8) < T) k[1] = u24(mk.y);
+                        if ((mp.z >> 8) < T) k[2] = u24(mk.z);
+                        if ((mp.w >> 8) < T) k[3] = u24(mk.w);
+                    }
+#pragma unroll
+                    for (int l = 0; l < 4; ++l)
+                        if (4 * q + l >= n) k[l] = 0.0f;
+                }
+                o[q] = make_float4(k[0], k[1], k[2], k[3]);
+            }
+            row = dst + (size_t)r * ld;
+        }
+        __syncthreads();  // the row's keys are visible to the whole block
+
+        float res[2] = {0.0f, 0.0f};
+        const int kind = sd.kind;
+        if (kind == KNAP_THRESHOLD) {
+            long long tw = 0, tv = 0;
+            for (int i = t; i < n; i += BLOCK)
+                if (row[i] > 0.5f) {
+                    tw += __ldg(sd.w + i);
+                    tv += __ldg(sd.v + i);
+                }
+            tw = block_sum_ll<BLOCK>(tw, red_ll);
+            tv = block_sum_ll<BLOCK>(tv, red_ll);
+            const float twf = (float)tw, tvf = (float)tv;
+            res[0] = (twf > sd.cap) ? __fsub_rn(tvf, __fmul_rn(__fsub_rn(twf, sd.cap), 1000.0f)) : tvf;
+        } else {
+            // stable argsort by (okey, index): bucket histogram, scan, scatter, rank in bucket
+            const int NB = round_up(n, BLOCK);
+            const float nbf = (float)NB;
+            for (int i = t; i < n; i += BLOCK) perm[i] = (int32_t)atomicAdd(&cnt[bucket_of(row[i], nbf, NB)], 1u);
+            __syncthreads();
+            {
+                const int ch = NB / BLOCK;
+                uint32_t sum = 0;
+                for (int j = t * ch; j < t * ch + ch; ++j) sum += cnt[j];
+                uint32_t run = block_exclusive_scan<BLOCK>(sum, warp_tot, nullptr);
+                for (int j = t * ch; j < t * ch + ch; ++j) {
+                    const uint32_t c = cnt[j];
+                    cnt[j] = run;
+                    run += c;
+                }
+                if (t == 0) cnt[NB] = (uint32_t)n;
+            }
+            __syncthreads();
+            for (int i = t; i < n; i += BLOCK) {
+                const float k = row[i];
+                sc[cnt[bucket_of(k, nbf, NB)] + (uint32_t)perm[i]] = ((unsigned long long)okey(k) << 32) | (uint32_t)i;
+            }
+            __syncthreads();
+            for (int i = t; i < n; i += BLOCK) {
+                const float k = row[i];
+                const int b = bucket_of(k, nbf, NB);
+                const uint32_t b0 = cnt[b], b1 = cnt[b + 1];
+                const unsigned long long me = ((unsigned long long)okey(k) << 32) | (uint32_t)i;
+                uint32_t rk = b0;
+                for (uint32_t q = b0; q < b1; ++q) rk += (sc[q] < me) ? 1u : 0u;
+                perm[rk] = i;
+            }
+            __syncthreads();
+            for (int j = t; j <= NB; j += BLOCK) cnt[j] = 0u;  // for the next row
+            if (kind == TSP_COORDS) {
+                const float* xy = sd.xy;
+                canon_sum<BLOCK, 1>(n, [&](int e, float* d) {
+                    const int a = perm[e], b = perm[(e + 1 < n) ? e + 1 : 0];
+                    d[0] = edge_xy(xy, a, b);
+                }, red_f, res);
+            } else if (kind == TSP_MATRIX) {
+                const float* mat = sd.mat;
+                canon_sum<BLOCK, 1>(n, [&](int e, float* d) {
+                    const int a = perm[e], b = perm[(e + 1 < n) ? e + 1 : 0];
+                    d[0] = __ldg(mat + (size_t)a * n + b);
+                }, red_f, res);
+            } else if (kind == BITSP_COORDS) {
+                const float* xy0 = sd.xy;
+                const float* xy1 = sd.xy2;
+                canon_sum<BLOCK, 2>(n + 1, [&](int e, float* d) {
+                    const int a = (e == 0) ? 0 : perm[e - 1] + 1;
+                    const int b = (e == n) ? 0 : perm[e] + 1;
+                    d[0] = edge_xy(xy0, a, b);
+                    d[1] = edge_xy(xy1, a, b);
+                }, red_f, res);
+            } else if (kind == BITSP_MATRIX) {
+                const float* m0 = sd.mat;
+                const float* m1 = sd.mat2;
+                const size_t np1 = (size_t)n + 1;
+                canon_sum<BLOCK, 2>(n + 1, [&](int e, float* d) {
+                    const int a = (e == 0) ? 0 : perm[e - 1] + 1;
+                    const int b = (e == n) ? 0 : perm[e] + 1;
+                    d[0] = __ldg(m0 + (size_t)a * np1 + b);
+                    d[1] = __ldg(m1 + (size_t)a * np1 + b);
+                }, red_f, res);
+            } else if (kind == KNAP_GREEDY) {
+                res[0] = knap_greedy<BLOCK>(perm, n, sd.w, sd.v, sd.capi, red_ll, misc);
+            }
+            if (L.perm_out) {
+                int32_t* po = L.perm_out + (size_t)r * n;
+                for (int i = t; i < n; i += BLOCK) po[i] = perm[i];
+            }
+        }
+        if (t == 0) dfit[(size_t)r * m] = res[0];
+        if (t == 1 && m > 1) dfit[(size_t)r * m + 1] = res[1];
         __syncthreads();
     }
 }
@@ -737,6 +1001,23 @@ RowTile pick_tile(int n) {
 
 int row_max_n() { return 4 * 1024 * 4; }
 
+int row_max_n_global() { return 1 << 22; }
+
+bool row_needs_global(int n, int pts, int kind) {
+    if (n > row_max_n()) return true;
+    const RowTile t = pick_tile(n);
+    return row_smem_bytes(t, n, pts, kind, false) > kRowSmemCap;
+}
+
+int row_global_grid(int rows, int max_n) {
+    const size_t budget = (size_t)2 << 30;  // scratch for at most 2 GiB of CTAs
+    int g = 2 * device_sm_count();
+    const size_t by_mem = budget / row_global_stride(max_n);
+    if ((size_t)g > by_mem) g = (int)by_mem;
+    if (g > rows) g = rows;
+    return g < 1 ? 1 : g;
+}
+
 using RowFn = void (*)(RowLaunch);
 
 static RowFn row_fn(const RowTile& t) {
@@ -787,6 +1068,13 @@ cudaError_t prepare_rows(const RowTile& tile, size_t smem, int* per_sm) {
 }
 
 cudaError_t launch_rows(const RowLaunch& L, int kind, const RowTile& tile, int grid, cudaStream_t s) {
+    if (tile.block == 0) {  // rows beyond shared memory: global-scratch kernel
+        if (!L.gscratch || L.gstride < row_global_stride(L.max_n)) return cudaErrorInvalidValue;
+        if (L.ntasks <= 0 || grid <= 0) return cudaSuccess;
+        if (grid > L.ntasks) grid = L.ntasks;
+        row_kernel_big<<<grid, kBigBlock, 0, s>>>(L);
+        return cudaGetLastError();
+    }
     RowFn fn = row_fn(tile);
     if (!fn) return cudaErrorInvalidValue;
     if (L.ntasks <= 0 || grid <= 0) return cudaSuccess;

@@ -32,6 +32,8 @@ struct RowLaunch {
     int32_t max_n;           // largest chromosome among the populations launched
     int32_t max_points;      // largest coordinate count (n, or n+1 with a depot)
     int32_t stage_xy;        // stage coordinates in shared memory
+    void* gscratch;          // global-scratch kernel (RowTile{0,0}): grid slices of gstride bytes
+    size_t gstride;
     int32_t task_group;      // tasks dealt to CTAs in groups of this many consecutive tasks (0, 1: one)
 };
 
@@ -43,6 +45,14 @@ int tile_candidates(int n, RowTile* out, int cap);
 size_t row_smem_bytes(const RowTile& t, int max_n, int max_points, int kind, bool stage_xy);
 // largest n the in-shared-memory row kernel supports
 int row_max_n();
+// Rows whose sort does not fit in shared memory are decoded by a kernel with its sort
+// scratch in global memory: launch_rows with kGlobalTile and RowLaunch::gscratch /
+// gstride set (row_global_stride(max_n) bytes for each of the grid's CTAs).
+constexpr RowTile kGlobalTile{0, 0};
+int row_max_n_global();
+bool row_needs_global(int n, int pts, int kind);
+size_t row_global_stride(int max_n);
+int row_global_grid(int rows, int max_n);
 // one-time set-up for a tile / shared-memory size: raises the dynamic shared-memory limit
 // and returns the resident CTAs per SM (0 if the tile cannot run with that much memory)
 cudaError_t prepare_rows(const RowTile& tile, size_t smem, int* per_sm);

@@ -1154,6 +1154,8 @@ static RowLaunch nsga_rows(const NsgaState& s, int mode) {
     L.max_n = s.n;
     L.max_points = s.max_points;
     L.stage_xy = s.stage ? 1 : 0;
+    L.gscratch = s.gscratch;
+    L.gstride = s.gstride;
     return L;
 }
 
@@ -1259,6 +1261,8 @@ int32_t nsga_get_best(NsgaState& s, cudaStream_t st, float* keys, int32_t* perm,
         L.max_n = s.n;
         L.max_points = s.max_points;
         L.stage_xy = s.stage ? 1 : 0;
+        L.gscratch = s.gscratch;
+        L.gstride = s.gstride;
         e = launch_rows(L, s.kind, s.tile, 1, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e == cudaSuccess) e = cudaMemcpy(perm, tmpp, (size_t)s.n * 4, cudaMemcpyDeviceToHost);

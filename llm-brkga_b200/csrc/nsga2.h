@@ -21,6 +21,8 @@ struct NsgaState {
     int hist_cap = 0;
     int div_interval = 0;
     bool ready = false;
+    void* gscratch = nullptr;  // global-memory row kernel scratch (tile kGlobalTile)
+    size_t gstride = 0;
 };
 
 int32_t nsga_setup(NsgaState& s, Population& pop, PopDesc* dd, PopDesc& hdesc, const RowTile& tile, int grid,
