@@ -40,14 +40,19 @@ typedef enum {
     BRKGA_KNAP_THRESHOLD = 3,    /* KnapsackConfig: gene > 0.5 selects, penalty x1000 (knapsack_config.hpp:43) */
     BRKGA_KNAP_GREEDY = 4,       /* key-order first-fit greedy knapsack (no reference counterpart)          */
     BRKGA_BITSP_COORDS = 5,      /* MultiTSPConfig with two coordinate sets, depot = point 0                */
-    BRKGA_BITSP_MATRIX = 6       /* MultiTSPConfig(dist, time, name) (configs/multi_tsp_config.hpp:25-52)   */
+    BRKGA_BITSP_MATRIX = 6,      /* MultiTSPConfig(dist, time, name) (configs/multi_tsp_config.hpp:25-52)   */
+    BRKGA_TSPJ = 7               /* TSPJConfig(travel, jobs, name): tour + job assignment, makespan
+                                    (configs/tspj_config.hpp:40-66, 555-626)                                */
 } brkga_problem_kind;
 
 /* Instance data (HOST pointers; copied to the device at creation).
  *   TSP:      n cities; coords [n][2] or matrix [n][n]
  *   bi-TSP:   n genes, n+1 points with point 0 the depot; coords/coords2 [n+1][2] or
  *             matrix/matrix2 [n+1][n+1]
- *   knapsack: n items; weights, values [n] (integers); capacity                        */
+ *   knapsack: n items; weights, values [n] (integers); capacity
+ *   TSPJ:     n cities besides the depot (node 0) and n job types; matrix = travel times
+ *             [n+1][n+1], matrix2 = job durations [n+1][n+1] (row = city, column = job
+ *             type); chromosomes hold 2n keys, the n city keys then the n job keys      */
 typedef struct {
     int32_t kind;
     int32_t n;

@@ -21,7 +21,7 @@ LIB_PATH = os.path.join(PKG_DIR, "lib", "libbrkga_b200.so")
 REPO_DIR = os.path.dirname(PKG_DIR)
 HEADER_PATH = os.path.join(REPO_DIR, "include", "brkga_b200.h")
 
-TSP_COORDS, TSP_MATRIX, KNAP_THRESHOLD, KNAP_GREEDY, BITSP_COORDS, BITSP_MATRIX = 1, 2, 3, 4, 5, 6
+TSP_COORDS, TSP_MATRIX, KNAP_THRESHOLD, KNAP_GREEDY, BITSP_COORDS, BITSP_MATRIX, TSPJ = 1, 2, 3, 4, 5, 6, 7
 
 STATUS = {0: "OK", -1: "INVALID", -2: "OOM", -3: "CUDA", -4: "TIMEOUT", -5: "CANCELLED",
           -6: "UNSUPPORTED", -7: "BUSY", -8: "NOT_READY"}
@@ -174,7 +174,10 @@ class Problem:
                         arr(matrix2, np.float32), arr(weights, np.int32), arr(values, np.int32), float(capacity))
         h = C.c_void_p()
         check(lib().brkga_problem_create(C.byref(d), device, C.byref(h)))
-        self.h, self.kind, self.n, self.device = h, kind, n, device
+        # n is the chromosome length (genes); a TSPJ instance of c cities has 2c genes
+        self.h, self.kind, self.device = h, kind, device
+        self.n = 2 * n if kind == TSPJ else n
+        self.cities = n
         self.capacity = capacity
 
     @property
@@ -228,6 +231,13 @@ def bitsp(coords, coords2, device=0):
 def bitsp_matrix(matrix, matrix2, device=0):
     matrix = np.asarray(matrix, np.float32)
     return Problem(BITSP_MATRIX, matrix.shape[0] - 1, matrix=matrix, matrix2=matrix2, device=device)
+
+
+def tspj(travel, jobs, device=0):
+    """TSPJ (TSPJConfig): travel times and job durations over the depot and c cities,
+    both [c+1][c+1]; chromosomes hold 2c keys (city keys, then job keys)"""
+    travel = np.asarray(travel, np.float32)
+    return Problem(TSPJ, travel.shape[0] - 1, matrix=travel, matrix2=jobs, device=device)
 
 
 def params(population_size=100, elite_size=20, mutant_size=10, elite_prob=0.7, max_generations=1000, seed=1,

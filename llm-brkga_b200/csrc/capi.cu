@@ -61,8 +61,9 @@ int32_t make_problem(const brkga_problem_desc* d, int device, std::shared_ptr<Pr
     if (!d) return fail(BRKGA_ERR_INVALID, "null problem description");
     const int n = d->n;
     if (n < 1) return fail(BRKGA_ERR_INVALID, "chromosome length must be >= 1");
-    if (n > row_max_n_global())
-        return fail(BRKGA_ERR_UNSUPPORTED, "chromosome length " + std::to_string(n) + " exceeds " +
+    const long long genes = (d->kind == BRKGA_TSPJ) ? 2ll * n : (long long)n;
+    if (genes > row_max_n_global())
+        return fail(BRKGA_ERR_UNSUPPORTED, "chromosome length " + std::to_string(genes) + " exceeds " +
                                                std::to_string(row_max_n_global()));
     auto pd = std::make_shared<ProblemData>();
     pd->device = device;
@@ -112,6 +113,19 @@ int32_t make_problem(const brkga_problem_desc* d, int device, std::shared_ptr<Pr
         pd->w = (int32_t*)p;
         if (st == BRKGA_OK) st = upload(*pd, d->values, (size_t)n * 4, &p);
         pd->v = (int32_t*)p;
+        break;
+    }
+    case BRKGA_TSPJ: {
+        // TSPJConfig (configs/tspj_config.hpp:40-66): travel times and job durations over the
+        // depot and n cities; the chromosome is the n city keys followed by the n job keys
+        pd->m = 1;
+        if (!d->matrix || !d->matrix2) return fail(BRKGA_ERR_INVALID, "TSPJ needs travel and job matrices");
+        const size_t D = (size_t)n + 1;
+        st = upload(*pd, d->matrix, D * D * 4, &p);
+        pd->mat = (float*)p;
+        if (st == BRKGA_OK) st = upload(*pd, d->matrix2, D * D * 4, &p);
+        pd->mat2 = (float*)p;
+        pd->n = 2 * n;
         break;
     }
     default:

@@ -18,6 +18,7 @@ enum Kind : int32_t {
     KNAP_GREEDY = 4,
     BITSP_COORDS = 5,
     BITSP_MATRIX = 6,
+    TSPJ = 7,
 };
 
 // stream tags: Philox counter word 3 = (island << 8) | tag
@@ -84,8 +85,8 @@ struct PopDesc {
     int32_t kind, n, ld, m;   // m = number of objectives (1 or 2)
     const float* xy;          // TSP [n][2]; bi-TSP [n+1][2]
     const float* xy2;
-    const float* mat;         // TSP [n][n]; bi-TSP [n+1][n+1]
-    const float* mat2;
+    const float* mat;         // TSP [n][n]; bi-TSP [n+1][n+1]; TSPJ travel times [c+1][c+1] (n = 2c)
+    const float* mat2;        // bi-TSP second matrix; TSPJ job durations [c+1][c+1]
     const int32_t* w;
     const int32_t* v;
     float cap;                // knapsack capacity (threshold fitness, float like the reference)

@@ -79,11 +79,15 @@ __device__ __forceinline__ int bucket_of(float key, float nbf, int nb) {
 // Counters must be zero on entry; they are left holding bucket offsets (the caller
 // re-zeroes them while it no longer needs them).  Bucket count NB = 4 * G * BLOCK >= n,
 // thread t owns the contiguous buckets [4Gt, 4Gt + 4G) for the scan.
+// Keys [split, n) form a second segment sorted on its own (TSPJ's job keys after its city
+// keys): it takes the upper half of the buckets, so no bucket mixes the segments and
+// positions [split, n) of the permutation hold the second segment's order.
 template <int BLOCK, int G>
-__device__ void row_argsort(const float (&k)[G][4], int n, const RowSmem& s, uint32_t* warp_tot) {
+__device__ void row_argsort(const float (&k)[G][4], int n, int split, const RowSmem& s, uint32_t* warp_tot) {
     constexpr int KB = 4 * G, NB = KB * BLOCK;
     const int t = threadIdx.x;
-    const float nbf = (float)NB;
+    const int nbs = (split < n) ? NB / 2 : NB;
+    const float nbf = (float)nbs;
     uint32_t bs[G][4];  // (bucket << 16) | slot
 #pragma unroll
     for (int g = 0; g < G; ++g)
@@ -91,7 +95,7 @@ __device__ void row_argsort(const float (&k)[G][4], int n, const RowSmem& s, uin
         for (int l = 0; l < 4; ++l) {
             const int i = 4 * (t + g * BLOCK) + l;
             if (i < n) {
-                const int b = bucket_of(k[g][l], nbf, NB);
+                const int b = bucket_of(k[g][l], nbf, nbs) + ((i >= split) ? nbs : 0);
                 const uint32_t slot = atomicAdd(&s.cnt[b], 1u);
                 bs[g][l] = ((uint32_t)b << 16) | slot;
             }
@@ -290,6 +294,45 @@ __device__ float knap_greedy(const int32_t* perm, int n, const int32_t* __restri
     }
     __syncthreads();
     return (float)(v0 + vt);
+}
+
+// TSPJ makespan (configs/tspj_config.hpp:555-585): the city tour from the depot (node 0)
+// and back; at each position the arrival time plus the duration of the job type assigned
+// to that position; the larger of the tour length and the latest job completion.  perm[0,
+// c) is the city order (cities perm+1), perm[c, 2c) the job order (types perm-c+1).  One
+// warp adds in the reference's own sequential order, so the value equals the reference's
+// fitness function bit for bit.
+template <int BLOCK>
+__device__ float tspj_makespan(const int32_t* perm, int nc, const float* __restrict__ travel,
+                               const float* __restrict__ jobs, float* red) {
+    const int lane = threadIdx.x & 31;
+    if (threadIdx.x < 32) {
+        const size_t D = (size_t)nc + 1;
+        float run = 0.0f, mjc = 0.0f;
+        for (int c0 = 0; c0 < nc; c0 += 32) {
+            const int i = c0 + lane;
+            float e = 0.0f, jd = 0.0f;
+            if (i < nc) {
+                const int city = perm[i] + 1;
+                const int prev = (i == 0) ? 0 : perm[i - 1] + 1;
+                const int job = perm[nc + i] - nc + 1;
+                e = __ldg(travel + (size_t)prev * D + city);
+                jd = __ldg(jobs + (size_t)city * D + job);
+            }
+            const int cnt = min(32, nc - c0);
+            for (int q = 0; q < cnt; ++q) {
+                run = __fadd_rn(run, __shfl_sync(0xffffffffu, e, q));
+                const float jc = __fadd_rn(run, __shfl_sync(0xffffffffu, jd, q));
+                mjc = (mjc < jc) ? jc : mjc;
+            }
+        }
+        const float tt = __fadd_rn(run, __ldg(travel + (size_t)(perm[nc - 1] + 1) * D));
+        if (lane == 0) red[0] = (tt < mjc) ? mjc : tt;
+    }
+    __syncthreads();
+    const float v = red[0];
+    __syncthreads();
+    return v;
 }
 
 // ---------------------------------------------------------------------------------------
@@ -533,7 +576,7 @@ __global__ void __launch_bounds__(BLOCK, RowResidency<BLOCK, G>::value) row_kern
                 const float twf = (float)tw, tvf = (float)tv;
                 res[0] = (twf > sd.cap) ? __fsub_rn(tvf, __fmul_rn(__fsub_rn(twf, sd.cap), 1000.0f)) : tvf;
             } else {
-                row_argsort<BLOCK, G>(k, n, s, warp_tot);
+                row_argsort<BLOCK, G>(k, n, (kind == TSPJ) ? n / 2 : n, s, warp_tot);
                 zero_counters<BLOCK, G>(s);  // ready for the next row (separated by the row-end barrier)
                 const int32_t* perm = s.perm;
                 if (kind == TSP_COORDS) {
@@ -570,6 +613,8 @@ __global__ void __launch_bounds__(BLOCK, RowResidency<BLOCK, G>::value) row_kern
                     }, red_f, res);
                 } else if (kind == KNAP_GREEDY) {
                     res[0] = knap_greedy<BLOCK>(s.perm, n, sd.w, sd.v, sd.capi, red_ll, misc);
+                } else if (kind == TSPJ) {
+                    res[0] = tspj_makespan<BLOCK>(perm, n / 2, sd.mat, sd.mat2, red_f);
                 }
                 if (L.perm_out) {
                     int32_t* po = L.perm_out + (size_t)r * n;
@@ -768,8 +813,11 @@ __global__ void __launch_bounds__(kBigBlock) row_kernel_big(RowLaunch L) {
         } else {
             // stable argsort by (okey, index): bucket histogram, scan, scatter, rank in bucket
             const int NB = round_up(n, BLOCK);
-            const float nbf = (float)NB;
-            for (int i = t; i < n; i += BLOCK) perm[i] = (int32_t)atomicAdd(&cnt[bucket_of(row[i], nbf, NB)], 1u);
+            const int split = (kind == TSPJ) ? n / 2 : n;  // two segments: buckets split in halves
+            const int nbs = (split < n) ? NB / 2 : NB;
+            const float nbf = (float)nbs;
+            auto bucket = [&](float k, int i) { return bucket_of(k, nbf, nbs) + ((i >= split) ? nbs : 0); };
+            for (int i = t; i < n; i += BLOCK) perm[i] = (int32_t)atomicAdd(&cnt[bucket(row[i], i)], 1u);
             __syncthreads();
             {
                 const int ch = NB / BLOCK;
@@ -786,12 +834,12 @@ __global__ void __launch_bounds__(kBigBlock) row_kernel_big(RowLaunch L) {
             __syncthreads();
             for (int i = t; i < n; i += BLOCK) {
                 const float k = row[i];
-                sc[cnt[bucket_of(k, nbf, NB)] + (uint32_t)perm[i]] = ((unsigned long long)okey(k) << 32) | (uint32_t)i;
+                sc[cnt[bucket(k, i)] + (uint32_t)perm[i]] = ((unsigned long long)okey(k) << 32) | (uint32_t)i;
             }
             __syncthreads();
             for (int i = t; i < n; i += BLOCK) {
                 const float k = row[i];
-                const int b = bucket_of(k, nbf, NB);
+                const int b = bucket(k, i);
                 const uint32_t b0 = cnt[b], b1 = cnt[b + 1];
                 const unsigned long long me = ((unsigned long long)okey(k) << 32) | (uint32_t)i;
                 uint32_t rk = b0;
@@ -833,6 +881,8 @@ __global__ void __launch_bounds__(kBigBlock) row_kernel_big(RowLaunch L) {
                 }, red_f, res);
             } else if (kind == KNAP_GREEDY) {
                 res[0] = knap_greedy<BLOCK>(perm, n, sd.w, sd.v, sd.capi, red_ll, misc);
+            } else if (kind == TSPJ) {
+                res[0] = tspj_makespan<BLOCK>(perm, n / 2, sd.mat, sd.mat2, red_f);
             }
             if (L.perm_out) {
                 int32_t* po = L.perm_out + (size_t)r * n;

@@ -145,6 +145,56 @@ static float knap_threshold(const orc_problem* pb, const float* keys) {
     return tvf;
 }
 
+/* TSPJConfig::calculate_tspj_fitness (configs/tspj_config.hpp:555-585): perm[0, c) is the
+ * city order (city perm+1), perm[c, 2c) the job order (job type perm-c+1).  The travel
+ * time and the arrival times are the same sequential float sum; std::max is
+ * (a < b) ? b : a. */
+static float tspj_makespan(const orc_problem* pb, const int32_t* perm) {
+    int c = pb->n / 2;
+    size_t D = (size_t)c + 1;
+    float travel = 0.0f, mjc = 0.0f;
+    int cur = 0;
+    for (int i = 0; i < c; ++i) {
+        int city = perm[i] + 1, job = perm[c + i] - c + 1;
+        travel = travel + pb->mat[(size_t)cur * D + city];
+        float jc = travel + pb->mat2[(size_t)city * D + job];
+        mjc = (mjc < jc) ? jc : mjc;
+        cur = city;
+    }
+    float tt = travel + pb->mat[(size_t)cur * D];
+    return (tt < mjc) ? mjc : tt;
+}
+
+static double tspj_makespan64(const orc_problem* pb, const int32_t* perm) {
+    int c = pb->n / 2;
+    size_t D = (size_t)c + 1;
+    double travel = 0.0, mjc = 0.0;
+    int cur = 0;
+    for (int i = 0; i < c; ++i) {
+        int city = perm[i] + 1, job = perm[c + i] - c + 1;
+        travel += pb->mat[(size_t)cur * D + city];
+        double jc = travel + pb->mat2[(size_t)city * D + job];
+        if (mjc < jc) mjc = jc;
+        cur = city;
+    }
+    double tt = travel + pb->mat[(size_t)cur * D];
+    return (tt < mjc) ? mjc : tt;
+}
+
+/* the decode of one chromosome: one argsort, or for TSPJ one per component (city keys,
+ * then job keys: TSPJConfig::decode_solution_internal, configs/tspj_config.hpp:606-626),
+ * the second component's positions offset by c */
+void orc_decode_problem(const orc_problem* pb, const float* keys, int32_t* perm) {
+    if (pb->kind == ORC_TSPJ) {
+        int c = pb->n / 2;
+        orc_decode(keys, c, perm);
+        orc_decode(keys + c, c, perm + c);
+        for (int i = 0; i < c; ++i) perm[c + i] += c;
+    } else {
+        orc_decode(keys, pb->n, perm);
+    }
+}
+
 static float knap_greedy(const orc_problem* pb, const int32_t* perm) {
     /* first-fit in key order: take item iff the running weight stays <= capacity */
     int64_t cap = (int64_t)floor((double)pb->cap);
@@ -193,6 +243,7 @@ void orc_eval_perm(const orc_problem* pb, const int32_t* perm, const float* keys
     }
     case ORC_KNAP_THRESHOLD: out[0] = knap_threshold(pb, keys); break;
     case ORC_KNAP_GREEDY: out[0] = knap_greedy(pb, perm); break;
+    case ORC_TSPJ: out[0] = tspj_makespan(pb, perm); break;
     default: out[0] = NAN;
     }
 }
@@ -221,6 +272,8 @@ void orc_eval_perm_f64(const orc_problem* pb, const int32_t* perm, double* out) 
         }
         out[0] = s0;
         out[1] = s1;
+    } else if (pb->kind == ORC_TSPJ) {
+        out[0] = tspj_makespan64(pb, perm);
     } else {
         out[0] = NAN;
     }
@@ -241,7 +294,7 @@ void orc_evaluate(const orc_problem* pb, const float* keys, int rows, int ld, fl
     int32_t* perm = (int32_t*)malloc(sizeof(int32_t) * (size_t)(pb->n > 0 ? pb->n : 1));
     for (int r = 0; r < rows; ++r) {
         const float* k = keys + (size_t)r * ld;
-        if (pb->kind != ORC_KNAP_THRESHOLD) orc_decode(k, pb->n, perm);
+        if (pb->kind != ORC_KNAP_THRESHOLD) orc_decode_problem(pb, k, perm);
         orc_eval_perm(pb, perm, k, fit + (size_t)r * m);
     }
     free(perm);

@@ -68,7 +68,9 @@ enum {
     ORC_KNAP_THRESHOLD = 3,   /* key > 0.5, configs/knapsack_config.hpp:43-62           */
     ORC_KNAP_GREEDY = 4,      /* key-order first-fit greedy (no reference counterpart)  */
     ORC_BITSP_COORDS = 5,     /* depot tour, two coordinate sets [n+1][2]               */
-    ORC_BITSP_MATRIX = 6      /* depot tour, two [n+1][n+1] matrices, configs/multi_tsp_config.hpp:54-103 */
+    ORC_BITSP_MATRIX = 6,     /* depot tour, two [n+1][n+1] matrices, configs/multi_tsp_config.hpp:54-103 */
+    ORC_TSPJ = 7              /* n = 2c genes; mat = travel [c+1][c+1], mat2 = job durations [c+1][c+1],
+                                 configs/tspj_config.hpp:555-626                                       */
 };
 
 typedef struct {
@@ -97,6 +99,8 @@ float orc_edge(const float* xy, int a, int b);
 float orc_canon_sum(const float* d, int nedges);
 /* evaluate one decoded row; out has num_objectives entries (canonical FP32) */
 void orc_eval_perm(const orc_problem* pb, const int32_t* perm, const float* keys, float* out);
+/* the problem's decode of one chromosome (two argsorts for TSPJ, see orc_evaluate) */
+void orc_decode_problem(const orc_problem* pb, const float* keys, int32_t* perm);
 /* FP64 restatement of the same objective (tour lengths only), for error bounds */
 void orc_eval_perm_f64(const orc_problem* pb, const int32_t* perm, double* out);
 /* sequential FP32 tour sum in the reference's order (configs/tsp_config.hpp:186-190) */

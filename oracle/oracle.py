@@ -16,7 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liboracle.so")
 REF_PATH = os.path.join(HERE, "_ref", "libref.so")
 
-TSP_COORDS, TSP_MATRIX, KNAP_THRESHOLD, KNAP_GREEDY, BITSP_COORDS, BITSP_MATRIX = 1, 2, 3, 4, 5, 6
+TSP_COORDS, TSP_MATRIX, KNAP_THRESHOLD, KNAP_GREEDY, BITSP_COORDS, BITSP_MATRIX, TSPJ = 1, 2, 3, 4, 5, 6, 7
 
 _f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
 _f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
@@ -68,6 +68,7 @@ def lib():
         L.orc_canon_sum.restype = C.c_float
         L.orc_canon_sum.argtypes = [_f32p, C.c_int]
         L.orc_eval_perm.argtypes = [C.POINTER(Problem), _i32p, _f32p, _f32p]
+        L.orc_decode_problem.argtypes = [C.POINTER(Problem), _f32p, _i32p]
         L.orc_eval_perm_f64.argtypes = [C.POINTER(Problem), _i32p, _f64p]
         L.orc_tsp_len_seq.restype = C.c_float
         L.orc_tsp_len_seq.argtypes = [C.POINTER(Problem), _i32p]
@@ -157,6 +158,18 @@ def evaluate(pb: OracleProblem, keys, ld=None):
     fit = np.empty((rows, pb.m), np.float32)
     lib().orc_evaluate(C.byref(pb.s), keys, rows, ld, fit)
     return fit[:, 0].copy() if pb.m == 1 else fit
+
+
+def decode_problem(pb: OracleProblem, keys):
+    """the problem's own decode of each row (TSPJ: city order, then job order offset by c)"""
+    keys = np.ascontiguousarray(np.atleast_2d(keys), dtype=np.float32)
+    out = np.zeros((keys.shape[0], pb.n), np.int32)
+    for r in range(keys.shape[0]):
+        row = np.ascontiguousarray(keys[r, :pb.n])
+        p = np.zeros(pb.n, np.int32)
+        lib().orc_decode_problem(C.byref(pb.s), row, p)
+        out[r] = p
+    return out
 
 
 def eval_f64(pb: OracleProblem, perm):
@@ -283,6 +296,7 @@ def ref():
         R.ref_tsp_eval.argtypes = [C.c_void_p, C.c_void_p, C.c_int, _f32p, C.c_int, _f32p, C.c_void_p]
         R.ref_knap_eval.argtypes = [_f32p, _f32p, C.c_float, C.c_int, _f32p, C.c_int, _f32p]
         R.ref_bitsp_eval.argtypes = [_f32p, _f32p, C.c_int, _f32p, C.c_int, _f32p]
+        R.ref_tspj_eval.argtypes = [_f32p, _f32p, C.c_int, _f32p, C.c_int, _f32p, C.c_void_p]
         R.ref_pareto.argtypes = [_f32p, C.c_int, _i32p, _f32p]
         R.ref_nsga2_select.argtypes = [_f32p, C.c_int, C.c_int, _i32p]
         R.ref_brkga_generation.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_uint32,

@@ -49,6 +49,7 @@
 #include "configs/tsp_config.hpp"
 #include "configs/knapsack_config.hpp"
 #include "configs/multi_tsp_config.hpp"
+#include "configs/tspj_config.hpp"
 #undef private
 #undef protected
 
@@ -132,6 +133,34 @@ int ref_bitsp_eval(const float* m0, const float* m1, int dim, const float* keys,
             set_keys(ind, keys + (size_t)r * n, n);
             obj[2 * r] = cfg.objective_functions[0](ind);
             obj[2 * r + 1] = cfg.objective_functions[1](ind);
+        }
+        return 0;
+    } catch (...) {
+        return -1;
+    }
+}
+
+// TSPJConfig decode + makespan (configs/tspj_config.hpp:555-626); matrices are dim x dim
+// (depot + c cities), each key row holds the c city keys then the c job keys; perm gets
+// the city tour (cities 1..c) then the job order (types 1..c)
+int ref_tspj_eval(const float* travel, const float* jobs, int dim, const float* keys, int rows, float* fit,
+                  int32_t* perm) {
+    try {
+        TSPJConfig<float> cfg(flat_to_matrix(travel, dim), flat_to_matrix(jobs, dim), "ref");
+        const int c = dim - 1;
+        Individual<float> ind(std::vector<int>{c, c});
+        for (int r = 0; r < rows; r++) {
+            const float* row = keys + (size_t)r * 2 * c;
+            ind.chromosomes[0].assign(row, row + c);
+            ind.chromosomes[1].assign(row + c, row + 2 * c);
+            fit[r] = cfg.fitness_function(ind);
+            if (perm) {
+                auto sol = cfg.decoder(ind);
+                for (int i = 0; i < c; i++) {
+                    perm[(size_t)r * 2 * c + i] = (int32_t)sol[0][i];
+                    perm[(size_t)r * 2 * c + c + i] = (int32_t)sol[1][i];
+                }
+            }
         }
         return 0;
     } catch (...) {

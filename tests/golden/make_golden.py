@@ -2,7 +2,7 @@
 (hsaseendran/llm-brkga headers compiled into oracle/_ref/libref.so by oracle/Makefile) on
 seeded synthetic inputs.  Run in this container, where the reference tree exists:
 
-    make -C oracle ref && CUDA_VISIBLE_DEVICES= python tests/golden/make_golden.py
+    make -C oracle ref && CUDA_VISIBLE_DEVICES= python tests/golden/make_golden.py [name ...]
 
 The reference must see no GPU so that it takes its CPU path.  Inputs are seeded numpy
 draws (uniform coordinates and keys, uniform integer knapsack items); nothing is read
@@ -33,7 +33,11 @@ def main():
     out["select"] = RC.ref_select_case(N=200, P=100, seed=7)
     out["generation"] = RC.ref_generation_case(n=20, P=40, E=8, M=4, rho=0.7, seed=8)
     out["nsga_offspring"] = RC.ref_nsga_offspring_case(n=15, P=24, rho=0.7, seed=9)
+    out["tspj20"] = RC.ref_tspj_case(c=20, rows=16, seed=10)
+    only = sys.argv[1:]  # optional: names of the fixtures to (re)generate
     for name, d in out.items():
+        if only and name not in only:
+            continue
         np.savez_compressed(os.path.join(HERE, name + ".npz"), **d)
         print(name, {k: v.shape for k, v in d.items()})
 

@@ -36,3 +36,15 @@ def wild_keys(rows, n, seed):
     specials = np.array([0.0, -0.0, np.inf, -np.inf, 1.0, 0.5], np.float32)
     flat[idx] = specials[rng.integers(0, specials.size, idx.size)]
     return k
+
+
+def tspj_instance(c, seed):
+    """TSPJ data over the depot and c cities: travel times = Euclidean distances of seeded
+    points in [0,100)^2 (as the reference's *_TT.csv files hold), job durations uniform in
+    [1,100) per (city, job type), the depot row zero"""
+    rng = np.random.default_rng(seed)
+    xy = rng.random((c + 1, 2)) * 100.0
+    travel = np.sqrt(((xy[:, None, :] - xy[None, :, :]) ** 2).sum(-1)).astype(np.float32)
+    jobs = (1.0 + rng.random((c + 1, c + 1)) * 99.0).astype(np.float32)
+    jobs[0, :] = 0.0
+    return travel, jobs

@@ -159,6 +159,30 @@ def check_bitsp(d):
         assert np.max(np.abs(f64 - d["obj"][r]) / f64) <= 1e-5
 
 
+def ref_tspj_case(c, rows, seed, key_fn=None):
+    R = O.ref()
+    travel, jobs = I.tspj_instance(c, seed)
+    keys = (key_fn or I.keys)(rows, 2 * c, seed + 1)
+    fit = np.zeros(rows, np.float32)
+    perm = np.zeros((rows, 2 * c), np.int32)
+    assert R.ref_tspj_eval(travel, jobs, c + 1, keys, rows, fit, perm.ctypes.data) == 0
+    return dict(travel=travel, jobs=jobs, keys=keys, fit=fit, perm=perm)
+
+
+def check_tspj(d):
+    # the reference sums in sequence and so does the oracle: bit-exact makespans
+    c = d["keys"].shape[1] // 2
+    pb = O.OracleProblem(O.TSPJ, 2 * c, mat=d["travel"], mat2=d["jobs"])
+    perm = O.decode_problem(pb, d["keys"])
+    ref = d["perm"].copy()
+    ref[:, :c] -= 1       # reference cities 1..c -> key indices 0..c-1
+    ref[:, c:] += c - 1   # reference job types 1..c -> key indices c..2c-1
+    np.testing.assert_array_equal(perm, ref)
+    np.testing.assert_array_equal(O.evaluate(pb, d["keys"]).view(np.uint32), d["fit"].view(np.uint32))
+    f64 = np.array([O.eval_f64(pb, p)[0] for p in perm])
+    assert np.max(np.abs(f64 - d["fit"]) / np.maximum(f64, 1e-30)) <= 1e-5
+
+
 def check_pareto(d, crowd=True):
     rank = O.pareto_ranks(d["obj"])
     np.testing.assert_array_equal(rank, d["rank"])
@@ -213,6 +237,8 @@ LIVE = {
     "tsp_matrix": lambda: check_tsp(ref_tsp_matrix_case(40, 8, 3), matrix=True),
     "knap": lambda: [check_knap(ref_knap_case(n, 8, n)) for n in (1, 50, 5000)],
     "bitsp": lambda: [check_bitsp(ref_bitsp_case(n, 8, n)) for n in (1, 20, 300)],
+    "tspj": lambda: [check_tspj(ref_tspj_case(c, 8, 40 + c)) for c in (1, 2, 5, 52, 300)],
+    "tspj_ties": lambda: [check_tspj(ref_tspj_case(c, 8, 50 + c, key_fn=I.tied_keys)) for c in (6, 100)],
     "pareto": lambda: [check_pareto(ref_pareto_case(N, N, False)) for N in (1, 2, 3, 500, 4096)],
     "pareto_dup": lambda: [check_pareto(ref_pareto_case(N, N, True), crowd=False) for N in (64, 2048)],
     "select": lambda: [check_select(ref_select_case(N, N // 2, N)) for N in (40, 1000)],

@@ -60,6 +60,10 @@ def test_golden_tsp_matrix():
     RC.check_tsp(golden("tsp_matrix9"), matrix=True)
 
 
+def test_golden_tspj():
+    RC.check_tspj(golden("tspj20"))
+
+
 def test_golden_knapsack_threshold():
     RC.check_knap(golden("knap200"))
 
