@@ -79,6 +79,11 @@ typedef struct {
     int32_t device;              /* CUDA device ordinal                                       */
     int32_t diversity_interval;  /* NSGA-II ensure_minimum_diversity period (0 = off)         */
     double mutation_rate;        /* NSGA-II per-gene reset rate (<= 0: the reference's 5/n)   */
+    int32_t local_search_interval;     /* TSPJ random 2-opt local search after generation g when
+                                          g - 1 > 0 and (g - 1) % interval == 0; 0 = off
+                                          (core/solver.hpp:459-461, 562-615)                   */
+    int32_t local_search_individuals;  /* top ranks searched per island (at most its elite size) */
+    int32_t local_search_moves;        /* random segment reversals per individual              */
 } brkga_params;
 
 typedef struct brkga_problem brkga_problem;
@@ -136,6 +141,19 @@ int32_t brkga_generation_step(brkga_problem* pb, const float* d_pop, const float
  * for generation 0 and their fitness. */
 int32_t brkga_init_population(brkga_problem* pb, float* d_pop, float* d_fitness, int32_t P, int32_t ld,
                               uint64_t seed, int32_t island, void* stream);
+
+/* Random 2-opt local search on rows [0, num_to_improve) of d_pop (the elites, in rank
+ * order, as the reference's island loop leaves them): replaces
+ * TSPJConfig::apply_local_search_gpu (configs/tspj_config.hpp:72-136), i.e.
+ * random_2opt_kernel + evaluation + restore_if_worse_kernel (core/cuda_kernels.cuh:166-246).
+ * Each row's city keys get num_moves reversals of a random segment [i, j] (skipped when
+ * j - i < 2); the row and d_fitness[row] change only if the new makespan is lower.  Draws
+ * come from Philox keyed by seed at (move, row, generation, island).  TSPJ problems only;
+ * rows must fit the shared-memory row kernel.  ld = 0 means round_up(chrom_len, 4);
+ * d_pop must be 16-byte aligned with ld a multiple of 4. */
+int32_t brkga_local_search(brkga_problem* pb, float* d_pop, float* d_fitness, int32_t num_to_improve,
+                           int32_t chrom_len, int32_t ld, int32_t num_moves, uint64_t seed, uint32_t generation,
+                           int32_t island, void* stream);
 
 /* Pareto ranks of N points with m objectives (minimisation), d_obj [N][m].  Replaces
  * Population::fast_non_dominated_sort (core/population.hpp:409-440). */

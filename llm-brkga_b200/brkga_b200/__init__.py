@@ -43,7 +43,9 @@ class Params(C.Structure):
     _fields_ = [("population_size", C.c_int32), ("elite_size", C.c_int32), ("mutant_size", C.c_int32),
                 ("elite_prob", C.c_double), ("max_generations", C.c_int32), ("seed", C.c_uint64),
                 ("num_islands", C.c_int32), ("migration_interval", C.c_int32), ("num_migrants", C.c_int32),
-                ("device", C.c_int32), ("diversity_interval", C.c_int32), ("mutation_rate", C.c_double)]
+                ("device", C.c_int32), ("diversity_interval", C.c_int32), ("mutation_rate", C.c_double),
+                ("local_search_interval", C.c_int32), ("local_search_individuals", C.c_int32),
+                ("local_search_moves", C.c_int32)]
 
 
 class ServerConfig(C.Structure):
@@ -82,6 +84,7 @@ def lib():
         "brkga_generation_step": (_i32, [_vp, _vp, _vp, _vp, _vp, _vp, _i32, _i32, _i32, _d, _i32, _u64, _u32,
                                          _i32, _vp]),
         "brkga_init_population": (_i32, [_vp, _vp, _vp, _i32, _i32, _u64, _i32, _vp]),
+        "brkga_local_search": (_i32, [_vp, _vp, _vp, _i32, _i32, _i32, _i32, _u64, _u32, _i32, _vp]),
         "brkga_pareto_rank": (_i32, [_vp, _i32, _i32, _vp, _vp]),
         "brkga_pareto_rank_bitmatrix": (_i32, [_vp, _i32, _i32, _vp, _vp]),
         "brkga_pareto_rank_noalloc": (_i32, [_vp, _i32, _i32, _vp, _vp]),
@@ -242,9 +245,10 @@ def tspj(travel, jobs, device=0):
 
 def params(population_size=100, elite_size=20, mutant_size=10, elite_prob=0.7, max_generations=1000, seed=1,
            num_islands=1, migration_interval=0, num_migrants=0, device=0, diversity_interval=25,
-           mutation_rate=0.0):
+           mutation_rate=0.0, local_search_interval=0, local_search_individuals=100, local_search_moves=5):
     return Params(population_size, elite_size, mutant_size, elite_prob, max_generations, seed, num_islands,
-                  migration_interval, num_migrants, device, diversity_interval, mutation_rate)
+                  migration_interval, num_migrants, device, diversity_interval, mutation_rate,
+                  local_search_interval, local_search_individuals, local_search_moves)
 
 
 # ---------------------------------------------------------------------------------------
@@ -355,6 +359,12 @@ def generation_step(problem, d_pop, d_fit, d_sorted, d_next, d_next_fit, P, E, M
     check(lib().brkga_generation_step(problem.h, _dptr(d_pop), _dptr(d_fit), _dptr(d_sorted), _dptr(d_next),
                                       _dptr(d_next_fit), P, E, M, rho, ld, seed, generation, island,
                                       _stream(stream)))
+
+
+def local_search(problem, d_pop, d_fit, num_to_improve, num_moves, seed, generation, ld=0, island=0, stream=None):
+    """TSPJ random 2-opt on rows [0, num_to_improve) (brkga_local_search)"""
+    check(lib().brkga_local_search(problem.h, _dptr(d_pop), _dptr(d_fit), num_to_improve, problem.n, ld,
+                                   num_moves, seed, generation, island, _stream(stream)))
 
 
 def init_population(problem, d_pop, d_fit, P, ld, seed, island=0, stream=None):

@@ -333,6 +333,8 @@ static int32_t make_member(std::shared_ptr<ProblemData> pd, const brkga_params& 
     Shape sh;
     int32_t st = make_shape(*pd, prm, &sh);
     if (st != BRKGA_OK) return st;
+    if (pd->kind == BRKGA_TSPJ && prm.local_search_interval > 0)
+        return fail(BRKGA_ERR_UNSUPPORTED, "local search runs in brkga_create engines, not in batches or the server");
     if (row_needs_global(pd->n, points_of(*pd), pd->kind))
         return fail(BRKGA_ERR_UNSUPPORTED, "batched and served rows must fit the shared-memory row kernel (n = " +
                                                std::to_string(pd->n) + " does not); solve it with brkga_create");

@@ -273,6 +273,9 @@ void brkga_params_default(brkga_params* p) {
     p->device = 0;
     p->diversity_interval = 25;
     p->mutation_rate = 0.0;
+    p->local_search_interval = 0;  // off; the reference's island loop uses 2, 100, 5 (core/solver.hpp:166)
+    p->local_search_individuals = 100;
+    p->local_search_moves = 5;
 }
 
 int32_t brkga_problem_create(const brkga_problem_desc* desc, int32_t device, brkga_problem** out) {
@@ -409,6 +412,44 @@ int32_t brkga_generation_step(brkga_problem* pb, const float* d_pop, const float
     DeviceGuard g(pd.device);
     cudaError_t e = launch_op_rows(L, pd, (cudaStream_t)stream);
     if (e != cudaSuccess) return cuda_fail(e, "generation launch");
+    return BRKGA_OK;
+}
+
+int32_t brkga_local_search(brkga_problem* pb, float* d_pop, float* d_fitness, int32_t num_to_improve,
+                           int32_t chrom_len, int32_t ld, int32_t num_moves, uint64_t seed, uint32_t generation,
+                           int32_t island, void* stream) {
+    if (!pb || !d_pop || !d_fitness) return fail(BRKGA_ERR_INVALID, "null argument");
+    const ProblemData& pd = *pb->d;
+    if (pd.kind != BRKGA_TSPJ) return fail(BRKGA_ERR_UNSUPPORTED, "local search is defined for TSPJ problems");
+    if (chrom_len != pd.n)
+        return fail(BRKGA_ERR_INVALID, "chrom_len " + std::to_string(chrom_len) + " != problem size " +
+                                           std::to_string(pd.n));
+    if (num_to_improve < 0 || num_moves < 0) return fail(BRKGA_ERR_INVALID, "negative count");
+    if (ld <= 0) ld = round_up(pd.n, 4);
+    if (ld % 4 != 0 || ld < pd.n) return fail(BRKGA_ERR_INVALID, "ld must be a multiple of 4 and >= chrom_len");
+    if ((uintptr_t)d_pop & 15) return fail(BRKGA_ERR_INVALID, "buffer must be 16-byte aligned");
+    if (row_needs_global(pd.n, points_of(pd), pd.kind))
+        return fail(BRKGA_ERR_UNSUPPORTED, "local search needs rows that fit the shared-memory row kernel");
+    if (num_to_improve == 0 || num_moves == 0) return BRKGA_OK;
+    RowLaunch L;
+    std::memset(&L, 0, sizeof(L));
+    fill_instance(L.single, pd);
+    L.single.ld = ld;
+    L.single.keys[0] = d_pop;
+    L.single.fit[0] = d_fitness;
+    L.single.P = num_to_improve;
+    L.single.seed = seed;
+    L.single.island = (uint32_t)island;
+    L.single.gen = generation;
+    L.ntasks = num_to_improve;
+    L.mode = MODE_LSEARCH;
+    L.ls_moves = num_moves;
+    L.ls_force = 1;
+    L.max_n = pd.n;
+    L.max_points = points_of(pd);
+    DeviceGuard g(pd.device);
+    cudaError_t e = launch_op_rows(L, pd, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "local search launch");
     return BRKGA_OK;
 }
 

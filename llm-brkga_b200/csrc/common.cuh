@@ -32,6 +32,7 @@ enum Tag : uint32_t {
     TAG_NSGA_MUTP = 7,
     TAG_NSGA_MUTK = 8,
     TAG_NSGA_REFILL = 9,
+    TAG_LS = 10,
 };
 
 // ---------------------------------------------------------------------------------------
@@ -124,9 +125,16 @@ struct PopDesc {
     // unchanged by every kernel; `advanced` records whether the last generation ran
     uint32_t gen_limit;
     int32_t advanced;
+    // TSPJ random 2-opt local search period (0 = off)
+    int32_t ls_interval;
 };
 
 __host__ __device__ __forceinline__ bool at_limit(const PopDesc& d) { return d.gen_limit != 0u && d.gen >= d.gen_limit; }
+
+// local search after generation gen (the reference's counter is gen - 1, core/solver.hpp:459-460)
+__host__ __device__ __forceinline__ bool ls_due(const PopDesc& d) {
+    return d.ls_interval > 0 && d.gen >= 2u && ((d.gen - 1u) % (uint32_t)d.ls_interval) == 0u;
+}
 
 // ---------------------------------------------------------------------------------------
 // block collectives

@@ -117,6 +117,8 @@ struct brkga_engine {
     NsgaState nsga;
     void* gscratch = nullptr;  // sort scratch of the global-memory row kernel (rows beyond shared memory)
     size_t gstride = 0;
+    int ls_count = 0;          // TSPJ local search: top ranks searched per island (0 = off)
+    Task* d_tasks_ls = nullptr;
 };
 
 static RowLaunch base_launch(brkga_engine* e, int mode) {
@@ -147,6 +149,18 @@ static cudaError_t enqueue_brkga_gen(brkga_engine* e, bool mig) {
     if (err != cudaSuccess) return err;
     err = launch_sort_pops(e->dd, sh.k, sh.Pi, 1, e->stream);
     if (err != cudaSuccess) return err;
+    if (e->ls_count > 0) {
+        // random 2-opt on the best ranks when due (decided on the device from the generation
+        // counter, so captured graphs stay valid), then re-rank (core/solver.hpp:459-461)
+        RowLaunch Ls = base_launch(e, MODE_LSEARCH);
+        Ls.tasks = (sh.k > 1) ? e->d_tasks_ls : nullptr;
+        Ls.ntasks = sh.k * e->ls_count;
+        Ls.ls_moves = e->pop.prm.local_search_moves;
+        err = launch_rows(Ls, e->pop.pd->kind, e->tile, e->grid, e->stream);
+        if (err != cudaSuccess) return err;
+        err = launch_sort_pops_after_ls(e->dd, sh.k, sh.Pi, e->stream);
+        if (err != cudaSuccess) return err;
+    }
     if (mig) {
         err = launch_migrate(e->dd, 1, sh.k, e->pop.prm.num_migrants, sh.n, e->stream);
         if (err != cudaSuccess) return err;
@@ -285,6 +299,17 @@ int32_t brkga_create(brkga_problem* pbh, const brkga_params* params, brkga_engin
         d.cur = 0;
         d.gen = 0;
     }
+    // TSPJ random 2-opt local search (the reference runs it in its island loop on
+    // problems whose config has one: TSPJConfig, configs/tspj_config.hpp:69-136)
+    if (!sh.mo && pd->kind == BRKGA_TSPJ && params->local_search_interval > 0 &&
+        params->local_search_individuals > 0 && params->local_search_moves > 0) {
+        if (row_needs_global(sh.n, points_of(*pd), pd->kind)) {
+            destroy_engine(e);
+            return fail(BRKGA_ERR_UNSUPPORTED, "local search needs rows that fit the shared-memory row kernel");
+        }
+        e->ls_count = std::min(params->local_search_individuals, sh.Ei);
+        for (auto& d : e->hd) d.ls_interval = params->local_search_interval;
+    }
     // pool allocations and clears are ordered on the engine stream: complete them before
     // the synchronous uploads below touch the memory
     err = cudaStreamSynchronize(e->stream);
@@ -316,6 +341,17 @@ int32_t brkga_create(brkga_problem* pbh, const brkga_params* params, brkga_engin
         cudaMemcpy(p, ta.data(), ta.size() * sizeof(Task), cudaMemcpyHostToDevice);
         e->nt_gen = (int)tg.size();
         e->nt_all = (int)ta.size();
+        if (e->ls_count > 0) {
+            std::vector<Task> tl;
+            for (int i = 0; i < sh.k; ++i)
+                for (int q = 0; q < e->ls_count; ++q) tl.push_back({i, q});
+            if ((st = dalloc(e->pop, &p, tl.size() * sizeof(Task))) != BRKGA_OK) {
+                destroy_engine(e);
+                return st;
+            }
+            e->d_tasks_ls = (Task*)p;
+            cudaMemcpy(p, tl.data(), tl.size() * sizeof(Task), cudaMemcpyHostToDevice);
+        }
     } else {
         e->nt_gen = sh.Pi;
         e->nt_all = sh.Pi;

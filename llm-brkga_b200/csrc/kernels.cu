@@ -401,6 +401,13 @@ __global__ void __launch_bounds__(BLOCK, RowResidency<BLOCK, G>::value) row_kern
         if ((L.mode == MODE_GEN || L.mode == MODE_NSGA_OFF) && at_limit(sd)) continue;
         if (L.mode == MODE_NSGA_REFILL && !sd.advanced) continue;
         if (!L.tasks && L.mode == MODE_GEN) r = (task < P - E) ? E + task : task - (P - E);
+        // local search: task = rank q; the row is the q-th best (the operator form works on
+        // rows in rank order already)
+        const int lsq = r;
+        if (L.mode == MODE_LSEARCH) {
+            if (!L.ls_force && (!ls_due(sd) || at_limit(sd))) continue;
+            if (!L.ls_force) r = __ldg(sd.sorted + lsq);
+        }
 
         float k[G][4];
         float* dst = nullptr;
@@ -468,6 +475,12 @@ __global__ void __launch_bounds__(BLOCK, RowResidency<BLOCK, G>::value) row_kern
             gdraw = sd.gen;
             build = BUILD_RANDOM;
             tag0 = TAG_NSGA_REFILL;
+        } else if (L.mode == MODE_LSEARCH) {
+            // random 2-opt (core/cuda_kernels.cuh:166-246): the row is rewritten in place, and
+            // only when the search improved it
+            dst = sd.keys[cur];
+            dfit = sd.fit[cur];
+            store = false;
         } else {  // MODE_EVAL: given keys
             dfit = sd.fit[cur];
             store = false;
@@ -536,6 +549,46 @@ __global__ void __launch_bounds__(BLOCK, RowResidency<BLOCK, G>::value) row_kern
                     }
                 }
             }
+        }
+
+        if (L.mode == MODE_LSEARCH) {
+            // reverse random segments [i, j] of the city keys (the first n/2 genes), as the
+            // reference's random_2opt_kernel: i, j uniform over the cities, ordered, skipped
+            // when j - i < 2; the composites buffer is free until the decode
+            const int c = n / 2;
+            float* sk = reinterpret_cast<float*>(s.sc);
+#pragma unroll
+            for (int gg = 0; gg < G; ++gg)
+#pragma unroll
+                for (int l = 0; l < 4; ++l) {
+                    const int i = 4 * (t + gg * BLOCK) + l;
+                    if (i < c) sk[i] = k[gg][l];
+                }
+            __syncthreads();
+            for (int mv = 0; mv < L.ls_moves; ++mv) {
+                const uint4 x = draw4(sd.seed, (uint32_t)mv, (uint32_t)lsq, sd.gen, isl | TAG_LS);
+                int i = (int)pick(x.x, (uint32_t)c), j = (int)pick(x.y, (uint32_t)c);
+                if (i > j) {
+                    const int tmp = i;
+                    i = j;
+                    j = tmp;
+                }
+                if (j - i >= 2)
+                    for (int p = t; p < (j - i + 1) / 2; p += BLOCK) {
+                        const float u = sk[i + p];
+                        sk[i + p] = sk[j - p];
+                        sk[j - p] = u;
+                    }
+                __syncthreads();
+            }
+#pragma unroll
+            for (int gg = 0; gg < G; ++gg)
+#pragma unroll
+                for (int l = 0; l < 4; ++l) {
+                    const int i = 4 * (t + gg * BLOCK) + l;
+                    if (i < c) k[gg][l] = sk[i];
+                }
+            __syncthreads();
         }
 
         if (store) {
@@ -621,8 +674,30 @@ __global__ void __launch_bounds__(BLOCK, RowResidency<BLOCK, G>::value) row_kern
                     for (int i = t; i < n; i += BLOCK) po[i] = perm[i];
                 }
             }
-            if (t == 0) dfit[(size_t)r * m] = res[0];
-            if (t == 1 && m > 1) dfit[(size_t)r * m + 1] = res[1];
+            if (L.mode == MODE_LSEARCH) {
+                // keep the searched row only if it is better (restore_if_worse_kernel)
+                const float old = dfit[(size_t)r * m];
+                if (sd.maximize ? (res[0] > old) : (res[0] < old)) {
+                    __syncthreads();  // every thread has read the old value
+                    float4* o = reinterpret_cast<float4*>(dst + (size_t)r * ld);
+#pragma unroll
+                    for (int gg = 0; gg < G; ++gg) {
+                        const int q = t + gg * BLOCK;
+                        if (4 * q < ld) {
+                            float4 v;
+                            v.x = (4 * q + 0 < n) ? k[gg][0] : 0.0f;
+                            v.y = (4 * q + 1 < n) ? k[gg][1] : 0.0f;
+                            v.z = (4 * q + 2 < n) ? k[gg][2] : 0.0f;
+                            v.w = (4 * q + 3 < n) ? k[gg][3] : 0.0f;
+                            o[q] = v;
+                        }
+                    }
+                    if (t == 0) dfit[(size_t)r * m] = res[0];
+                }
+            } else {
+                if (t == 0) dfit[(size_t)r * m] = res[0];
+                if (t == 1 && m > 1) dfit[(size_t)r * m + 1] = res[1];
+            }
         }
         __syncthreads();
     }
@@ -680,6 +755,13 @@ __global__ void __launch_bounds__(kBigBlock) row_kernel_big(RowLaunch L) {
         if ((L.mode == MODE_GEN || L.mode == MODE_NSGA_OFF) && at_limit(sd)) continue;
         if (L.mode == MODE_NSGA_REFILL && !sd.advanced) continue;
         if (!L.tasks && L.mode == MODE_GEN) r = (task < P - E) ? E + task : task - (P - E);
+        // local search: task = rank q; the row is the q-th best (the operator form works on
+        // rows in rank order already)
+        const int lsq = r;
+        if (L.mode == MODE_LSEARCH) {
+            if (!L.ls_force && (!ls_due(sd) || at_limit(sd))) continue;
+            if (!L.ls_force) r = __ldg(sd.sorted + lsq);
+        }
 
         enum { BUILD_LOAD, BUILD_COPY, BUILD_RANDOM, BUILD_CROSS, BUILD_NSGA };
         int build = BUILD_LOAD;
@@ -911,6 +993,7 @@ struct RankArgs {
     const float* fit;     // raw mode: segments of P fitness values
     int32_t* sorted;
     int P, maximize, flip;
+    int only_ls;          // engine mode: only populations whose local search was due
 };
 
 __host__ __device__ inline int next_pow2(int x) {
@@ -929,6 +1012,7 @@ __global__ void __launch_bounds__(RK_THREADS) rank_kernel(RankArgs a) {
     uint32_t gen_new = 0;
     if (d) {
         if (a.flip && at_limit(*d)) return;
+        if (a.only_ls && (!ls_due(*d) || at_limit(*d))) return;
         P = d->P;
         mx = d->maximize;
         m = d->m;
@@ -1150,7 +1234,7 @@ cudaError_t prepare_sort(int maxP) {
 cudaError_t launch_sort_raw(const float* fit, int P, int segments, int maximize, int32_t* sorted,
                             cudaStream_t s) {
     if (P <= 0 || segments <= 0) return cudaSuccess;
-    RankArgs a{nullptr, fit, sorted, P, maximize, 0};
+    RankArgs a{nullptr, fit, sorted, P, maximize, 0, 0};
     dim3 grid((P + RK_CH - 1) / RK_CH, segments);
     rank_kernel<<<grid, RK_THREADS, (size_t)P * 8, s>>>(a);
     return cudaGetLastError();
@@ -1158,7 +1242,15 @@ cudaError_t launch_sort_raw(const float* fit, int P, int segments, int maximize,
 
 cudaError_t launch_sort_pops(PopDesc* descs, int npops, int maxP, int flip, cudaStream_t s) {
     if (npops <= 0) return cudaSuccess;
-    RankArgs a{descs, nullptr, nullptr, 0, 0, flip};
+    RankArgs a{descs, nullptr, nullptr, 0, 0, flip, 0};
+    dim3 grid((maxP + RK_CH - 1) / RK_CH, npops);
+    rank_kernel<<<grid, RK_THREADS, (size_t)maxP * 8, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sort_pops_after_ls(PopDesc* descs, int npops, int maxP, cudaStream_t s) {
+    if (npops <= 0) return cudaSuccess;
+    RankArgs a{descs, nullptr, nullptr, 0, 0, 0, 1};
     dim3 grid((maxP + RK_CH - 1) / RK_CH, npops);
     rank_kernel<<<grid, RK_THREADS, (size_t)maxP * 8, s>>>(a);
     return cudaGetLastError();

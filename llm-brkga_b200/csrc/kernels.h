@@ -8,7 +8,14 @@
 
 namespace bk {
 
-enum Mode : int32_t { MODE_INIT = 0, MODE_GEN = 1, MODE_EVAL = 2, MODE_NSGA_OFF = 3, MODE_NSGA_REFILL = 4 };
+enum Mode : int32_t {
+    MODE_INIT = 0,
+    MODE_GEN = 1,
+    MODE_EVAL = 2,
+    MODE_NSGA_OFF = 3,
+    MODE_NSGA_REFILL = 4,
+    MODE_LSEARCH = 5,  // TSPJ random 2-opt on the top ranks (task = rank)
+};
 
 // one unit of row work: population `pid`, row `row` of that population
 struct Task {
@@ -35,6 +42,8 @@ struct RowLaunch {
     void* gscratch;          // global-scratch kernel (RowTile{0,0}): grid slices of gstride bytes
     size_t gstride;
     int32_t task_group;      // tasks dealt to CTAs in groups of this many consecutive tasks (0, 1: one)
+    int32_t ls_moves;        // MODE_LSEARCH: segment reversals per individual
+    int32_t ls_force;        // MODE_LSEARCH: run whatever the generation (operator); rank q = row q
 };
 
 // smallest tile whose capacity (4 * block * groups) covers n
@@ -69,6 +78,8 @@ cudaError_t raise_smem_limit(const void* fn, size_t smem);
 // elite partition of raw fitness segments: sorted[seg*P + r]
 cudaError_t launch_sort_raw(const float* fit, int P, int segments, int maximize, int32_t* sorted,
                             cudaStream_t s);
+// re-rank after a local search pass: only populations for which it was due
+cudaError_t launch_sort_pops_after_ls(PopDesc* descs, int npops, int maxP, cudaStream_t s);
 // engine sort: for each population, sort fit[cur^flip]; when flip, swap buffers and gen++;
 // history[gen] = best
 cudaError_t launch_sort_pops(PopDesc* descs, int npops, int maxP, int flip, cudaStream_t s);

@@ -300,6 +300,31 @@ void orc_evaluate(const orc_problem* pb, const float* keys, int rows, int ld, fl
     free(perm);
 }
 
+void orc_local_search(const orc_problem* pb, float* pop, float* fit, const int32_t* rows, int count, int ld,
+                      int moves, uint64_t seed, uint32_t gen, int island) {
+    int c = pb->n / 2;
+    float* row = (float*)malloc(sizeof(float) * (size_t)(ld > 0 ? ld : 1));
+    for (int q = 0; q < count; ++q) {
+        int r = rows[q];
+        memcpy(row, pop + (size_t)r * ld, sizeof(float) * (size_t)ld);
+        for (int mv = 0; mv < moves; ++mv) {
+            uint32_t st = ((uint32_t)island << 8) | ORC_TAG_LS;
+            int i = (int)orc_pick(orc_draw(seed, (uint32_t)mv, (uint32_t)q, gen, st, 0), (uint32_t)c);
+            int j = (int)orc_pick(orc_draw(seed, (uint32_t)mv, (uint32_t)q, gen, st, 1), (uint32_t)c);
+            if (i > j) { int tmp = i; i = j; j = tmp; }
+            if (j - i < 2) continue;
+            while (i < j) { float u = row[i]; row[i] = row[j]; row[j] = u; ++i; --j; }
+        }
+        float f;
+        orc_evaluate(pb, row, 1, ld, &f);
+        if (orc_maximize(pb) ? (f > fit[r]) : (f < fit[r])) {
+            memcpy(pop + (size_t)r * ld, row, sizeof(float) * (size_t)ld);
+            fit[r] = f;
+        }
+    }
+    free(row);
+}
+
 /* ================================================================================ */
 /* BRKGA                                                                            */
 /* ================================================================================ */

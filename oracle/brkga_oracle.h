@@ -40,7 +40,8 @@ enum {
     ORC_TAG_NSGA_COIN = 6,  /* uniform crossover coins, core/solver.hpp:1058-1074   */
     ORC_TAG_NSGA_MUTP = 7,  /* per-gene mutation test, core/solver.hpp:1077-1091    */
     ORC_TAG_NSGA_MUTK = 8,  /* replacement key for a mutated gene                   */
-    ORC_TAG_NSGA_REFILL = 9 /* random refill of ensure_minimum_diversity            */
+    ORC_TAG_NSGA_REFILL = 9, /* random refill of ensure_minimum_diversity           */
+    ORC_TAG_LS = 10          /* TSPJ local search segments, core/cuda_kernels.cuh:188-195 */
 };
 
 /* draw word `lane` (0..3) of Philox block (word, row, gen, (island<<8)|tag) keyed by seed */
@@ -99,6 +100,13 @@ float orc_edge(const float* xy, int a, int b);
 float orc_canon_sum(const float* d, int nedges);
 /* evaluate one decoded row; out has num_objectives entries (canonical FP32) */
 void orc_eval_perm(const orc_problem* pb, const int32_t* perm, const float* keys, float* out);
+/* Random 2-opt local search (TSPJConfig::apply_local_search_gpu, configs/tspj_config.hpp:72-136,
+ * with random_2opt_kernel / restore_if_worse_kernel, core/cuda_kernels.cuh:166-246) on
+ * rows[0, count), the best ranks: `moves` reversals of a city-key segment [i, j] (i, j
+ * drawn over the c = n/2 cities at (move, q, gen, island<<8 | ORC_TAG_LS), ordered,
+ * skipped when j - i < 2); the row and fit[row] change only if the makespan improved. */
+void orc_local_search(const orc_problem* pb, float* pop, float* fit, const int32_t* rows, int count, int ld,
+                      int moves, uint64_t seed, uint32_t gen, int island);
 /* the problem's decode of one chromosome (two argsorts for TSPJ, see orc_evaluate) */
 void orc_decode_problem(const orc_problem* pb, const float* keys, int32_t* perm);
 /* FP64 restatement of the same objective (tour lengths only), for error bounds */

@@ -69,6 +69,8 @@ def lib():
         L.orc_canon_sum.argtypes = [_f32p, C.c_int]
         L.orc_eval_perm.argtypes = [C.POINTER(Problem), _i32p, _f32p, _f32p]
         L.orc_decode_problem.argtypes = [C.POINTER(Problem), _f32p, _i32p]
+        L.orc_local_search.argtypes = [C.POINTER(Problem), _f32p, _f32p, _i32p, C.c_int, C.c_int, C.c_int,
+                                       C.c_uint64, C.c_uint32, C.c_int]
         L.orc_eval_perm_f64.argtypes = [C.POINTER(Problem), _i32p, _f64p]
         L.orc_tsp_len_seq.restype = C.c_float
         L.orc_tsp_len_seq.argtypes = [C.POINTER(Problem), _i32p]
@@ -158,6 +160,12 @@ def evaluate(pb: OracleProblem, keys, ld=None):
     fit = np.empty((rows, pb.m), np.float32)
     lib().orc_evaluate(C.byref(pb.s), keys, rows, ld, fit)
     return fit[:, 0].copy() if pb.m == 1 else fit
+
+
+def local_search(pb: OracleProblem, pop, fit, rows, count, ld, moves, seed, gen, island=0):
+    """TSPJ random 2-opt on rows[:count] (in place)"""
+    lib().orc_local_search(C.byref(pb.s), pop, fit, np.ascontiguousarray(rows, np.int32), count, ld, moves,
+                           seed, gen, island)
 
 
 def decode_problem(pb: OracleProblem, keys):

@@ -67,3 +67,84 @@ def test_tspj_batch_equals_standalone(cuda):
         assert best[i, 0] == s.get_best_individual()[2]
         s.close()
     batch.close()
+
+
+def test_local_search_op(cuda):
+    """brkga_local_search on rows in rank order, against the oracle: same rows changed, same
+    keys and makespans"""
+    import torch
+    c, P, moves = 60, 48, 5
+    pb, po = problems(c, seed=30)
+    ld = (2 * c + 3) // 4 * 4
+    keys = np.zeros((P, ld), np.float32)
+    keys[:, :2 * c] = I.keys(P, 2 * c, seed=31)
+    fit = O.evaluate(po, keys, ld)
+    d_pop = torch.from_numpy(keys.copy()).to(cuda)
+    d_fit = torch.from_numpy(fit.copy()).to(cuda)
+    B().local_search(pb, d_pop, d_fit, P, moves, 99, 7, ld=ld, island=1)
+    ref_pop, ref_fit = keys.copy(), fit.copy()
+    O.local_search(po, ref_pop, ref_fit, np.arange(P), P, ld, moves, 99, 7, 1)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(d_pop.cpu().numpy(), ref_pop)
+    np.testing.assert_array_equal(d_fit.cpu().numpy(), ref_fit)
+    improved = int(np.sum(ref_fit < fit))
+    assert 0 < improved < P, improved  # the check sees both outcomes
+
+
+def oracle_run_ls(po, P, E, M, rho, seed, k, G, ld, interval, count, moves, mig_interval=0, migrants=0):
+    """oracle generations with the local search pass after generation g when g - 1 > 0 and
+    (g - 1) % interval == 0 (then re-rank), before migration"""
+    Pi, Ei, Mi = P // k, E // k, M // k
+    prs = [O.params(Pi, Ei, Mi, rho, seed, i) for i in range(k)]
+    pops, fits, srts = [], [], []
+    for i in range(k):
+        p, f = O.brkga_init(po, prs[i], ld)
+        pops.append(p)
+        fits.append(f)
+        srts.append(O.sort_fitness(f))
+    hist = [min(f[s[0]] for f, s in zip(fits, srts))]
+    cnt = min(count, Ei)
+    for g in range(1, G + 1):
+        for i in range(k):
+            pops[i], fits[i] = O.brkga_generation(po, prs[i], g, pops[i], fits[i], srts[i], ld)
+            srts[i] = O.sort_fitness(fits[i])
+            if g - 1 > 0 and (g - 1) % interval == 0:
+                O.local_search(po, pops[i], fits[i], srts[i], cnt, ld, moves, seed, g, i)
+                srts[i] = O.sort_fitness(fits[i])
+        if k > 1 and mig_interval > 0 and g % mig_interval == 0:
+            pop = np.ascontiguousarray(np.concatenate(pops))
+            fit = np.ascontiguousarray(np.concatenate(fits))
+            srt = np.ascontiguousarray(np.concatenate(srts))
+            O.migrate(k, Pi, migrants, po.n, ld, False, pop, fit, srt)
+            pops = [pop[i * Pi:(i + 1) * Pi].copy() for i in range(k)]
+            fits = [fit[i * Pi:(i + 1) * Pi].copy() for i in range(k)]
+            srts = [srt[i * Pi:(i + 1) * Pi].copy() for i in range(k)]
+        hist.append(min(f[s[0]] for f, s in zip(fits, srts)))
+    keys = np.concatenate([p[s][:, :po.n] for p, s in zip(pops, srts)])
+    fit = np.concatenate([f[s] for f, s in zip(fits, srts)])
+    return keys, fit, np.array(hist, np.float32)
+
+
+@pytest.mark.parametrize("k", [1, 2])
+def test_engine_local_search_bit_exact(cuda, k):
+    c, P, E, M, G = 30, 160, 40, 16, 12
+    pb, po = problems(c, seed=40 + k)
+    prm = B().params(P, E, M, 0.75, G, seed=5, num_islands=k, migration_interval=5 if k > 1 else 0,
+                     num_migrants=2 if k > 1 else 0, local_search_interval=2, local_search_individuals=100,
+                     local_search_moves=5)
+    s = B().Solver(pb, prm)
+    s.run()
+    keys, fit = s.get_population()
+    rk, rf, rh = oracle_run_ls(po, P, E, M, 0.75, 5, k, G, (2 * c + 3) // 4 * 4, 2, 100, 5,
+                               5 if k > 1 else 0, 2)
+    np.testing.assert_array_equal(keys, rk)
+    np.testing.assert_array_equal(fit, rf)
+    np.testing.assert_array_equal(s.get_fitness_history(), rh)
+    s.close()
+
+
+def test_local_search_rejected_in_batches(cuda):
+    pb, _ = problems(10, seed=50)
+    with pytest.raises(B().BrkgaError) as ei:
+        B().Batch([pb], [B().params(32, 6, 3, 0.75, 5, seed=1, local_search_interval=2)])
+    assert ei.value.code == -6
