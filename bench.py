@@ -385,12 +385,20 @@ sys.path[:0] = [{os.path.join(ROOT, 'oracle')!r}]
 import numpy as np
 import oracle as O
 a = {a!r}
-xy = np.random.default_rng(a['seed']).random((a['pts'], 2), dtype=np.float32) * np.float32(a.get('scale', 1.0))
-xy2 = np.random.default_rng(a['seed'] + 1).random((a['pts'], 2), dtype=np.float32)
+if a.get('tspj'):
+    rng = np.random.default_rng(a['seed'])
+    pts = rng.random((a['n'] + 1, 2)) * 100.0
+    xy = np.ascontiguousarray(np.sqrt(((pts[:, None, :] - pts[None, :, :]) ** 2).sum(-1)).astype(np.float32))
+    xy2 = (1.0 + rng.random((a['n'] + 1, a['n'] + 1)) * 99.0).astype(np.float32)
+    xy2[0, :] = 0.0
+else:
+    xy = np.random.default_rng(a['seed']).random((a['pts'], 2), dtype=np.float32) * np.float32(a.get('scale', 1.0))
+    xy2 = np.random.default_rng(a['seed'] + 1).random((a['pts'], 2), dtype=np.float32)
 if not O.ref_available():
     print(json.dumps(dict(value=None))); sys.exit(0)
 R = O.ref()
-h = R.ref_solver_create({kind}, a['n'], xy.ctypes.data, xy2.ctypes.data, None, None, 0.0, a['P'], a['E'], a['M'], 0.7)
+h = R.ref_solver_create({kind}, a['n'], xy.ctypes.data, xy2.ctypes.data, None, None, 0.0, a['P'], a['E'], a['M'],
+                        0.75 if a.get('tspj') else 0.7)
 R.ref_solver_evolve(h, 1)
 g, t = 0, 0.0
 while t < {seconds} and g < {max_gens}:
@@ -602,6 +610,17 @@ def workload_quality(args):
     return out
 
 
+def tspj_instance(c, seed):
+    """TSPJ data over the depot and c cities: Euclidean travel times of seeded points in
+    [0,100)^2, job durations uniform in [1,100) per (city, job type), depot row zero"""
+    rng = np.random.default_rng(seed)
+    xy = rng.random((c + 1, 2)) * 100.0
+    travel = np.sqrt(((xy[:, None, :] - xy[None, :, :]) ** 2).sum(-1)).astype(np.float32)
+    jobs = (1.0 + rng.random((c + 1, c + 1)) * 99.0).astype(np.float32)
+    jobs[0, :] = 0.0
+    return travel, jobs
+
+
 def run_workload(args):
     import torch
     torch.cuda.init()
@@ -622,6 +641,18 @@ def run_workload(args):
                               dict(population_size=2048, elite_size=0, mutant_size=204, elite_prob=0.7,
                                    max_generations=600, seed=3), args.generations, 5,
                               dict(seed=3, pts=501, n=500, P=2048, E=0, M=0))
+    elif w == "tspj":
+        import brkga_b200 as B
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        # TSPJConfig::configure_for_multi_gpu on one GPU at 100 cities (configs/tspj_config.hpp:829-849):
+        # population 1000, elite 200, mutants 100, rho 0.75; random 2-opt every 2 generations
+        # on 100 elites with 5 moves (core/solver.hpp:166)
+        travel, jobs = tspj_instance(100, 11)
+        out = workload_solver(args, "TSPJ c=100 pop 1000 (local search on)", lambda: B.tspj(travel, jobs),
+                              dict(population_size=1000, elite_size=200, mutant_size=100, elite_prob=0.75,
+                                   max_generations=100000, seed=11, local_search_interval=2,
+                                   local_search_individuals=100, local_search_moves=5), args.generations, 7,
+                              dict(seed=11, tspj=True, n=100, P=1000, E=200, M=100))
     elif w == "batch":
         out = workload_batch(args)
     elif w == "serve":
@@ -666,7 +697,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--profile-op", action="store_true", help="operator kernels only (profiler captures)")
-    ap.add_argument("--workload", default="tsp1000", choices=["tsp1000", "tsp52", "nsga", "batch", "serve", "quality"])
+    ap.add_argument("--workload", default="tsp1000", choices=["tsp1000", "tsp52", "nsga", "tspj", "batch", "serve", "quality"])
     ap.add_argument("--generations", type=int, default=500)
     ap.add_argument("--instances", type=int, default=256)
     ap.add_argument("--rate", type=float, default=200.0)

@@ -113,6 +113,12 @@ public:
     int migration_interval = 0;
     int num_migrants = 0;
     int device = 0;
+    // random 2-opt local search for configs that have one (TSPJ); the reference runs it in
+    // its multi-GPU island loop every 2 generations on 100 elites with 5 moves
+    // (core/solver.hpp:166, 459-461); 0 = off
+    int local_search_interval = 0;
+    int local_search_individuals = 100;
+    int local_search_moves = 5;
 
     explicit BRKGAConfig(int chrom_len) : BRKGAConfig(std::vector<int>{chrom_len}) {}
     explicit BRKGAConfig(const std::vector<int>& lens, int n_objectives = 1)
@@ -362,6 +368,114 @@ private:
     std::string name_;
 };
 
+// configs/tspj_config.hpp:24-983: a tour over the depot (node 0) and c cities plus an
+// assignment of c job types to the tour positions; chromosome = c city keys then c job
+// keys; fitness = makespan (max of the tour length and the latest arrival + job time)
+template <typename T>
+class TSPJConfig : public DeviceProblemConfig<T> {
+public:
+    TSPJConfig(const std::vector<std::vector<T>>& travel, const std::vector<std::vector<T>>& jobs,
+               const std::string& name = "TSPJ")
+        : DeviceProblemConfig<T>(std::vector<int>{(int)travel.size() - 1, (int)travel.size() - 1}),
+          num_cities_((int)travel.size() - 1), name_(name) {
+        const int dim = (int)travel.size();
+        if (dim < 2 || (int)jobs.size() != dim) throw std::invalid_argument("TSPJ needs two (c+1) x (c+1) matrices");
+        std::vector<float> a((size_t)dim * dim), b((size_t)dim * dim);
+        for (int i = 0; i < dim; ++i) {
+            if ((int)travel[i].size() != dim || (int)jobs[i].size() != dim)
+                throw std::invalid_argument("TSPJ matrices must be square and of equal size");
+            for (int j = 0; j < dim; ++j) {
+                a[(size_t)i * dim + j] = (float)travel[i][j];
+                b[(size_t)i * dim + j] = (float)jobs[i][j];
+            }
+        }
+        brkga_problem_desc d{};
+        d.kind = BRKGA_TSPJ;
+        d.n = num_cities_;
+        d.matrix = a.data();
+        d.matrix2 = b.data();
+        this->create(d);
+        this->comparator = [](T x, T y) { return x < y; };
+        this->threads_per_block = 256;
+        this->update_cuda_grid_size();
+    }
+    bool has_local_search() const override { return true; }
+
+    // configs/tspj_config.hpp:727-770: <name>_TT.csv / <name>_JT.csv, or
+    // <name>_cost_table_by_coordinates.csv / <name>_tasktime_table.csv, given either file
+    static std::unique_ptr<TSPJConfig<T>> load_from_file(const std::string& filename) {
+        const size_t slash = filename.find_last_of('/');
+        const std::string dir = (slash == std::string::npos) ? "." : filename.substr(0, slash);
+        std::string base = (slash == std::string::npos) ? filename : filename.substr(slash + 1);
+        const size_t dot = base.find_last_of('.');
+        if (dot != std::string::npos) base = base.substr(0, dot);
+        std::string tt, jt, name;
+        auto cut = [&](const std::string& tag) { return base.substr(0, base.find(tag)); };
+        if (base.find("_TT") != std::string::npos) {
+            name = cut("_TT"), tt = filename, jt = dir + "/" + name + "_JT.csv";
+        } else if (base.find("_JT") != std::string::npos) {
+            name = cut("_JT"), jt = filename, tt = dir + "/" + name + "_TT.csv";
+        } else if (base.find("_cost_table_by_coordinates") != std::string::npos) {
+            name = cut("_cost_table_by_coordinates"), tt = filename, jt = dir + "/" + name + "_tasktime_table.csv";
+        } else if (base.find("_tasktime_table") != std::string::npos) {
+            name = cut("_tasktime_table"), jt = filename,
+            tt = dir + "/" + name + "_cost_table_by_coordinates.csv";
+        } else {
+            throw std::runtime_error(
+                "TSPJ CSV files must be named with '_TT'/'_JT' or '_cost_table_by_coordinates'/'_tasktime_table' suffix");
+        }
+        if (!std::ifstream(tt).good()) throw std::runtime_error("Travel times file not found: " + tt);
+        if (!std::ifstream(jt).good()) throw std::runtime_error("Job times file not found: " + jt);
+        return std::make_unique<TSPJConfig<T>>(load_csv_matrix(tt), load_csv_matrix(jt), name);
+    }
+    // configs/tspj_config.hpp:803-825
+    static void configure_for_size(TSPJConfig<T>* c, int n) {
+        if (n <= 10) {
+            c->population_size = 300, c->elite_size = 60, c->mutant_size = 30, c->max_generations = 500;
+        } else if (n <= 20) {
+            c->population_size = 600, c->elite_size = 120, c->mutant_size = 60, c->max_generations = 1000;
+        } else if (n <= 50) {
+            c->population_size = 1000, c->elite_size = 200, c->mutant_size = 100, c->max_generations = 2000;
+        } else {
+            c->population_size = 2000, c->elite_size = 350, c->mutant_size = 200, c->max_generations = 30000;
+        }
+        c->elite_prob = 0.75;
+        c->update_cuda_grid_size();
+    }
+    int get_num_cities() const { return num_cities_; }
+    int get_num_jobs() const { return num_cities_; }
+    const std::string& get_instance_name() const { return name_; }
+
+private:
+    // comma-separated rows; '#' lines and empty lines skipped; unparsable cells read as 0
+    // (configs/tspj_config.hpp:773-800)
+    static std::vector<std::vector<T>> load_csv_matrix(const std::string& path) {
+        std::ifstream f(path);
+        std::vector<std::vector<T>> m;
+        std::string line;
+        while (std::getline(f, line)) {
+            if (line.empty() || line[0] == '#') continue;
+            std::vector<T> row;
+            std::stringstream ss(line);
+            std::string cell;
+            while (std::getline(ss, cell, ',')) {
+                const size_t a = cell.find_first_not_of(" \t\r\n");
+                if (a == std::string::npos) continue;
+                cell = cell.substr(a, cell.find_last_not_of(" \t\r\n") - a + 1);
+                try {
+                    row.push_back((T)std::stod(cell));
+                } catch (const std::exception&) {
+                    row.push_back(T(0));
+                }
+            }
+            if (!row.empty()) m.push_back(row);
+        }
+        return m;
+    }
+    int num_cities_;
+    std::string name_;
+};
+
 // core/solver.hpp:44-1726: device-resident population, one CUDA graph per chunk of
 // generations; run / initialize / evolve_generation / get_best_individual /
 // get_pareto_front / get_fitness_history / get_config / export_pareto_front
@@ -385,6 +499,11 @@ public:
         p.migration_interval = config_->migration_interval;
         p.num_migrants = config_->num_migrants;
         p.device = config_->device;
+        if (config_->has_local_search()) {
+            p.local_search_interval = config_->local_search_interval;
+            p.local_search_individuals = config_->local_search_individuals;
+            p.local_search_moves = config_->local_search_moves;
+        }
         brkga_b200_detail::check(brkga_create(pb, &p, &e_), "Solver");
         n_ = config_->get_total_chromosome_length();
         best_ = Individual<T>(config_->component_lengths, config_->num_objectives > 1 ? config_->num_objectives : 0);
@@ -409,7 +528,12 @@ public:
     const Individual<T>& get_best_individual() {
         std::vector<float> k(n_), f(2);
         brkga_b200_detail::check(brkga_get_best(e_, k.data(), nullptr, f.data()), "get_best_individual");
-        best_.chromosomes[0].assign(k.begin(), k.end());
+        size_t off = 0;  // the flat key row, component by component (core/solver.hpp:300-312)
+        for (size_t c = 0; c < best_.chromosomes.size(); ++c) {
+            const size_t len = (size_t)config_->component_lengths[c];
+            best_.chromosomes[c].assign(k.begin() + off, k.begin() + off + len);
+            off += len;
+        }
         best_.fitness = f[0];
         if (config_->num_objectives > 1) best_.objectives = {(T)f[0], (T)f[1]};
         best_.evaluated = true;

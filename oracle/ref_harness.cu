@@ -334,7 +334,8 @@ static void* make_solver(std::unique_ptr<BRKGAConfig<float>> cfg, int P, int E, 
     return h;
 }
 
-// kind 1: TSP from coordinates; 3: threshold knapsack; 5: bi-objective TSP (coords of dim points)
+// kind 1: TSP from coordinates; 3: threshold knapsack; 5: bi-objective TSP (coords of dim points);
+// 7: TSPJ (travel and job matrices)
 void* ref_solver_create(int kind, int n, const float* xy, const float* xy2, const float* w,
                         const float* v, float cap, int P, int E, int M, double rho) {
     try {
@@ -343,6 +344,10 @@ void* ref_solver_create(int kind, int n, const float* xy, const float* xy2, cons
         } else if (kind == 3) {
             std::vector<float> W(w, w + n), V(v, v + n);
             return make_solver(std::make_unique<KnapsackConfig<float>>(W, V, cap, "ref"), P, E, M, rho);
+        } else if (kind == 7) {  // TSPJ: xy / xy2 carry the (n+1) x (n+1) travel and job matrices
+            return make_solver(std::make_unique<TSPJConfig<float>>(flat_to_matrix(xy, n + 1), flat_to_matrix(xy2, n + 1),
+                                                                  "ref"),
+                               P, E, M, rho);
         } else if (kind == 5) {
             return make_solver(std::make_unique<MultiTSPConfig<float>>(coords_to_matrix(xy, n + 1),
                                                                       coords_to_matrix(xy2, n + 1), "ref"),

@@ -148,3 +148,26 @@ def test_local_search_rejected_in_batches(cuda):
     with pytest.raises(B().BrkgaError) as ei:
         B().Batch([pb], [B().params(32, 6, 3, 0.75, 5, seed=1, local_search_interval=2)])
     assert ei.value.code == -6
+
+
+def test_cpp_tspj_dropin_program(cuda, tmp_path):
+    """the reference-style C++ program (_TT/_JT CSV files -> TSPJConfig::load_from_file ->
+    Solver with local search) gives the same best makespan and decode as the Python binding
+    on the same matrices and seed"""
+    import json
+    import os
+    import subprocess
+    exe = os.path.join(os.path.dirname(B().LIB_PATH), "..", "build", "solve_tspj")
+    r = subprocess.run([exe, str(tmp_path), "20", "3", "128", "25", "12", "40"], capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0, r.stderr
+    out = json.loads(r.stdout.strip().splitlines()[-1])
+    travel = np.loadtxt(tmp_path / "synthetic_TT.csv", delimiter=",", dtype=np.float32)
+    jobs = np.loadtxt(tmp_path / "synthetic_JT.csv", delimiter=",", dtype=np.float32)
+    assert travel.shape == (21, 21) and out["history"] == 41
+    s = B().Solver(B().tspj(travel, jobs), B().params(128, 25, 12, 0.7, 40, seed=7, local_search_interval=2))
+    s.run()
+    _, perm, best = s.get_best_individual()
+    assert np.float32(out["best"]) == best
+    assert out["perm"] == perm.tolist()
+    s.close()
