@@ -41,9 +41,18 @@ typedef enum {
     BRKGA_KNAP_GREEDY = 4,       /* key-order first-fit greedy knapsack (no reference counterpart)          */
     BRKGA_BITSP_COORDS = 5,      /* MultiTSPConfig with two coordinate sets, depot = point 0                */
     BRKGA_BITSP_MATRIX = 6,      /* MultiTSPConfig(dist, time, name) (configs/multi_tsp_config.hpp:25-52)   */
-    BRKGA_TSPJ = 7               /* TSPJConfig(travel, jobs, name): tour + job assignment, makespan
+    BRKGA_TSPJ = 7,              /* TSPJConfig(travel, jobs, name): tour + job assignment, makespan
                                     (configs/tspj_config.hpp:40-66, 555-626)                                */
+    BRKGA_JOBSCHED = 8,          /* JobSchedulingGPUConfig(job_times, machines): gene i puts job i on
+                                    machine floor(key * machines); makespan = largest machine load
+                                    (configs/job_scheduling_gpu_config.hpp:30-52, 132-148)                  */
+    BRKGA_CONTINUOUS = 9         /* ContinuousOptGPUConfig(n, lower, upper, function): x = key *
+                                    (upper - lower) + lower; sphere / Rastrigin / Rosenbrock
+                                    (configs/continuous_opt_gpu_config.hpp:37-57, 114-173)                  */
 } brkga_problem_kind;
+
+/* functions of BRKGA_CONTINUOUS (the reference's OptimizationFunction) */
+typedef enum { BRKGA_FN_SPHERE = 0, BRKGA_FN_RASTRIGIN = 1, BRKGA_FN_ROSENBROCK = 2 } brkga_function;
 
 /* Instance data (HOST pointers; copied to the device at creation).
  *   TSP:      n cities; coords [n][2] or matrix [n][n]
@@ -52,7 +61,9 @@ typedef enum {
  *   knapsack: n items; weights, values [n] (integers); capacity
  *   TSPJ:     n cities besides the depot (node 0) and n job types; matrix = travel times
  *             [n+1][n+1], matrix2 = job durations [n+1][n+1] (row = city, column = job
- *             type); chromosomes hold 2n keys, the n city keys then the n job keys      */
+ *             type); chromosomes hold 2n keys, the n city keys then the n job keys
+ *   job scheduling: n jobs; job_times [n]; machines >= 1
+ *   continuous: n variables; function (brkga_function); lower < upper                  */
 typedef struct {
     int32_t kind;
     int32_t n;
@@ -63,6 +74,11 @@ typedef struct {
     const int32_t* weights;
     const int32_t* values;
     float capacity;
+    const float* job_times;      /* job scheduling                                            */
+    int32_t machines;
+    int32_t function;            /* continuous                                                */
+    float lower;
+    float upper;
 } brkga_problem_desc;
 
 /* GA parameters (BRKGAConfig fields, core/config.hpp:17-30, plus the engine's own). */

@@ -22,6 +22,8 @@ REPO_DIR = os.path.dirname(PKG_DIR)
 HEADER_PATH = os.path.join(REPO_DIR, "include", "brkga_b200.h")
 
 TSP_COORDS, TSP_MATRIX, KNAP_THRESHOLD, KNAP_GREEDY, BITSP_COORDS, BITSP_MATRIX, TSPJ = 1, 2, 3, 4, 5, 6, 7
+JOBSCHED, CONTINUOUS = 8, 9
+SPHERE, RASTRIGIN, ROSENBROCK = 0, 1, 2
 
 STATUS = {0: "OK", -1: "INVALID", -2: "OOM", -3: "CUDA", -4: "TIMEOUT", -5: "CANCELLED",
           -6: "UNSUPPORTED", -7: "BUSY", -8: "NOT_READY"}
@@ -36,7 +38,8 @@ class BrkgaError(RuntimeError):
 class ProblemDesc(C.Structure):
     _fields_ = [("kind", C.c_int32), ("n", C.c_int32), ("coords", C.c_void_p), ("coords2", C.c_void_p),
                 ("matrix", C.c_void_p), ("matrix2", C.c_void_p), ("weights", C.c_void_p),
-                ("values", C.c_void_p), ("capacity", C.c_float)]
+                ("values", C.c_void_p), ("capacity", C.c_float), ("job_times", C.c_void_p),
+                ("machines", C.c_int32), ("function", C.c_int32), ("lower", C.c_float), ("upper", C.c_float)]
 
 
 class Params(C.Structure):
@@ -163,7 +166,7 @@ class Problem:
     """Device-resident instance (TSPConfig / KnapsackConfig / MultiTSPConfig data)."""
 
     def __init__(self, kind, n, coords=None, coords2=None, matrix=None, matrix2=None, weights=None, values=None,
-                 capacity=0.0, device=0):
+                 capacity=0.0, device=0, job_times=None, machines=0, function=0, lower=0.0, upper=0.0):
         keep = []
 
         def arr(a, dt):
@@ -174,7 +177,8 @@ class Problem:
             return a.ctypes.data
 
         d = ProblemDesc(kind, n, arr(coords, np.float32), arr(coords2, np.float32), arr(matrix, np.float32),
-                        arr(matrix2, np.float32), arr(weights, np.int32), arr(values, np.int32), float(capacity))
+                        arr(matrix2, np.float32), arr(weights, np.int32), arr(values, np.int32), float(capacity),
+                        arr(job_times, np.float32), int(machines), int(function), float(lower), float(upper))
         h = C.c_void_p()
         check(lib().brkga_problem_create(C.byref(d), device, C.byref(h)))
         # n is the chromosome length (genes); a TSPJ instance of c cities has 2c genes
@@ -241,6 +245,19 @@ def tspj(travel, jobs, device=0):
     both [c+1][c+1]; chromosomes hold 2c keys (city keys, then job keys)"""
     travel = np.asarray(travel, np.float32)
     return Problem(TSPJ, travel.shape[0] - 1, matrix=travel, matrix2=jobs, device=device)
+
+
+def jobsched(job_times, machines, device=0):
+    """job scheduling (JobSchedulingGPUConfig): gene i puts job i on machine
+    floor(key * machines); fitness = makespan"""
+    jt = np.asarray(job_times, np.float32)
+    return Problem(JOBSCHED, jt.shape[0], job_times=jt, machines=machines, device=device)
+
+
+def continuous(n, lower, upper, function=SPHERE, device=0):
+    """continuous optimisation (ContinuousOptGPUConfig): sphere, Rastrigin or Rosenbrock
+    over n variables x = key * (upper - lower) + lower"""
+    return Problem(CONTINUOUS, n, function=function, lower=lower, upper=upper, device=device)
 
 
 def params(population_size=100, elite_size=20, mutant_size=10, elite_prob=0.7, max_generations=1000, seed=1,
@@ -462,7 +479,7 @@ class Server:
             pass
 
     def submit(self, kind, n, prm, stall=0, coords=None, coords2=None, matrix=None, matrix2=None, weights=None,
-               values=None, capacity=0.0):
+               values=None, capacity=0.0, job_times=None, machines=0, function=0, lower=0.0, upper=0.0):
         keep = []
 
         def arr(a, dt):
@@ -473,7 +490,8 @@ class Server:
             return a.ctypes.data
 
         d = ProblemDesc(kind, n, arr(coords, np.float32), arr(coords2, np.float32), arr(matrix, np.float32),
-                        arr(matrix2, np.float32), arr(weights, np.int32), arr(values, np.int32), float(capacity))
+                        arr(matrix2, np.float32), arr(weights, np.int32), arr(values, np.int32), float(capacity),
+                        arr(job_times, np.float32), int(machines), int(function), float(lower), float(upper))
         rid = C.c_int64()
         check(lib().brkga_server_submit(self.h, C.byref(d), C.byref(prm), stall, C.byref(rid)))
         return rid.value

@@ -328,6 +328,93 @@ public:
     const std::vector<T>& get_values() const { return values_; }
     T get_capacity() const { return capacity_; }
 
+    // configs/knapsack_config.hpp:180-304: ".csv" files hold "weight,value[,capacity]" rows
+    // (the first row with a numeric third field gives the capacity, else half the total
+    // weight); other files hold "num_items capacity" and then "weight value" lines; '#'
+    // lines are comments
+    static std::unique_ptr<KnapsackConfig<T>> load_from_file(const std::string& filename, bool greedy = false) {
+        std::ifstream f(filename);
+        if (!f.good()) throw std::runtime_error("File does not exist: " + filename);
+        const size_t slash = filename.find_last_of('/');
+        std::string name = (slash == std::string::npos) ? filename : filename.substr(slash + 1);
+        const size_t dot = name.find_last_of('.');
+        const std::string ext = (dot == std::string::npos) ? "" : name.substr(dot + 1);
+        if (dot != std::string::npos) name = name.substr(0, dot);
+        std::vector<T> w, v;
+        T cap = 0;
+        std::string line;
+        if (ext == "csv") {
+            bool have_cap = false;
+            while (std::getline(f, line)) {
+                if (line.empty() || line[0] == '#') continue;
+                std::vector<std::string> fields;
+                std::stringstream ss(line);
+                std::string cell;
+                while (std::getline(ss, cell, ',')) {
+                    const size_t a = cell.find_first_not_of(" \t\r\n");
+                    fields.push_back(a == std::string::npos ? std::string()
+                                                            : cell.substr(a, cell.find_last_not_of(" \t\r\n") - a + 1));
+                }
+                if (fields.size() < 2) continue;
+                if (!have_cap && fields.size() >= 3) {
+                    try {
+                        cap = (T)std::stod(fields[2]);
+                        have_cap = true;
+                    } catch (...) {
+                    }
+                }
+                try {
+                    const T wi = (T)std::stod(fields[0]), vi = (T)std::stod(fields[1]);
+                    w.push_back(wi);
+                    v.push_back(vi);
+                } catch (...) {
+                }
+            }
+            if (w.empty()) throw std::runtime_error("No valid items found in CSV file");
+            if (!have_cap) {
+                T total = 0;
+                for (T x : w) total += x;
+                cap = total * (T)0.5;
+            }
+        } else {
+            bool items = false;
+            int count = 0;
+            while (std::getline(f, line)) {
+                if (line.empty() || line[0] == '#') continue;
+                std::istringstream is(line);
+                if (!items) {
+                    if (is >> count >> cap) items = true;
+                } else {
+                    T wi, vi;
+                    if (is >> wi >> vi) {
+                        w.push_back(wi);
+                        v.push_back(vi);
+                    }
+                }
+            }
+            if (w.empty()) throw std::runtime_error("No items found in file");
+        }
+        return std::make_unique<KnapsackConfig<T>>(w, v, cap, name, greedy);
+    }
+    // configs/knapsack_config.hpp:157-178 draws real weights and values; the device
+    // knapsack sums integers, so this draws integers in [1, max] (std::mt19937(seed))
+    static std::unique_ptr<KnapsackConfig<T>> create_random(int num_items, T max_weight = 50, T max_value = 100,
+                                                           T capacity_ratio = 0.5,
+                                                           const std::string& name = "Random_Knapsack",
+                                                           unsigned seed = 1, bool greedy = false) {
+        std::mt19937 rng(seed);
+        std::uniform_int_distribution<int> dw(1, (int)max_weight), dv(1, (int)max_value);
+        std::vector<T> w(num_items), v(num_items);
+        T total = 0;
+        for (int i = 0; i < num_items; ++i) {
+            w[i] = (T)dw(rng);
+            v[i] = (T)dv(rng);
+            total += w[i];
+        }
+        return std::make_unique<KnapsackConfig<T>>(w, v, total * capacity_ratio, name + "_" + std::to_string(num_items),
+                                                   greedy);
+    }
+
 private:
     std::vector<T> weights_, values_;
     T capacity_;
@@ -365,6 +452,92 @@ public:
     int get_num_cities() const { return this->component_lengths[0]; }
 
 private:
+    std::string name_;
+};
+
+// configs/job_scheduling_gpu_config.hpp:16-197: gene i puts job i on machine
+// (int)(key * machines); fitness = makespan (largest machine load), minimised
+template <typename T>
+class JobSchedulingGPUConfig : public DeviceProblemConfig<T> {
+public:
+    JobSchedulingGPUConfig(const std::vector<T>& jobs, int machines, const std::string& name = "JobScheduling_GPU")
+        : DeviceProblemConfig<T>((int)jobs.size()), job_times_(jobs), machines_(machines), name_(name) {
+        if (machines <= 0) throw std::invalid_argument("Number of machines must be positive");
+        std::vector<float> jt(jobs.begin(), jobs.end());
+        brkga_problem_desc d{};
+        d.kind = BRKGA_JOBSCHED;
+        d.n = (int)jobs.size();
+        d.job_times = jt.data();
+        d.machines = machines;
+        this->create(d);
+        this->comparator = [](T a, T b) { return a < b; };
+        this->threads_per_block = 256;
+        this->update_cuda_grid_size();
+    }
+    // configs/job_scheduling_gpu_config.hpp:216-229
+    static std::unique_ptr<JobSchedulingGPUConfig<T>> create_test_instance(int num_jobs = 50, int num_machines = 5) {
+        std::vector<T> jobs;
+        for (int i = 0; i < num_jobs; ++i) jobs.push_back((T)(10 + (i % 40)));
+        return std::make_unique<JobSchedulingGPUConfig<T>>(
+            jobs, num_machines, "Test_GPU_J" + std::to_string(num_jobs) + "_M" + std::to_string(num_machines));
+    }
+    bool is_gpu_available() const { return this->pb_ != nullptr; }
+    int get_num_machines() const { return machines_; }
+
+private:
+    std::vector<T> job_times_;
+    int machines_;
+    std::string name_;
+};
+
+// configs/continuous_opt_gpu_config.hpp:20-240: x = key * (upper - lower) + lower
+enum class OptimizationFunction { SPHERE, RASTRIGIN, ROSENBROCK };
+
+template <typename T>
+class ContinuousOptGPUConfig : public DeviceProblemConfig<T> {
+public:
+    ContinuousOptGPUConfig(int num_vars, T lower, T upper, OptimizationFunction func = OptimizationFunction::SPHERE,
+                           const std::string& name = "ContinuousOpt_GPU")
+        : DeviceProblemConfig<T>(num_vars), lower_(lower), upper_(upper), func_(func), name_(name) {
+        brkga_problem_desc d{};
+        d.kind = BRKGA_CONTINUOUS;
+        d.n = num_vars;
+        d.function = func == OptimizationFunction::RASTRIGIN    ? BRKGA_FN_RASTRIGIN
+                     : func == OptimizationFunction::ROSENBROCK ? BRKGA_FN_ROSENBROCK
+                                                                : BRKGA_FN_SPHERE;
+        d.lower = (float)lower;
+        d.upper = (float)upper;
+        this->create(d);
+        this->comparator = [](T a, T b) { return a < b; };
+        this->threads_per_block = 256;
+        this->update_cuda_grid_size();
+    }
+    // configs/continuous_opt_gpu_config.hpp:216-237
+    static std::unique_ptr<ContinuousOptGPUConfig<T>> create_sphere(int num_vars = 30) {
+        return std::make_unique<ContinuousOptGPUConfig<T>>(num_vars, (T)-5.12, (T)5.12, OptimizationFunction::SPHERE,
+                                                           "Sphere_GPU_" + std::to_string(num_vars));
+    }
+    static std::unique_ptr<ContinuousOptGPUConfig<T>> create_rastrigin(int num_vars = 30) {
+        return std::make_unique<ContinuousOptGPUConfig<T>>(num_vars, (T)-5.12, (T)5.12,
+                                                           OptimizationFunction::RASTRIGIN,
+                                                           "Rastrigin_GPU_" + std::to_string(num_vars));
+    }
+    static std::unique_ptr<ContinuousOptGPUConfig<T>> create_rosenbrock(int num_vars = 30) {
+        return std::make_unique<ContinuousOptGPUConfig<T>>(num_vars, (T)-5.0, (T)10.0,
+                                                           OptimizationFunction::ROSENBROCK,
+                                                           "Rosenbrock_GPU_" + std::to_string(num_vars));
+    }
+    // the decision variables of a chromosome
+    std::vector<T> decode(const Individual<T>& ind) const {
+        std::vector<T> x;
+        for (T g : ind.chromosomes[0]) x.push_back(g * (upper_ - lower_) + lower_);
+        return x;
+    }
+    bool is_gpu_available() const { return this->pb_ != nullptr; }
+
+private:
+    T lower_, upper_;
+    OptimizationFunction func_;
     std::string name_;
 };
 

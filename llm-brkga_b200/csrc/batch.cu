@@ -658,7 +658,8 @@ struct Request {
 };
 
 size_t estimate_bytes(const brkga_problem_desc& d, const brkga_params& p) {
-    const size_t n = (size_t)std::max(1, d.n), ld = (n + 3) / 4 * 4;
+    const size_t n = (size_t)std::max(1, d.n);
+    const size_t genes = (d.kind == BRKGA_TSPJ) ? 2 * n : n, ld = (genes + 3) / 4 * 4;
     const bool mo = d.kind == BRKGA_BITSP_COORDS || d.kind == BRKGA_BITSP_MATRIX;
     const size_t P = (size_t)std::max(1, p.population_size);
     const size_t rows = mo ? 2 * P : P;
@@ -670,6 +671,7 @@ size_t estimate_bytes(const brkga_problem_desc& d, const brkga_params& p) {
     case BRKGA_TSP_MATRIX: b += n * n * 4; break;
     case BRKGA_BITSP_COORDS: b += 2 * (n + 1) * 8; break;
     case BRKGA_BITSP_MATRIX: b += 2 * (n + 1) * (n + 1) * 4; break;
+    case BRKGA_TSPJ: b += 2 * (n + 1) * (n + 1) * 4; break;
     default: b += n * 8;
     }
     return b + 4096;
@@ -721,6 +723,12 @@ static int32_t server_copy_desc(Request* r, const brkga_problem_desc* d) {
         r->desc.weights = cp_i(d->weights, n, r->weights);
         r->desc.values = cp_i(d->values, n, r->values);
         break;
+    case BRKGA_TSPJ:
+        r->desc.matrix = cp_f(d->matrix, (n + 1) * (n + 1), r->matrix);
+        r->desc.matrix2 = cp_f(d->matrix2, (n + 1) * (n + 1), r->matrix2);
+        break;
+    case BRKGA_JOBSCHED: r->desc.job_times = cp_f(d->job_times, n, r->coords); break;
+    case BRKGA_CONTINUOUS: break;
     default: return fail(BRKGA_ERR_INVALID, "unknown problem kind");
     }
     return BRKGA_OK;
@@ -794,12 +802,13 @@ int32_t brkga_server_submit(brkga_server* s, const brkga_problem_desc* desc, con
     if (!s || !desc || !params || !request_id) return fail(BRKGA_ERR_INVALID, "null argument");
     if (params->max_generations <= 0) return fail(BRKGA_ERR_INVALID, "max_generations must be > 0");
     if (params->num_islands > 1) return fail(BRKGA_ERR_UNSUPPORTED, "served requests run one population each");
-    if (desc->n < 1 || desc->n > row_max_n()) return fail(BRKGA_ERR_UNSUPPORTED, "chromosome length out of range");
+    const long long genes = (desc->kind == BRKGA_TSPJ) ? 2ll * desc->n : (long long)desc->n;
+    if (desc->n < 1 || genes > row_max_n()) return fail(BRKGA_ERR_UNSUPPORTED, "chromosome length out of range");
     {
-        const int pts = (desc->kind == BRKGA_BITSP_COORDS) ? desc->n + 1 : desc->n;
-        if (row_needs_global(desc->n, pts, desc->kind))
-            return fail(BRKGA_ERR_UNSUPPORTED, "served rows must fit the shared-memory row kernel (n = " +
-                                                   std::to_string(desc->n) + " does not)");
+        const int pts = (desc->kind == BRKGA_BITSP_COORDS) ? desc->n + 1 : (int)genes;
+        if (row_needs_global((int)genes, pts, desc->kind))
+            return fail(BRKGA_ERR_UNSUPPORTED, "served rows must fit the shared-memory row kernel (" +
+                                                   std::to_string(genes) + " genes do not)");
     }
     auto* r = new Request;
     int32_t st = server_copy_desc(r, desc);

@@ -128,6 +128,26 @@ int32_t make_problem(const brkga_problem_desc* d, int device, std::shared_ptr<Pr
         pd->n = 2 * n;
         break;
     }
+    case BRKGA_JOBSCHED:
+        // JobSchedulingGPUConfig (configs/job_scheduling_gpu_config.hpp:30-52): minimise the makespan
+        pd->m = 1;
+        if (!d->job_times) return fail(BRKGA_ERR_INVALID, "job scheduling needs job_times");
+        if (d->machines < 1) return fail(BRKGA_ERR_INVALID, "machines must be >= 1");
+        pd->machines = d->machines;
+        st = upload(*pd, d->job_times, (size_t)n * 4, &p);
+        pd->jt = (float*)p;
+        break;
+    case BRKGA_CONTINUOUS:
+        // ContinuousOptGPUConfig (configs/continuous_opt_gpu_config.hpp:37-57): minimise
+        pd->m = 1;
+        if (d->function < BRKGA_FN_SPHERE || d->function > BRKGA_FN_ROSENBROCK)
+            return fail(BRKGA_ERR_INVALID, "unknown continuous function " + std::to_string(d->function));
+        if (!std::isfinite(d->lower) || !std::isfinite(d->upper) || !(d->lower < d->upper))
+            return fail(BRKGA_ERR_INVALID, "need finite bounds with lower < upper");
+        pd->function = d->function;
+        pd->lo = d->lower;
+        pd->hi = d->upper;
+        break;
     default:
         return fail(BRKGA_ERR_INVALID, "unknown problem kind " + std::to_string(d->kind));
     }
@@ -150,6 +170,11 @@ void fill_instance(PopDesc& d, const ProblemData& pd) {
     d.v = pd.v;
     d.cap = pd.cap;
     d.capi = pd.capi;
+    d.jt = pd.jt;
+    d.machines = pd.machines;
+    d.function = pd.function;
+    d.lo = pd.lo;
+    d.hi = pd.hi;
     d.maximize = pd.maximize;
 }
 

@@ -19,7 +19,11 @@ enum Kind : int32_t {
     BITSP_COORDS = 5,
     BITSP_MATRIX = 6,
     TSPJ = 7,
+    JOBSCHED = 8,
+    CONTINUOUS = 9,
 };
+
+enum Function : int32_t { FN_SPHERE = 0, FN_RASTRIGIN = 1, FN_ROSENBROCK = 2 };
 
 // stream tags: Philox counter word 3 = (island << 8) | tag
 enum Tag : uint32_t {
@@ -90,6 +94,10 @@ struct PopDesc {
     const float* mat2;        // bi-TSP second matrix; TSPJ job durations [c+1][c+1]
     const int32_t* w;
     const int32_t* v;
+    const float* jt;          // job scheduling: job times [n]
+    int32_t machines;
+    int32_t function;         // continuous: Function and bounds
+    float lo, hi;
     float cap;                // knapsack capacity (threshold fitness, float like the reference)
     int32_t maximize;
     long long capi;           // floor(cap) for the greedy decoder

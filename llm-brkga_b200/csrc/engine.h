@@ -48,6 +48,10 @@ struct ProblemData {
     float* mat2 = nullptr;
     int32_t* w = nullptr;
     int32_t* v = nullptr;
+    float* jt = nullptr;     // job scheduling: job times
+    int machines = 0;
+    int function = 0;        // continuous: brkga_function, bounds
+    float lo = 0.0f, hi = 0.0f;
     size_t bytes = 0;
     std::vector<void*> allocs;
     ~ProblemData();

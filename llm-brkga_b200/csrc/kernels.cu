@@ -335,6 +335,90 @@ __device__ float tspj_makespan(const int32_t* perm, int nc, const float* __restr
     return v;
 }
 
+// ContinuousOptGPUConfig (configs/continuous_opt_gpu_config.hpp:114-173): x = key * (upper -
+// lower) + lower; sphere sum x^2; Rastrigin 10 n + sum (x^2 - 10 cos(2 pi x)); Rosenbrock
+// sum 100 (x_{i+1} - x_i^2)^2 + (1 - x_i)^2.  keys in index order (shared or global memory).
+// One warp adds the terms in the reference's sequential order, so sphere and Rosenbrock
+// equal the reference's values bit for bit; Rastrigin goes through the device cosf.
+template <int BLOCK>
+__device__ float continuous_fitness(const float* keys, int n, int fn, float lo, float hi, float* red) {
+    const int lane = threadIdx.x & 31;
+    if (threadIdx.x < 32) {
+        const float range = __fsub_rn(hi, lo);
+        const float two_pi = __fmul_rn(2.0f, 3.14159265358979323846f);
+        float sum = (fn == FN_RASTRIGIN) ? __fmul_rn(10.0f, (float)n) : 0.0f;
+        const int terms = (fn == FN_ROSENBROCK) ? n - 1 : n;
+        for (int c0 = 0; c0 < terms; c0 += 32) {
+            const int i = c0 + lane;
+            float term = 0.0f;
+            if (i < terms) {
+                const float x = __fadd_rn(__fmul_rn(keys[i], range), lo);
+                if (fn == FN_SPHERE) {
+                    term = __fmul_rn(x, x);
+                } else if (fn == FN_RASTRIGIN) {
+                    term = __fsub_rn(__fmul_rn(x, x), __fmul_rn(10.0f, cosf(__fmul_rn(two_pi, x))));
+                } else {
+                    const float xn = __fadd_rn(__fmul_rn(keys[i + 1], range), lo);
+                    const float t1 = __fsub_rn(xn, __fmul_rn(x, x));
+                    const float t2 = __fsub_rn(1.0f, x);
+                    term = __fadd_rn(__fmul_rn(__fmul_rn(100.0f, t1), t1), __fmul_rn(t2, t2));
+                }
+            }
+            const int cnt = min(32, terms - c0);
+            for (int q = 0; q < cnt; ++q) sum = __fadd_rn(sum, __shfl_sync(0xffffffffu, term, q));
+        }
+        if (lane == 0) red[0] = sum;
+    }
+    __syncthreads();
+    const float v = red[0];
+    __syncthreads();
+    return v;
+}
+
+// JobSchedulingGPUConfig (configs/job_scheduling_gpu_config.hpp:132-148): job i goes to
+// machine (int)(key_i * machines), capped at machines - 1; each machine's load adds its
+// jobs in index order; the makespan is the largest load.  Lane l of warp w keeps machine
+// 32 w + l (and every BLOCK-th after it) and adds the jobs of each 32-job chunk in order,
+// so every load equals the reference's sequential float sum bit for bit.
+template <int BLOCK>
+__device__ float jobsched_makespan(const float* keys, int n, const float* __restrict__ jt, int M, float* red) {
+    constexpr int NW = BLOCK / 32;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const float mf = (float)M;
+    float best = -INFINITY;
+    for (int m0 = warp * 32; m0 < M; m0 += BLOCK) {
+        float load = 0.0f;
+        for (int c0 = 0; c0 < n; c0 += 32) {
+            const int i = c0 + lane;
+            int mid = -1;
+            float v = 0.0f;
+            if (i < n) {
+                int mm = (int)__fmul_rn(keys[i], mf);
+                mid = mm >= M ? M - 1 : (mm < 0 ? 0 : mm);
+                v = __ldg(jt + i);
+            }
+            const int cnt = min(32, n - c0);
+            for (int q = 0; q < cnt; ++q) {
+                const int mq = __shfl_sync(0xffffffffu, mid, q);
+                const float vq = __shfl_sync(0xffffffffu, v, q);
+                if (mq == m0 + lane) load = __fadd_rn(load, vq);
+            }
+        }
+        if (m0 + lane < M) best = (best < load) ? load : best;
+    }
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) {
+        const float other = __shfl_xor_sync(0xffffffffu, best, o);
+        best = (best < other) ? other : best;
+    }
+    if (lane == 0) red[warp] = best;
+    __syncthreads();
+    float r = red[0];
+    for (int w = 1; w < NW; ++w) r = (r < red[w]) ? red[w] : r;
+    __syncthreads();
+    return r;
+}
+
 // ---------------------------------------------------------------------------------------
 // the fused row kernel
 // ---------------------------------------------------------------------------------------
@@ -359,7 +443,7 @@ __global__ void __launch_bounds__(BLOCK, RowResidency<BLOCK, G>::value) row_kern
     __shared__ PopDesc sd;
     __shared__ uint32_t warp_tot[32];
     __shared__ long long red_ll[32];
-    __shared__ float red_f[16];
+    __shared__ float red_f[32];
     __shared__ long long misc[4];
 
     const int t = threadIdx.x;
@@ -628,6 +712,19 @@ __global__ void __launch_bounds__(BLOCK, RowResidency<BLOCK, G>::value) row_kern
                 tv = block_sum_ll<BLOCK>(tv, red_ll);
                 const float twf = (float)tw, tvf = (float)tv;
                 res[0] = (twf > sd.cap) ? __fsub_rn(tvf, __fmul_rn(__fsub_rn(twf, sd.cap), 1000.0f)) : tvf;
+            } else if (kind == CONTINUOUS || kind == JOBSCHED) {
+                // no decode: the keys in index order, staged where the sort composites go
+                float* sk = reinterpret_cast<float*>(s.sc);
+#pragma unroll
+                for (int gg = 0; gg < G; ++gg)
+#pragma unroll
+                    for (int l = 0; l < 4; ++l) {
+                        const int i = 4 * (t + gg * BLOCK) + l;
+                        if (i < n) sk[i] = k[gg][l];
+                    }
+                __syncthreads();
+                res[0] = (kind == CONTINUOUS) ? continuous_fitness<BLOCK>(sk, n, sd.function, sd.lo, sd.hi, red_f)
+                                              : jobsched_makespan<BLOCK>(sk, n, sd.jt, sd.machines, red_f);
             } else {
                 row_argsort<BLOCK, G>(k, n, (kind == TSPJ) ? n / 2 : n, s, warp_tot);
                 zero_counters<BLOCK, G>(s);  // ready for the next row (separated by the row-end barrier)
@@ -724,7 +821,7 @@ __global__ void __launch_bounds__(kBigBlock) row_kernel_big(RowLaunch L) {
     __shared__ PopDesc sd;
     __shared__ uint32_t warp_tot[32];
     __shared__ long long red_ll[32];
-    __shared__ float red_f[16];
+    __shared__ float red_f[32];
     __shared__ long long misc[4];
     const int t = threadIdx.x;
     unsigned char* base = static_cast<unsigned char*>(L.gscratch) + (size_t)blockIdx.x * L.gstride;
@@ -892,6 +989,10 @@ __global__ void __launch_bounds__(kBigBlock) row_kernel_big(RowLaunch L) {
             tv = block_sum_ll<BLOCK>(tv, red_ll);
             const float twf = (float)tw, tvf = (float)tv;
             res[0] = (twf > sd.cap) ? __fsub_rn(tvf, __fmul_rn(__fsub_rn(twf, sd.cap), 1000.0f)) : tvf;
+        } else if (kind == CONTINUOUS) {
+            res[0] = continuous_fitness<BLOCK>(row, n, sd.function, sd.lo, sd.hi, red_f);
+        } else if (kind == JOBSCHED) {
+            res[0] = jobsched_makespan<BLOCK>(row, n, sd.jt, sd.machines, red_f);
         } else {
             // stable argsort by (okey, index): bucket histogram, scan, scatter, rank in bucket
             const int NB = round_up(n, BLOCK);

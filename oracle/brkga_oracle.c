@@ -195,6 +195,73 @@ void orc_decode_problem(const orc_problem* pb, const float* keys, int32_t* perm)
     }
 }
 
+/* JobSchedulingGPUConfig::calculate_scheduling_fitness (configs/job_scheduling_gpu_config.hpp:132-148) */
+static float jobsched_makespan(const orc_problem* pb, const float* keys) {
+    int M = pb->machines;
+    float* load = (float*)calloc((size_t)M, sizeof(float));
+    for (int i = 0; i < pb->n; ++i) {
+        int m = (int)(keys[i] * (float)M);
+        if (m >= M) m = M - 1;
+        if (m < 0) m = 0;
+        load[m] += pb->jt[i];
+    }
+    float best = load[0];
+    for (int m = 1; m < M; ++m)
+        if (best < load[m]) best = load[m];
+    free(load);
+    return best;
+}
+
+/* ContinuousOptGPUConfig::calculate_sphere / _rastrigin / _rosenbrock
+ * (configs/continuous_opt_gpu_config.hpp:131-173), float arithmetic in the same order */
+static float continuous_value(const orc_problem* pb, const float* keys) {
+    const float range = pb->hi - pb->lo;
+    const int n = pb->n;
+    if (pb->function == 1) {
+        const float A = 10.0f, PI = 3.14159265358979323846f;
+        float sum = A * (float)n;
+        for (int i = 0; i < n; ++i) {
+            float x = keys[i] * range + pb->lo;
+            sum += x * x - A * cosf(2 * PI * x);
+        }
+        return sum;
+    }
+    float sum = 0.0f;
+    if (pb->function == 2) {
+        for (int i = 0; i + 1 < n; ++i) {
+            float x = keys[i] * range + pb->lo;
+            float xn = keys[i + 1] * range + pb->lo;
+            float t1 = xn - x * x;
+            float t2 = 1 - x;
+            sum += 100 * t1 * t1 + t2 * t2;
+        }
+        return sum;
+    }
+    for (int i = 0; i < n; ++i) {
+        float x = keys[i] * range + pb->lo;
+        sum += x * x;
+    }
+    return sum;
+}
+
+static double continuous_value64(const orc_problem* pb, const float* keys) {
+    const double range = (double)pb->hi - (double)pb->lo;
+    const int n = pb->n;
+    double sum = (pb->function == 1) ? 10.0 * n : 0.0;
+    for (int i = 0; i < n; ++i) {
+        double x = keys[i] * range + pb->lo;
+        if (pb->function == 0) sum += x * x;
+        else if (pb->function == 1) sum += x * x - 10.0 * cos(2.0 * 3.14159265358979323846 * x);
+        else if (i + 1 < n) {
+            double xn = keys[i + 1] * range + pb->lo;
+            sum += 100.0 * (xn - x * x) * (xn - x * x) + (1.0 - x) * (1.0 - x);
+        }
+    }
+    return sum;
+}
+
+double orc_continuous_f64(const orc_problem* pb, const float* keys) { return continuous_value64(pb, keys); }
+
 static float knap_greedy(const orc_problem* pb, const int32_t* perm) {
     /* first-fit in key order: take item iff the running weight stays <= capacity */
     int64_t cap = (int64_t)floor((double)pb->cap);
@@ -244,6 +311,8 @@ void orc_eval_perm(const orc_problem* pb, const int32_t* perm, const float* keys
     case ORC_KNAP_THRESHOLD: out[0] = knap_threshold(pb, keys); break;
     case ORC_KNAP_GREEDY: out[0] = knap_greedy(pb, perm); break;
     case ORC_TSPJ: out[0] = tspj_makespan(pb, perm); break;
+    case ORC_JOBSCHED: out[0] = jobsched_makespan(pb, keys); break;
+    case ORC_CONTINUOUS: out[0] = continuous_value(pb, keys); break;
     default: out[0] = NAN;
     }
 }
@@ -294,7 +363,8 @@ void orc_evaluate(const orc_problem* pb, const float* keys, int rows, int ld, fl
     int32_t* perm = (int32_t*)malloc(sizeof(int32_t) * (size_t)(pb->n > 0 ? pb->n : 1));
     for (int r = 0; r < rows; ++r) {
         const float* k = keys + (size_t)r * ld;
-        if (pb->kind != ORC_KNAP_THRESHOLD) orc_decode_problem(pb, k, perm);
+        if (pb->kind != ORC_KNAP_THRESHOLD && pb->kind != ORC_JOBSCHED && pb->kind != ORC_CONTINUOUS)
+            orc_decode_problem(pb, k, perm);
         orc_eval_perm(pb, perm, k, fit + (size_t)r * m);
     }
     free(perm);

@@ -70,8 +70,11 @@ enum {
     ORC_KNAP_GREEDY = 4,      /* key-order first-fit greedy (no reference counterpart)  */
     ORC_BITSP_COORDS = 5,     /* depot tour, two coordinate sets [n+1][2]               */
     ORC_BITSP_MATRIX = 6,     /* depot tour, two [n+1][n+1] matrices, configs/multi_tsp_config.hpp:54-103 */
-    ORC_TSPJ = 7              /* n = 2c genes; mat = travel [c+1][c+1], mat2 = job durations [c+1][c+1],
+    ORC_TSPJ = 7,             /* n = 2c genes; mat = travel [c+1][c+1], mat2 = job durations [c+1][c+1],
                                  configs/tspj_config.hpp:555-626                                       */
+    ORC_JOBSCHED = 8,         /* jt [n], machines: makespan, configs/job_scheduling_gpu_config.hpp:132-148 */
+    ORC_CONTINUOUS = 9        /* function 0 sphere / 1 Rastrigin / 2 Rosenbrock over [lo, hi],
+                                 configs/continuous_opt_gpu_config.hpp:114-173                        */
 };
 
 typedef struct {
@@ -84,6 +87,10 @@ typedef struct {
     const int32_t* w;      /* knapsack weights [n]                                 */
     const int32_t* v;      /* knapsack values  [n]                                 */
     float cap;             /* knapsack capacity                                    */
+    const float* jt;       /* job scheduling: job times [n]                        */
+    int32_t machines;
+    int32_t function;      /* continuous: function and bounds                      */
+    float lo, hi;
 } orc_problem;
 
 int orc_num_objectives(const orc_problem* pb);
@@ -107,6 +114,8 @@ void orc_eval_perm(const orc_problem* pb, const int32_t* perm, const float* keys
  * skipped when j - i < 2); the row and fit[row] change only if the makespan improved. */
 void orc_local_search(const orc_problem* pb, float* pop, float* fit, const int32_t* rows, int count, int ld,
                       int moves, uint64_t seed, uint32_t gen, int island);
+/* continuous objective in double precision (the tolerance reference for Rastrigin) */
+double orc_continuous_f64(const orc_problem* pb, const float* keys);
 /* the problem's decode of one chromosome (two argsorts for TSPJ, see orc_evaluate) */
 void orc_decode_problem(const orc_problem* pb, const float* keys, int32_t* perm);
 /* FP64 restatement of the same objective (tour lengths only), for error bounds */

@@ -17,6 +17,7 @@ LIB_PATH = os.path.join(HERE, "liboracle.so")
 REF_PATH = os.path.join(HERE, "_ref", "libref.so")
 
 TSP_COORDS, TSP_MATRIX, KNAP_THRESHOLD, KNAP_GREEDY, BITSP_COORDS, BITSP_MATRIX, TSPJ = 1, 2, 3, 4, 5, 6, 7
+JOBSCHED, CONTINUOUS = 8, 9
 
 _f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
 _f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
@@ -33,6 +34,7 @@ class Problem(C.Structure):
         ("kind", C.c_int32), ("n", C.c_int32),
         ("xy", C.c_void_p), ("xy2", C.c_void_p), ("mat", C.c_void_p), ("mat2", C.c_void_p),
         ("w", C.c_void_p), ("v", C.c_void_p), ("cap", C.c_float),
+        ("jt", C.c_void_p), ("machines", C.c_int32), ("function", C.c_int32), ("lo", C.c_float), ("hi", C.c_float),
     ]
 
 
@@ -69,6 +71,8 @@ def lib():
         L.orc_canon_sum.argtypes = [_f32p, C.c_int]
         L.orc_eval_perm.argtypes = [C.POINTER(Problem), _i32p, _f32p, _f32p]
         L.orc_decode_problem.argtypes = [C.POINTER(Problem), _f32p, _i32p]
+        L.orc_continuous_f64.restype = C.c_double
+        L.orc_continuous_f64.argtypes = [C.POINTER(Problem), _f32p]
         L.orc_local_search.argtypes = [C.POINTER(Problem), _f32p, _f32p, _i32p, C.c_int, C.c_int, C.c_int,
                                        C.c_uint64, C.c_uint32, C.c_int]
         L.orc_eval_perm_f64.argtypes = [C.POINTER(Problem), _i32p, _f64p]
@@ -110,7 +114,8 @@ def lib():
 # problem construction (keeps numpy buffers alive on the returned object)
 # ---------------------------------------------------------------------------------------
 class OracleProblem:
-    def __init__(self, kind, n, xy=None, xy2=None, mat=None, mat2=None, w=None, v=None, cap=0.0):
+    def __init__(self, kind, n, xy=None, xy2=None, mat=None, mat2=None, w=None, v=None, cap=0.0, jt=None,
+                 machines=0, function=0, lo=0.0, hi=0.0):
         self.kind, self.n = kind, n
         self._keep = []
 
@@ -122,7 +127,8 @@ class OracleProblem:
             return a.ctypes.data
 
         self.s = Problem(kind, n, ptr(xy, np.float32), ptr(xy2, np.float32), ptr(mat, np.float32),
-                         ptr(mat2, np.float32), ptr(w, np.int32), ptr(v, np.int32), float(cap))
+                         ptr(mat2, np.float32), ptr(w, np.int32), ptr(v, np.int32), float(cap),
+                         ptr(jt, np.float32), int(machines), int(function), float(lo), float(hi))
 
     @property
     def m(self):
@@ -166,6 +172,11 @@ def local_search(pb: OracleProblem, pop, fit, rows, count, ld, moves, seed, gen,
     """TSPJ random 2-opt on rows[:count] (in place)"""
     lib().orc_local_search(C.byref(pb.s), pop, fit, np.ascontiguousarray(rows, np.int32), count, ld, moves,
                            seed, gen, island)
+
+
+def continuous_f64(pb: OracleProblem, keys):
+    keys = np.ascontiguousarray(np.atleast_2d(keys)[:, :pb.n], dtype=np.float32)
+    return np.array([lib().orc_continuous_f64(C.byref(pb.s), np.ascontiguousarray(r)) for r in keys])
 
 
 def decode_problem(pb: OracleProblem, keys):
@@ -305,6 +316,8 @@ def ref():
         R.ref_knap_eval.argtypes = [_f32p, _f32p, C.c_float, C.c_int, _f32p, C.c_int, _f32p]
         R.ref_bitsp_eval.argtypes = [_f32p, _f32p, C.c_int, _f32p, C.c_int, _f32p]
         R.ref_tspj_eval.argtypes = [_f32p, _f32p, C.c_int, _f32p, C.c_int, _f32p, C.c_void_p]
+        R.ref_job_eval.argtypes = [_f32p, C.c_int, C.c_int, _f32p, C.c_int, _f32p]
+        R.ref_cont_eval.argtypes = [C.c_int, C.c_float, C.c_float, C.c_int, _f32p, C.c_int, _f32p]
         R.ref_pareto.argtypes = [_f32p, C.c_int, _i32p, _f32p]
         R.ref_nsga2_select.argtypes = [_f32p, C.c_int, C.c_int, _i32p]
         R.ref_brkga_generation.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_uint32,

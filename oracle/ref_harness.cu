@@ -50,6 +50,8 @@
 #include "configs/knapsack_config.hpp"
 #include "configs/multi_tsp_config.hpp"
 #include "configs/tspj_config.hpp"
+#include "configs/job_scheduling_gpu_config.hpp"
+#include "configs/continuous_opt_gpu_config.hpp"
 #undef private
 #undef protected
 
@@ -161,6 +163,40 @@ int ref_tspj_eval(const float* travel, const float* jobs, int dim, const float* 
                     perm[(size_t)r * 2 * c + c + i] = (int32_t)sol[1][i];
                 }
             }
+        }
+        return 0;
+    } catch (...) {
+        return -1;
+    }
+}
+
+// JobSchedulingGPUConfig::fitness_function (configs/job_scheduling_gpu_config.hpp:132-148)
+int ref_job_eval(const float* jt, int n, int machines, const float* keys, int rows, float* fit) {
+    try {
+        JobSchedulingGPUConfig<float> cfg(std::vector<float>(jt, jt + n), machines, "ref");
+        Individual<float> ind(n);
+        for (int r = 0; r < rows; r++) {
+            set_keys(ind, keys + (size_t)r * n, n);
+            fit[r] = cfg.fitness_function(ind);
+        }
+        return 0;
+    } catch (...) {
+        return -1;
+    }
+}
+
+// ContinuousOptGPUConfig::fitness_function (configs/continuous_opt_gpu_config.hpp:114-173);
+// function 0 sphere, 1 Rastrigin, 2 Rosenbrock
+int ref_cont_eval(int function, float lower, float upper, int n, const float* keys, int rows, float* fit) {
+    try {
+        const OptimizationFunction f = function == 1   ? OptimizationFunction::RASTRIGIN
+                                       : function == 2 ? OptimizationFunction::ROSENBROCK
+                                                       : OptimizationFunction::SPHERE;
+        ContinuousOptGPUConfig<float> cfg(n, lower, upper, f, "ref");
+        Individual<float> ind(n);
+        for (int r = 0; r < rows; r++) {
+            set_keys(ind, keys + (size_t)r * n, n);
+            fit[r] = cfg.fitness_function(ind);
         }
         return 0;
     } catch (...) {

@@ -183,6 +183,41 @@ def check_tspj(d):
     assert np.max(np.abs(f64 - d["fit"]) / np.maximum(f64, 1e-30)) <= 1e-5
 
 
+def ref_job_case(n, machines, rows, seed):
+    R = O.ref()
+    rng = np.random.default_rng(seed)
+    jt = (1.0 + rng.random(n) * 99.0).astype(np.float32)
+    keys = I.keys(rows, n, seed + 1)
+    fit = np.zeros(rows, np.float32)
+    assert R.ref_job_eval(jt, n, machines, keys, rows, fit) == 0
+    return dict(jt=jt, machines=np.int32(machines), keys=keys, fit=fit)
+
+
+def check_job(d):
+    n = d["keys"].shape[1]
+    pb = O.OracleProblem(O.JOBSCHED, n, jt=d["jt"], machines=int(d["machines"]))
+    np.testing.assert_array_equal(O.evaluate(pb, d["keys"]).view(np.uint32), d["fit"].view(np.uint32))
+
+
+CONT_BOUNDS = {0: (-5.12, 5.12), 1: (-5.12, 5.12), 2: (-5.0, 10.0)}  # create_sphere/_rastrigin/_rosenbrock
+
+
+def ref_cont_case(function, n, rows, seed):
+    R = O.ref()
+    lo, hi = CONT_BOUNDS[function]
+    keys = I.keys(rows, n, seed)
+    fit = np.zeros(rows, np.float32)
+    assert R.ref_cont_eval(function, lo, hi, n, keys, rows, fit) == 0
+    return dict(function=np.int32(function), lo=np.float32(lo), hi=np.float32(hi), keys=keys, fit=fit)
+
+
+def check_cont(d):
+    n = d["keys"].shape[1]
+    pb = O.OracleProblem(O.CONTINUOUS, n, function=int(d["function"]), lo=float(d["lo"]), hi=float(d["hi"]))
+    # the oracle adds in the reference's order with the same libm: bit-exact
+    np.testing.assert_array_equal(O.evaluate(pb, d["keys"]).view(np.uint32), d["fit"].view(np.uint32))
+
+
 def check_pareto(d, crowd=True):
     rank = O.pareto_ranks(d["obj"])
     np.testing.assert_array_equal(rank, d["rank"])
@@ -239,6 +274,8 @@ LIVE = {
     "bitsp": lambda: [check_bitsp(ref_bitsp_case(n, 8, n)) for n in (1, 20, 300)],
     "tspj": lambda: [check_tspj(ref_tspj_case(c, 8, 40 + c)) for c in (1, 2, 5, 52, 300)],
     "tspj_ties": lambda: [check_tspj(ref_tspj_case(c, 8, 50 + c, key_fn=I.tied_keys)) for c in (6, 100)],
+    "jobsched": lambda: [check_job(ref_job_case(n, M, 8, n + M)) for (n, M) in ((1, 1), (50, 5), (300, 32), (1000, 70))],
+    "continuous": lambda: [check_cont(ref_cont_case(f, n, 8, 7 * f + n)) for f in (0, 1, 2) for n in (1, 2, 30, 500)],
     "pareto": lambda: [check_pareto(ref_pareto_case(N, N, False)) for N in (1, 2, 3, 500, 4096)],
     "pareto_dup": lambda: [check_pareto(ref_pareto_case(N, N, True), crowd=False) for N in (64, 2048)],
     "select": lambda: [check_select(ref_select_case(N, N // 2, N)) for N in (40, 1000)],

@@ -201,3 +201,25 @@ def test_cpp_dropin_program(cuda, tmp_path):
     _, perm, fit = s.get_best_individual()
     assert np.float32(out["best"]) == fit
     assert out["tour"] == perm.tolist()
+
+
+def test_cpp_knapsack_files(cuda, tmp_path):
+    """KnapsackConfig::load_from_file reads the reference's text and CSV layouts to the same
+    instance, and the drop-in solve equals the Python binding's"""
+    import json
+    import os
+    import subprocess
+    exe = os.path.join(os.path.dirname(B().LIB_PATH), "..", "build", "solve_knapsack")
+    r = subprocess.run([exe, str(tmp_path), "60", "4", "50"], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    out = json.loads(r.stdout.strip().splitlines()[-1])
+    rows = [l.split() for l in open(tmp_path / "items.txt") if l.strip() and not l.startswith("#")]
+    n, cap = int(rows[0][0]), float(rows[0][1])
+    w = np.array([int(a) for a, _ in rows[1:]], np.int32)
+    v = np.array([int(b) for _, b in rows[1:]], np.int32)
+    assert len(w) == n and cap == out["capacity"]
+    s = B().Solver(B().knapsack(w, v, cap, greedy=False), B().params(400, 80, 40, 0.7, 50, seed=5))
+    s.run()
+    best = s.get_best_individual()[2]
+    assert np.float32(out["txt"]) == best and np.float32(out["csv"]) == best
+    s.close()
