@@ -331,6 +331,9 @@ def run_ours(args, rank, world):
                          "algorithmic_bytes_per_launch": alg, "kernel_ms": row_ms, "peak_kind": peak_kind,
                          "sort_kernel_ms": sort_ms},
             "gpu_launches": 2 * args.steps,
+            # rows decoded and evaluated per generation: children and mutants (elites keep
+            # their fitness, as the reference's host path does)
+            "individual_evaluations_per_s": value * (POP - ELITE),
             "clocks": clocks.summary(),
             "best_tour": best,
             "l2_warm_back_to_back_gens_per_s": warm_gens_per_s,
@@ -535,7 +538,7 @@ def workload_serve(args):
             "generations": gens, "max_active": args.max_active, "tick": args.tick}
 
 
-def reference_quality(xy, runs, gens):
+def reference_quality(xy, runs, gens, P=256, E=51, M=25):
     """best tour length of `runs` runs of the reference's own Solver on its CPU path
     (oracle/_ref, CUDA hidden); the reference seeds each run from the clock"""
     code = f"""
@@ -549,7 +552,7 @@ R = O.ref()
 xy = np.array({xy.tolist()!r}, dtype=np.float32)
 out = []
 for r in range({runs}):
-    h = R.ref_solver_create(1, {len(xy)}, xy.ctypes.data, None, None, None, 0.0, 256, 51, 25, 0.7)
+    h = R.ref_solver_create(1, {len(xy)}, xy.ctypes.data, None, None, None, 0.0, {P}, {E}, {M}, 0.7)
     R.ref_solver_evolve(h, {gens})
     out.append(R.ref_solver_best(h))
     R.ref_solver_destroy(h)
@@ -596,11 +599,26 @@ def workload_quality(args):
         s.run()
         same += int(np.float32(s.get_best_individual()[2]) == np.float32(ours[i]))
         s.close()
+    # the headline scale too, on fewer runs (the reference's CPU path takes about 0.09 s
+    # per generation there): TSP n=1000, P=2048, E=M=307, 100 generations, 4 runs each
+    xy2 = instance()
+    pb2 = B.tsp(xy2)
+    big = []
+    for sd in range(1, 5):
+        s = B.Solver(pb2, B.params(POP, ELITE, MUTANTS, RHO, 100, seed=sd))
+        s.run()
+        big.append(float(s.get_best_individual()[2]))
+        s.close()
+    out_big = {"ours_100_generations": _stats(big)}
     out = {"metric": "best tour over 32 seeds, TSP n=52 pop 256, 500 generations", "unit": "tour length",
+           "tsp1000_pop2048": out_big,
            "ours": _stats(ours), "ours_seconds_32_runs": secs, "ours_fp32_vs_fp64_max_rel": max(rel),
            "plain_solver_identical": f"{same}/{len(range(0, runs, 8))}", "generations": gens}
     if not args.no_cpu:
         ref = reference_quality(xy, runs, gens)
+        ref_big = reference_quality(xy2, 4, 100, P=POP, E=ELITE, M=MUTANTS)
+        if isinstance(ref_big, list):
+            out_big["reference_100_generations"] = _stats(ref_big)
         if isinstance(ref, list):
             out["reference"] = _stats(ref)
             out["mean_ours_minus_reference_rel"] = (out["ours"]["mean"] - out["reference"]["mean"]) / \
