@@ -430,10 +430,11 @@ __device__ __forceinline__ int tourn(int i1, int i2, const int32_t* rank, const 
     return i2;
 }
 
-// residency target: 1536 threads per SM for one float4 group per thread, 1024 otherwise
+// residency target: 1280 threads per SM for one float4 group per thread, 1024 otherwise
+// (measured at n = 1000: 5 CTAs of 256 with 51 registers beat 6 with 40 and 8 with 32)
 template <int BLOCK, int G>
 struct RowResidency {
-    static constexpr int want = (G == 1 ? 1536 : 1024) / BLOCK;
+    static constexpr int want = (G == 1 ? 1280 : 1024) / BLOCK;
     static constexpr int value = want < 1 ? 1 : (want > 32 ? 32 : want);
 };
 
