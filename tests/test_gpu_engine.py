@@ -93,15 +93,17 @@ def test_engine_knapsack_greedy(cuda):
     assert np.all(np.diff(rh) >= 0)  # elitism: the best never gets worse (maximise)
 
 
-def test_engine_islands_migration(cuda):
-    n, P, E, M, k, G = 60, 256, 40, 24, 4, 23
+@pytest.mark.parametrize("G,interval", [(23, 5), (45, 20)])
+def test_engine_islands_migration(cuda, G, interval):
+    # (45, 20): runs of 16 generations in one captured graph between migrations
+    n, P, E, M, k = 60, 256, 40, 24, 4
     xy = I.tsp_coords(n, seed=4)
     pb, po = B().tsp(xy), O.OracleProblem(O.TSP_COORDS, n, xy=xy)
-    prm = B().params(P, E, M, 0.7, G, seed=11, num_islands=k, migration_interval=5, num_migrants=2)
+    prm = B().params(P, E, M, 0.7, G, seed=11, num_islands=k, migration_interval=interval, num_migrants=2)
     s = B().Solver(pb, prm)
     s.run()
     keys, fit = s.get_population()
-    rk, rf, rh = oracle_islands(po, P, E, M, 0.7, 11, k, 5, 2, G, 60)
+    rk, rf, rh = oracle_islands(po, P, E, M, 0.7, 11, k, interval, 2, G, 60)
     np.testing.assert_array_equal(keys, rk)
     np.testing.assert_array_equal(fit, rf)
     np.testing.assert_array_equal(s.get_fitness_history(), rh)

@@ -125,18 +125,18 @@ def oracle_run_ls(po, P, E, M, rho, seed, k, G, ld, interval, count, moves, mig_
     return keys, fit, np.array(hist, np.float32)
 
 
-@pytest.mark.parametrize("k", [1, 2])
-def test_engine_local_search_bit_exact(cuda, k):
-    c, P, E, M, G = 30, 160, 40, 16, 12
+@pytest.mark.parametrize("k,G,mig", [(1, 12, 0), (2, 12, 5), (1, 36, 0), (2, 36, 20)])
+def test_engine_local_search_bit_exact(cuda, k, G, mig):
+    # G = 36: runs of 16 generations in one captured graph, local search inside them
+    c, P, E, M = 30, 160, 40, 16
     pb, po = problems(c, seed=40 + k)
-    prm = B().params(P, E, M, 0.75, G, seed=5, num_islands=k, migration_interval=5 if k > 1 else 0,
-                     num_migrants=2 if k > 1 else 0, local_search_interval=2, local_search_individuals=100,
+    prm = B().params(P, E, M, 0.75, G, seed=5, num_islands=k, migration_interval=mig,
+                     num_migrants=2 if mig else 0, local_search_interval=2, local_search_individuals=100,
                      local_search_moves=5)
     s = B().Solver(pb, prm)
     s.run()
     keys, fit = s.get_population()
-    rk, rf, rh = oracle_run_ls(po, P, E, M, 0.75, 5, k, G, (2 * c + 3) // 4 * 4, 2, 100, 5,
-                               5 if k > 1 else 0, 2)
+    rk, rf, rh = oracle_run_ls(po, P, E, M, 0.75, 5, k, G, (2 * c + 3) // 4 * 4, 2, 100, 5, mig, 2)
     np.testing.assert_array_equal(keys, rk)
     np.testing.assert_array_equal(fit, rf)
     np.testing.assert_array_equal(s.get_fitness_history(), rh)
