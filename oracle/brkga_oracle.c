@@ -90,7 +90,7 @@ void orc_decode_rows(const float* keys, int rows, int n, int ld, int32_t* perm) 
 /* problems                                                                         */
 /* ================================================================================ */
 int orc_num_objectives(const orc_problem* pb) {
-    return (pb->kind == ORC_BITSP_COORDS || pb->kind == ORC_BITSP_MATRIX) ? 2 : 1;
+    return (pb->kind == ORC_BITSP_COORDS || pb->kind == ORC_BITSP_MATRIX || pb->kind == ORC_MOVRP) ? 2 : 1;
 }
 int orc_maximize(const orc_problem* pb) {
     return pb->kind == ORC_KNAP_THRESHOLD || pb->kind == ORC_KNAP_GREEDY;
@@ -184,7 +184,21 @@ static double tspj_makespan64(const orc_problem* pb, const int32_t* perm) {
 /* the decode of one chromosome: one argsort, or for TSPJ one per component (city keys,
  * then job keys: TSPJConfig::decode_solution_internal, configs/tspj_config.hpp:606-626),
  * the second component's positions offset by c */
+void orc_movrp_values(const float* keys, int n, float* val) {
+    float h = 0.0f;
+    for (int i = 0; i < n; ++i) h += keys[i] * (float)(i + 1);
+    const float hb = h * 0.00001f;
+    for (int i = 0; i < n; ++i) val[i] = keys[i] + ((float)i * 0.00001f + hb);
+}
+
 void orc_decode_problem(const orc_problem* pb, const float* keys, int32_t* perm) {
+    if (pb->kind == ORC_MOVRP) {
+        float* val = (float*)malloc(sizeof(float) * (size_t)(pb->n > 0 ? pb->n : 1));
+        orc_movrp_values(keys, pb->n, val);
+        orc_decode(val, pb->n, perm);
+        free(val);
+        return;
+    }
     if (pb->kind == ORC_TSPJ) {
         int c = pb->n / 2;
         orc_decode(keys, c, perm);
@@ -273,6 +287,58 @@ static float knap_greedy(const orc_problem* pb, const int32_t* perm) {
     return (float)cv;
 }
 
+/* MultiObjectiveVRPConfig::decode_routes + decode_solution (configs/multi_objective_vrp_config.hpp:
+ * 214-313): customers in sorted order; a customer whose demand would push a non-empty route
+ * over capacity closes it (back to the depot) and opens the next; route lengths are float
+ * sums in visiting order; objectives are the float sum of route lengths in route order plus
+ * 100 per unit of overload of a route, and the longest route; each vehicle beyond the fleet
+ * adds 500 to both.  route_of (optional) receives the route index of each position. */
+static int movrp_walk(const orc_problem* pb, const int32_t* perm, float* out, int32_t* route_of) {
+    const int n = pb->n, cap = pb->vcap;
+    float dist = 0.0f, total = 0.0f, longest = 0.0f, pen = 0.0f;
+    int load = 0, last = 0, size = 0, routes = 0;
+    for (int j = 0; j < n; ++j) {
+        const int cust = perm[j] + 1, dem = pb->w[cust];
+        if (load + dem > cap && size > 0) {
+            dist += orc_edge(pb->xy, last, 0);
+            total += dist;
+            if (dist > longest) longest = dist;
+            if (load > cap) pen += (float)(load - cap) * 100.0f;
+            ++routes;
+            dist = 0.0f;
+            load = 0;
+            size = 0;
+            last = 0;
+        }
+        dist += orc_edge(pb->xy, last, cust);
+        load += dem;
+        ++size;
+        last = cust;
+        if (route_of) route_of[j] = routes;
+    }
+    if (size > 0) {
+        dist += orc_edge(pb->xy, last, 0);
+        total += dist;
+        if (dist > longest) longest = dist;
+        if (load > cap) pen += (float)(load - cap) * 100.0f;
+        ++routes;
+    }
+    if (out) {
+        out[0] = total + pen;
+        out[1] = longest;
+        if (routes > pb->machines) {
+            const float vp = (float)(routes - pb->machines) * 500.0f;
+            out[0] += vp;
+            out[1] += vp;
+        }
+    }
+    return routes;
+}
+
+int orc_movrp_routes(const orc_problem* pb, const int32_t* perm, int32_t* route_of) {
+    return movrp_walk(pb, perm, NULL, route_of);
+}
+
 void orc_eval_perm(const orc_problem* pb, const int32_t* perm, const float* keys, float* out) {
     int n = pb->n;
     switch (pb->kind) {
@@ -313,6 +379,7 @@ void orc_eval_perm(const orc_problem* pb, const int32_t* perm, const float* keys
     case ORC_TSPJ: out[0] = tspj_makespan(pb, perm); break;
     case ORC_JOBSCHED: out[0] = jobsched_makespan(pb, keys); break;
     case ORC_CONTINUOUS: out[0] = continuous_value(pb, keys); break;
+    case ORC_MOVRP: movrp_walk(pb, perm, out, NULL); break;
     default: out[0] = NAN;
     }
 }

@@ -73,8 +73,12 @@ enum {
     ORC_TSPJ = 7,             /* n = 2c genes; mat = travel [c+1][c+1], mat2 = job durations [c+1][c+1],
                                  configs/tspj_config.hpp:555-626                                       */
     ORC_JOBSCHED = 8,         /* jt [n], machines: makespan, configs/job_scheduling_gpu_config.hpp:132-148 */
-    ORC_CONTINUOUS = 9        /* function 0 sphere / 1 Rastrigin / 2 Rosenbrock over [lo, hi],
+    ORC_CONTINUOUS = 9,       /* function 0 sphere / 1 Rastrigin / 2 Rosenbrock over [lo, hi],
                                  configs/continuous_opt_gpu_config.hpp:114-173                        */
+    ORC_MOVRP = 10            /* n customers; xy [n+1][2] (node 0 = depot), w = demands [n+1],
+                                 vcap = vehicle capacity, machines = vehicles; objectives (total
+                                 distance + penalties, longest route + penalty),
+                                 configs/multi_objective_vrp_config.hpp:214-313                       */
 };
 
 typedef struct {
@@ -91,6 +95,7 @@ typedef struct {
     int32_t machines;
     int32_t function;      /* continuous: function and bounds                      */
     float lo, hi;
+    int32_t vcap;          /* MO-VRP vehicle capacity                              */
 } orc_problem;
 
 int orc_num_objectives(const orc_problem* pb);
@@ -116,8 +121,16 @@ void orc_local_search(const orc_problem* pb, float* pop, float* fit, const int32
                       int moves, uint64_t seed, uint32_t gen, int island);
 /* continuous objective in double precision (the tolerance reference for Rastrigin) */
 double orc_continuous_f64(const orc_problem* pb, const float* keys);
-/* the problem's decode of one chromosome (two argsorts for TSPJ, see orc_evaluate) */
+/* the problem's decode of one chromosome (two argsorts for TSPJ, see orc_evaluate; for
+ * MO-VRP the argsort of the biased values of orc_movrp_values) */
 void orc_decode_problem(const orc_problem* pb, const float* keys, int32_t* perm);
+/* MultiObjectiveVRPConfig::decode_routes sort values (configs/multi_objective_vrp_config.hpp:
+ * 219-230): h = sequential float sum of key[i] * (i + 1); value[i] = key[i] + (i * 1e-5f +
+ * h * 1e-5f), all in float without contraction */
+void orc_movrp_values(const float* keys, int n, float* val);
+/* MO-VRP routes of a decoded row: route index per sorted position (route_of[j] for
+ * customer perm[j] + 1); returns the route count */
+int orc_movrp_routes(const orc_problem* pb, const int32_t* perm, int32_t* route_of);
 /* FP64 restatement of the same objective (tour lengths only), for error bounds */
 void orc_eval_perm_f64(const orc_problem* pb, const int32_t* perm, double* out);
 /* sequential FP32 tour sum in the reference's order (configs/tsp_config.hpp:186-190) */

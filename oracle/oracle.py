@@ -18,6 +18,7 @@ REF_PATH = os.path.join(HERE, "_ref", "libref.so")
 
 TSP_COORDS, TSP_MATRIX, KNAP_THRESHOLD, KNAP_GREEDY, BITSP_COORDS, BITSP_MATRIX, TSPJ = 1, 2, 3, 4, 5, 6, 7
 JOBSCHED, CONTINUOUS = 8, 9
+MOVRP = 10
 
 _f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
 _f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
@@ -35,6 +36,7 @@ class Problem(C.Structure):
         ("xy", C.c_void_p), ("xy2", C.c_void_p), ("mat", C.c_void_p), ("mat2", C.c_void_p),
         ("w", C.c_void_p), ("v", C.c_void_p), ("cap", C.c_float),
         ("jt", C.c_void_p), ("machines", C.c_int32), ("function", C.c_int32), ("lo", C.c_float), ("hi", C.c_float),
+        ("vcap", C.c_int32),
     ]
 
 
@@ -71,6 +73,9 @@ def lib():
         L.orc_canon_sum.argtypes = [_f32p, C.c_int]
         L.orc_eval_perm.argtypes = [C.POINTER(Problem), _i32p, _f32p, _f32p]
         L.orc_decode_problem.argtypes = [C.POINTER(Problem), _f32p, _i32p]
+        L.orc_movrp_values.argtypes = [_f32p, C.c_int, _f32p]
+        L.orc_movrp_routes.restype = C.c_int
+        L.orc_movrp_routes.argtypes = [C.POINTER(Problem), _i32p, _i32p]
         L.orc_continuous_f64.restype = C.c_double
         L.orc_continuous_f64.argtypes = [C.POINTER(Problem), _f32p]
         L.orc_local_search.argtypes = [C.POINTER(Problem), _f32p, _f32p, _i32p, C.c_int, C.c_int, C.c_int,
@@ -115,7 +120,7 @@ def lib():
 # ---------------------------------------------------------------------------------------
 class OracleProblem:
     def __init__(self, kind, n, xy=None, xy2=None, mat=None, mat2=None, w=None, v=None, cap=0.0, jt=None,
-                 machines=0, function=0, lo=0.0, hi=0.0):
+                 machines=0, function=0, lo=0.0, hi=0.0, vcap=0):
         self.kind, self.n = kind, n
         self._keep = []
 
@@ -128,11 +133,11 @@ class OracleProblem:
 
         self.s = Problem(kind, n, ptr(xy, np.float32), ptr(xy2, np.float32), ptr(mat, np.float32),
                          ptr(mat2, np.float32), ptr(w, np.int32), ptr(v, np.int32), float(cap),
-                         ptr(jt, np.float32), int(machines), int(function), float(lo), float(hi))
+                         ptr(jt, np.float32), int(machines), int(function), float(lo), float(hi), int(vcap))
 
     @property
     def m(self):
-        return 2 if self.kind in (BITSP_COORDS, BITSP_MATRIX) else 1
+        return 2 if self.kind in (BITSP_COORDS, BITSP_MATRIX, MOVRP) else 1
 
     @property
     def maximize(self):
@@ -317,6 +322,7 @@ def ref():
         R.ref_bitsp_eval.argtypes = [_f32p, _f32p, C.c_int, _f32p, C.c_int, _f32p]
         R.ref_tspj_eval.argtypes = [_f32p, _f32p, C.c_int, _f32p, C.c_int, _f32p, C.c_void_p]
         R.ref_job_eval.argtypes = [_f32p, C.c_int, C.c_int, _f32p, C.c_int, _f32p]
+        R.ref_movrp_eval.argtypes = [_f32p, _i32p, C.c_int, C.c_int, C.c_int, _f32p, C.c_int, _f32p, C.c_void_p]
         R.ref_cont_eval.argtypes = [C.c_int, C.c_float, C.c_float, C.c_int, _f32p, C.c_int, _f32p]
         R.ref_pareto.argtypes = [_f32p, C.c_int, _i32p, _f32p]
         R.ref_nsga2_select.argtypes = [_f32p, C.c_int, C.c_int, _i32p]
@@ -325,6 +331,8 @@ def ref():
         R.ref_nsga2_offspring.argtypes = [_f32p, _f32p, C.c_int, C.c_int, C.c_double, C.c_uint32, _f32p, _i32p,
                                           _f32p, _f32p, _i32p, _u8p, _u8p, _f32p]
         R.ref_solver_create.restype = C.c_void_p
+        R.ref_solver_create_movrp.restype = C.c_void_p
+        R.ref_solver_create_movrp.argtypes = [_f32p, _i32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double]
         R.ref_solver_create.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                         C.c_float, C.c_int, C.c_int, C.c_int, C.c_double]
         R.ref_solver_mode.restype = C.c_char_p
@@ -344,3 +352,19 @@ def coords_matrix(xy):
     dx = xy[:, None, 0] - xy[None, :, 0]
     dy = xy[:, None, 1] - xy[None, :, 1]
     return np.sqrt(dx * dx + dy * dy).astype(np.float32)
+
+
+def movrp_values(keys):
+    """MultiObjectiveVRPConfig's biased sort values of one chromosome"""
+    keys = np.ascontiguousarray(keys, dtype=np.float32)
+    out = np.empty_like(keys)
+    lib().orc_movrp_values(keys, keys.shape[0], out)
+    return out
+
+
+def movrp_routes(pb: OracleProblem, perm):
+    """route index of each sorted position, and the route count"""
+    perm = np.ascontiguousarray(perm, dtype=np.int32)
+    route_of = np.zeros(pb.n, np.int32)
+    count = lib().orc_movrp_routes(C.byref(pb.s), perm, route_of)
+    return route_of, count

@@ -15,6 +15,8 @@
 #include <chrono>
 #include <cmath>
 #include <cstdint>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <filesystem>
 #include <fstream>
@@ -35,6 +37,7 @@
 #include <thread>
 #include <vector>
 #include <omp.h>
+#include <unistd.h>
 #include <cuda_runtime.h>
 #include <curand_kernel.h>
 #include <thrust/copy.h>
@@ -52,6 +55,7 @@
 #include "configs/tspj_config.hpp"
 #include "configs/job_scheduling_gpu_config.hpp"
 #include "configs/continuous_opt_gpu_config.hpp"
+#include "configs/multi_objective_vrp_config.hpp"
 #undef private
 #undef protected
 
@@ -162,6 +166,60 @@ int ref_tspj_eval(const float* travel, const float* jobs, int dim, const float* 
                     perm[(size_t)r * 2 * c + i] = (int32_t)sol[0][i];
                     perm[(size_t)r * 2 * c + c + i] = (int32_t)sol[1][i];
                 }
+            }
+        }
+        return 0;
+    } catch (...) {
+        return -1;
+    }
+}
+
+// MultiObjectiveVRPConfig (configs/multi_objective_vrp_config.hpp) built through its own file
+// reader (load_from_file, :78-165): the instance is written to a temporary file in that format,
+// coordinates with 9 significant digits so that they read back as the same floats.  xy [n+1][2]
+// with the depot first, demands [n+1]; the fleet goes in the name ("-k<V>").
+static std::unique_ptr<MultiObjectiveVRPConfig<float>> load_vrp(const float* xy, const int32_t* demands, int n,
+                                                                int capacity, int vehicles) {
+    char path[] = "/tmp/ref_movrp_XXXXXX";
+    const int fd = mkstemp(path);
+    if (fd < 0) return nullptr;
+    close(fd);
+    {
+        std::ofstream f(path);
+        f << "NAME : ref-n" << (n + 1) << "-k" << vehicles << "\n";
+        f << "DIMENSION : " << (n + 1) << "\n";
+        f << "CAPACITY : " << capacity << "\n";
+        f << "NODE_COORD_SECTION\n";
+        char buf[96];
+        for (int i = 0; i <= n; i++) {
+            std::snprintf(buf, sizeof(buf), "%d %.9g %.9g\n", i + 1, (double)xy[2 * i], (double)xy[2 * i + 1]);
+            f << buf;
+        }
+        f << "DEMAND_SECTION\n";
+        for (int i = 0; i <= n; i++) f << (i + 1) << " " << demands[i] << "\n";
+    }
+    auto cfg = MultiObjectiveVRPConfig<float>::load_from_file(path);
+    std::remove(path);
+    return cfg;
+}
+
+// decode_solution (:280-313) gives both objectives, decode_routes (:214-271) the visiting
+// order; perm receives the customers (1-based) in visiting order
+int ref_movrp_eval(const float* xy, const int32_t* demands, int n, int capacity, int vehicles, const float* keys,
+                   int rows, float* obj, int32_t* perm) {
+    try {
+        auto cfg = load_vrp(xy, demands, n, capacity, vehicles);
+        if (!cfg) return -1;
+        if (cfg->get_num_customers() != n || cfg->get_num_vehicles() != vehicles) return -2;
+        for (int r = 0; r < rows; r++) {
+            const float* row = keys + (size_t)r * n;
+            cfg->decode_solution(row, obj + (size_t)r * 2);
+            if (perm) {
+                auto routes = cfg->decode_routes(row);
+                size_t j = 0;
+                for (const auto& rt : routes)
+                    for (int c : rt.customers) perm[(size_t)r * n + j++] = c;
+                if (j != (size_t)n) return -3;
             }
         }
         return 0;
@@ -389,6 +447,19 @@ void* ref_solver_create(int kind, int n, const float* xy, const float* xy2, cons
                                                                       coords_to_matrix(xy2, n + 1), "ref"),
                                P, E, M, rho);
         }
+    } catch (...) {
+    }
+    return nullptr;
+}
+
+// MO-VRP (NSGA-II) through the same file reader, with the elite / mutant sizes
+// configure_for_size uses (P / 5, P / 6; the NSGA-II generation ignores both)
+void* ref_solver_create_movrp(const float* xy, const int32_t* demands, int n, int capacity, int vehicles, int P,
+                              double rho) {
+    try {
+        auto cfg = load_vrp(xy, demands, n, capacity, vehicles);
+        if (!cfg) return nullptr;
+        return make_solver(std::move(cfg), P, P / 5, P / 6, rho);
     } catch (...) {
     }
     return nullptr;

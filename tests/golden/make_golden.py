@@ -34,6 +34,11 @@ def main():
     out["generation"] = RC.ref_generation_case(n=20, P=40, E=8, M=4, rho=0.7, seed=8)
     out["nsga_offspring"] = RC.ref_nsga_offspring_case(n=15, P=24, rho=0.7, seed=9)
     out["tspj20"] = RC.ref_tspj_case(c=20, rows=16, seed=10)
+    out["movrp31"] = RC.ref_movrp_case(n=31, rows=16, seed=11, vehicles=5)
+    out["movrp_penalties60"] = RC.ref_movrp_case(n=60, rows=8, seed=12, vehicles=2, overload=True)
+    out["jobsched300"] = RC.ref_job_case(n=300, machines=32, rows=16, seed=13)
+    for f, name in enumerate(("sphere", "rastrigin", "rosenbrock")):
+        out["cont_" + name + "30"] = RC.ref_cont_case(function=f, n=30, rows=8, seed=14 + f)
     only = sys.argv[1:]  # optional: names of the fixtures to (re)generate
     for name, d in out.items():
         if only and name not in only:

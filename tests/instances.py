@@ -38,6 +38,22 @@ def wild_keys(rows, n, seed):
     return k
 
 
+def movrp_instance(n, seed, vehicles=None, overload=False):
+    """capacitated VRP over the depot (point 0) and n customers: coordinates uniform in
+    [0,100)^2, demands uniform in {1..30} (depot 0), capacity about 1.1 x total demand /
+    vehicles (vehicles defaults to max(3, n // 6), the reference's own estimate); with
+    overload one customer's demand exceeds the capacity"""
+    rng = np.random.default_rng(seed)
+    xy = (rng.random((n + 1, 2)) * 100.0).astype(np.float32)
+    dem = rng.integers(1, 31, n + 1).astype(np.int32)
+    dem[0] = 0
+    V = vehicles if vehicles is not None else max(3, n // 6)
+    cap = int(np.ceil(1.1 * dem.sum() / V))
+    if overload and n >= 2:
+        dem[1 + n // 2] = cap + 7
+    return xy, dem, cap, V
+
+
 def tspj_instance(c, seed):
     """TSPJ data over the depot and c cities: travel times = Euclidean distances of seeded
     points in [0,100)^2 (as the reference's *_TT.csv files hold), job durations uniform in

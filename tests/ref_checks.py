@@ -199,6 +199,27 @@ def check_job(d):
     np.testing.assert_array_equal(O.evaluate(pb, d["keys"]).view(np.uint32), d["fit"].view(np.uint32))
 
 
+def ref_movrp_case(n, rows, seed, vehicles=None, overload=False, key_fn=None):
+    R = O.ref()
+    xy, dem, cap, V = I.movrp_instance(n, seed, vehicles, overload)
+    keys = (key_fn or I.keys)(rows, n, seed + 1)
+    obj = np.zeros((rows, 2), np.float32)
+    perm = np.zeros((rows, n), np.int32)
+    assert R.ref_movrp_eval(xy, dem, n, cap, V, keys, rows, obj, perm.ctypes.data) == 0
+    return dict(xy=xy, dem=dem, cap=np.int32(cap), vehicles=np.int32(V), keys=keys, obj=obj, perm=perm)
+
+
+def movrp_problem(d):
+    n = d["keys"].shape[1]
+    return O.OracleProblem(O.MOVRP, n, xy=d["xy"], w=d["dem"], machines=int(d["vehicles"]), vcap=int(d["cap"]))
+
+
+def check_movrp(d):
+    pb = movrp_problem(d)
+    np.testing.assert_array_equal(O.decode_problem(pb, d["keys"]) + 1, d["perm"])
+    np.testing.assert_array_equal(O.evaluate(pb, d["keys"]).view(np.uint32), d["obj"].view(np.uint32))
+
+
 CONT_BOUNDS = {0: (-5.12, 5.12), 1: (-5.12, 5.12), 2: (-5.0, 10.0)}  # create_sphere/_rastrigin/_rosenbrock
 
 
@@ -276,6 +297,10 @@ LIVE = {
     "tspj_ties": lambda: [check_tspj(ref_tspj_case(c, 8, 50 + c, key_fn=I.tied_keys)) for c in (6, 100)],
     "jobsched": lambda: [check_job(ref_job_case(n, M, 8, n + M)) for (n, M) in ((1, 1), (50, 5), (300, 32), (1000, 70))],
     "continuous": lambda: [check_cont(ref_cont_case(f, n, 8, 7 * f + n)) for f in (0, 1, 2) for n in (1, 2, 30, 500)],
+    "movrp": lambda: [check_movrp(ref_movrp_case(n, 8, 60 + n, V, ov))
+                      for (n, V, ov) in ((1, None, False), (2, 1, False), (31, 5, False), (31, 2, False),
+                                         (100, None, True), (1000, None, False))],
+    "movrp_ties": lambda: [check_movrp(ref_movrp_case(n, 8, 70 + n, key_fn=I.tied_keys)) for n in (8, 200)],
     "pareto": lambda: [check_pareto(ref_pareto_case(N, N, False)) for N in (1, 2, 3, 500, 4096)],
     "pareto_dup": lambda: [check_pareto(ref_pareto_case(N, N, True), crowd=False) for N in (64, 2048)],
     "select": lambda: [check_select(ref_select_case(N, N // 2, N)) for N in (40, 1000)],

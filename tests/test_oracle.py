@@ -64,6 +64,20 @@ def test_golden_tspj():
     RC.check_tspj(golden("tspj20"))
 
 
+def test_golden_movrp():
+    RC.check_movrp(golden("movrp31"))
+    RC.check_movrp(golden("movrp_penalties60"))
+
+
+def test_golden_jobsched():
+    RC.check_job(golden("jobsched300"))
+
+
+@pytest.mark.parametrize("name", ["sphere", "rastrigin", "rosenbrock"])
+def test_golden_continuous(name):
+    RC.check_cont(golden("cont_" + name + "30"))
+
+
 def test_golden_knapsack_threshold():
     RC.check_knap(golden("knap200"))
 
