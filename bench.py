@@ -388,7 +388,12 @@ sys.path[:0] = [{os.path.join(ROOT, 'oracle')!r}]
 import numpy as np
 import oracle as O
 a = {a!r}
-if a.get('tspj'):
+if a.get('movrp'):
+    rng = np.random.default_rng(a['seed'])
+    xy = (rng.random((a['n'] + 1, 2)) * 100.0).astype(np.float32)
+    dem = rng.integers(1, 31, a['n'] + 1).astype(np.int32)
+    dem[0] = 0
+elif a.get('tspj'):
     rng = np.random.default_rng(a['seed'])
     pts = rng.random((a['n'] + 1, 2)) * 100.0
     xy = np.ascontiguousarray(np.sqrt(((pts[:, None, :] - pts[None, :, :]) ** 2).sum(-1)).astype(np.float32))
@@ -400,8 +405,11 @@ else:
 if not O.ref_available():
     print(json.dumps(dict(value=None))); sys.exit(0)
 R = O.ref()
-h = R.ref_solver_create({kind}, a['n'], xy.ctypes.data, xy2.ctypes.data, None, None, 0.0, a['P'], a['E'], a['M'],
-                        0.75 if a.get('tspj') else 0.7)
+if a.get('movrp'):
+    h = R.ref_solver_create_movrp(xy, dem, a['n'], a['cap'], a['V'], a['P'], 0.10)
+else:
+    h = R.ref_solver_create({kind}, a['n'], xy.ctypes.data, xy2.ctypes.data, None, None, 0.0, a['P'], a['E'],
+                            a['M'], 0.75 if a.get('tspj') else 0.7)
 R.ref_solver_evolve(h, 1)
 g, t = 0, 0.0
 while t < {seconds} and g < {max_gens}:
@@ -628,6 +636,17 @@ def workload_quality(args):
     return out
 
 
+def movrp_instance(n, seed):
+    """depot and n customers uniform in [0,100)^2, demands uniform in {1..30}, the fleet
+    max(3, n // 6) (the reference's estimate) and capacity 1.1 x total demand / fleet"""
+    rng = np.random.default_rng(seed)
+    xy = (rng.random((n + 1, 2)) * 100.0).astype(np.float32)
+    dem = rng.integers(1, 31, n + 1).astype(np.int32)
+    dem[0] = 0
+    V = max(3, n // 6)
+    return xy, dem, int(np.ceil(1.1 * dem.sum() / V)), V
+
+
 def tspj_instance(c, seed):
     """TSPJ data over the depot and c cities: Euclidean travel times of seeded points in
     [0,100)^2, job durations uniform in [1,100) per (city, job type), depot row zero"""
@@ -671,6 +690,15 @@ def run_workload(args):
                                    max_generations=100000, seed=11, local_search_interval=2,
                                    local_search_individuals=100, local_search_moves=5), args.generations, 7,
                               dict(seed=11, tspj=True, n=100, P=1000, E=200, M=100))
+    elif w == "movrp":
+        import brkga_b200 as B
+        # MultiObjectiveVRPConfig at 100 customers: configure_for_size gives population 1500
+        # and rho 0.10 (configs/multi_objective_vrp_config.hpp:190-211); NSGA-II
+        xy, dem, cap, V = movrp_instance(100, 12)
+        out = workload_solver(args, "NSGA-II MO-VRP n=100 pop 1500", lambda: B.movrp(xy, dem, cap, V),
+                              dict(population_size=1500, elite_size=300, mutant_size=0, elite_prob=0.10,
+                                   max_generations=100000, seed=12), args.generations, "movrp",
+                              dict(seed=12, movrp=True, n=100, P=1500, cap=cap, V=V))
     elif w == "batch":
         out = workload_batch(args)
     elif w == "serve":
@@ -715,7 +743,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--profile-op", action="store_true", help="operator kernels only (profiler captures)")
-    ap.add_argument("--workload", default="tsp1000", choices=["tsp1000", "tsp52", "nsga", "tspj", "batch", "serve", "quality"])
+    ap.add_argument("--workload", default="tsp1000",
+                    choices=["tsp1000", "tsp52", "nsga", "tspj", "movrp", "batch", "serve", "quality"])
     ap.add_argument("--generations", type=int, default=500)
     ap.add_argument("--instances", type=int, default=256)
     ap.add_argument("--rate", type=float, default=200.0)

@@ -46,9 +46,13 @@ typedef enum {
     BRKGA_JOBSCHED = 8,          /* JobSchedulingGPUConfig(job_times, machines): gene i puts job i on
                                     machine floor(key * machines); makespan = largest machine load
                                     (configs/job_scheduling_gpu_config.hpp:30-52, 132-148)                  */
-    BRKGA_CONTINUOUS = 9         /* ContinuousOptGPUConfig(n, lower, upper, function): x = key *
+    BRKGA_CONTINUOUS = 9,        /* ContinuousOptGPUConfig(n, lower, upper, function): x = key *
                                     (upper - lower) + lower; sphere / Rastrigin / Rosenbrock
                                     (configs/continuous_opt_gpu_config.hpp:37-57, 114-173)                  */
+    BRKGA_MOVRP = 10             /* MultiObjectiveVRPConfig: capacitated routes from one biased argsort;
+                                    objectives total distance and longest route, with the reference's
+                                    overload and fleet penalties (configs/multi_objective_vrp_config.hpp:
+                                    214-313); two objectives, so runs take the NSGA-II path            */
 } brkga_problem_kind;
 
 /* functions of BRKGA_CONTINUOUS (the reference's OptimizationFunction) */
@@ -63,7 +67,10 @@ typedef enum { BRKGA_FN_SPHERE = 0, BRKGA_FN_RASTRIGIN = 1, BRKGA_FN_ROSENBROCK 
  *             [n+1][n+1], matrix2 = job durations [n+1][n+1] (row = city, column = job
  *             type); chromosomes hold 2n keys, the n city keys then the n job keys
  *   job scheduling: n jobs; job_times [n]; machines >= 1
- *   continuous: n variables; function (brkga_function); lower < upper                  */
+ *   continuous: n variables; function (brkga_function); lower < upper
+ *   MO-VRP:   n customers; coords [n+1][2] with point 0 the depot; demands [n+1] (>= 0,
+ *             the depot's unused); vehicle_capacity >= 1; vehicles >= 1 (the fleet size the
+ *             reference reads from the instance name "-k<V>")                           */
 typedef struct {
     int32_t kind;
     int32_t n;
@@ -79,6 +86,9 @@ typedef struct {
     int32_t function;            /* continuous                                                */
     float lower;
     float upper;
+    const int32_t* demands;      /* MO-VRP                                                    */
+    int32_t vehicle_capacity;
+    int32_t vehicles;
 } brkga_problem_desc;
 
 /* GA parameters (BRKGAConfig fields, core/config.hpp:17-30, plus the engine's own). */

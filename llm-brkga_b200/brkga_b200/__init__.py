@@ -23,6 +23,7 @@ HEADER_PATH = os.path.join(REPO_DIR, "include", "brkga_b200.h")
 
 TSP_COORDS, TSP_MATRIX, KNAP_THRESHOLD, KNAP_GREEDY, BITSP_COORDS, BITSP_MATRIX, TSPJ = 1, 2, 3, 4, 5, 6, 7
 JOBSCHED, CONTINUOUS = 8, 9
+MOVRP = 10
 SPHERE, RASTRIGIN, ROSENBROCK = 0, 1, 2
 
 STATUS = {0: "OK", -1: "INVALID", -2: "OOM", -3: "CUDA", -4: "TIMEOUT", -5: "CANCELLED",
@@ -39,7 +40,8 @@ class ProblemDesc(C.Structure):
     _fields_ = [("kind", C.c_int32), ("n", C.c_int32), ("coords", C.c_void_p), ("coords2", C.c_void_p),
                 ("matrix", C.c_void_p), ("matrix2", C.c_void_p), ("weights", C.c_void_p),
                 ("values", C.c_void_p), ("capacity", C.c_float), ("job_times", C.c_void_p),
-                ("machines", C.c_int32), ("function", C.c_int32), ("lower", C.c_float), ("upper", C.c_float)]
+                ("machines", C.c_int32), ("function", C.c_int32), ("lower", C.c_float), ("upper", C.c_float),
+                ("demands", C.c_void_p), ("vehicle_capacity", C.c_int32), ("vehicles", C.c_int32)]
 
 
 class Params(C.Structure):
@@ -166,7 +168,8 @@ class Problem:
     """Device-resident instance (TSPConfig / KnapsackConfig / MultiTSPConfig data)."""
 
     def __init__(self, kind, n, coords=None, coords2=None, matrix=None, matrix2=None, weights=None, values=None,
-                 capacity=0.0, device=0, job_times=None, machines=0, function=0, lower=0.0, upper=0.0):
+                 capacity=0.0, device=0, job_times=None, machines=0, function=0, lower=0.0, upper=0.0,
+                 demands=None, vehicle_capacity=0, vehicles=0):
         keep = []
 
         def arr(a, dt):
@@ -178,7 +181,8 @@ class Problem:
 
         d = ProblemDesc(kind, n, arr(coords, np.float32), arr(coords2, np.float32), arr(matrix, np.float32),
                         arr(matrix2, np.float32), arr(weights, np.int32), arr(values, np.int32), float(capacity),
-                        arr(job_times, np.float32), int(machines), int(function), float(lower), float(upper))
+                        arr(job_times, np.float32), int(machines), int(function), float(lower), float(upper),
+                        arr(demands, np.int32), int(vehicle_capacity), int(vehicles))
         h = C.c_void_p()
         check(lib().brkga_problem_create(C.byref(d), device, C.byref(h)))
         # n is the chromosome length (genes); a TSPJ instance of c cities has 2c genes
@@ -252,6 +256,32 @@ def jobsched(job_times, machines, device=0):
     floor(key * machines); fitness = makespan"""
     jt = np.asarray(job_times, np.float32)
     return Problem(JOBSCHED, jt.shape[0], job_times=jt, machines=machines, device=device)
+
+
+def movrp(coords, demands, vehicle_capacity, vehicles, device=0):
+    """bi-objective capacitated VRP (MultiObjectiveVRPConfig): coords and demands of the
+    depot (point 0) and n customers; objectives total distance and longest route"""
+    coords = np.asarray(coords, np.float32)
+    return Problem(MOVRP, coords.shape[0] - 1, coords=coords, demands=demands, vehicle_capacity=vehicle_capacity,
+                   vehicles=vehicles, device=device)
+
+
+def movrp_routes(perm, demands, vehicle_capacity):
+    """the routes (customers 1..n in visiting order, as MultiObjectiveVRPConfig::decode_routes
+    lists them) of a row the device decoded, e.g. the permutation of get_best_individual:
+    report formatting only, the objectives come from the device"""
+    routes, cur, load = [], [], 0
+    for g in np.asarray(perm):
+        c = int(g) + 1
+        d = int(demands[c])
+        if load + d > vehicle_capacity and cur:
+            routes.append(cur)
+            cur, load = [], 0
+        cur.append(c)
+        load += d
+    if cur:
+        routes.append(cur)
+    return routes
 
 
 def continuous(n, lower, upper, function=SPHERE, device=0):
@@ -479,7 +509,8 @@ class Server:
             pass
 
     def submit(self, kind, n, prm, stall=0, coords=None, coords2=None, matrix=None, matrix2=None, weights=None,
-               values=None, capacity=0.0, job_times=None, machines=0, function=0, lower=0.0, upper=0.0):
+               values=None, capacity=0.0, job_times=None, machines=0, function=0, lower=0.0, upper=0.0,
+               demands=None, vehicle_capacity=0, vehicles=0):
         keep = []
 
         def arr(a, dt):
@@ -491,7 +522,8 @@ class Server:
 
         d = ProblemDesc(kind, n, arr(coords, np.float32), arr(coords2, np.float32), arr(matrix, np.float32),
                         arr(matrix2, np.float32), arr(weights, np.int32), arr(values, np.int32), float(capacity),
-                        arr(job_times, np.float32), int(machines), int(function), float(lower), float(upper))
+                        arr(job_times, np.float32), int(machines), int(function), float(lower), float(upper),
+                        arr(demands, np.int32), int(vehicle_capacity), int(vehicles))
         rid = C.c_int64()
         check(lib().brkga_server_submit(self.h, C.byref(d), C.byref(prm), stall, C.byref(rid)))
         return rid.value

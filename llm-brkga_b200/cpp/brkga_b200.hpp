@@ -119,6 +119,10 @@ public:
     int local_search_interval = 0;
     int local_search_individuals = 100;
     int local_search_moves = 5;
+    // NSGA-II (two objectives): fresh random offspring per generation.  The reference's
+    // NSGA-II ignores mutant_size (core/solver.hpp:1019-1032), so the default is 0 whatever
+    // mutant_size holds (MultiObjectiveVRPConfig::configure_for_size sets it to P / 6).
+    int nsga2_random_offspring = 0;
 
     explicit BRKGAConfig(int chrom_len) : BRKGAConfig(std::vector<int>{chrom_len}) {}
     explicit BRKGAConfig(const std::vector<int>& lens, int n_objectives = 1)
@@ -457,6 +461,139 @@ private:
 
 // configs/job_scheduling_gpu_config.hpp:16-197: gene i puts job i on machine
 // (int)(key * machines); fitness = makespan (largest machine load), minimised
+// configs/multi_objective_vrp_config.hpp:21-449: a capacitated VRP with two objectives (total
+// distance plus the overload and fleet penalties; the longest route).  Decode and objectives
+// run on the device (BRKGA_MOVRP); runs take the NSGA-II path.
+template <typename T>
+class MultiObjectiveVRPConfig : public DeviceProblemConfig<T> {
+public:
+    struct Customer {
+        int id;
+        T x, y;
+        int demand;
+    };
+    // nodes[0] is the depot; vehicles is the fleet the reference reads from the name ("-k<V>")
+    MultiObjectiveVRPConfig(const std::vector<Customer>& nodes, int vehicle_capacity, int vehicles,
+                            const std::string& name = "MO-VRP")
+        : DeviceProblemConfig<T>(std::vector<int>{(int)nodes.size() - 1}, 2), customers_(nodes),
+          capacity_(vehicle_capacity), vehicles_(vehicles), name_(name) {
+        if (nodes.size() < 2) throw std::invalid_argument("MO-VRP needs a depot and at least one customer");
+        std::vector<float> xy(2 * nodes.size());
+        std::vector<int32_t> dem(nodes.size());
+        for (size_t i = 0; i < nodes.size(); ++i) {
+            xy[2 * i] = (float)nodes[i].x;
+            xy[2 * i + 1] = (float)nodes[i].y;
+            dem[i] = nodes[i].demand;
+        }
+        brkga_problem_desc d{};
+        d.kind = BRKGA_MOVRP;
+        d.n = (int)nodes.size() - 1;
+        d.coords = xy.data();
+        d.demands = dem.data();
+        d.vehicle_capacity = vehicle_capacity;
+        d.vehicles = vehicles;
+        this->create(d);
+        this->update_cuda_grid_size();
+    }
+
+    // configs/multi_objective_vrp_config.hpp:78-165: "NAME : <name>", "DIMENSION : <depot +
+    // customers>", "CAPACITY : <c>", then NODE_COORD_SECTION (id x y, ids from 1, the depot
+    // first) and DEMAND_SECTION (id demand); the fleet is the number after "-k" in the name,
+    // else max(3, customers / 6)
+    static std::unique_ptr<MultiObjectiveVRPConfig<T>> load_from_file(const std::string& filename) {
+        std::ifstream f(filename);
+        if (!f.is_open()) throw std::runtime_error("Cannot open VRP file: " + filename);
+        auto value_after_colon = [](const std::string& line) {
+            const size_t c = line.find(':');
+            std::string v = (c == std::string::npos) ? line : line.substr(c + 1);
+            v.erase(0, v.find_first_not_of(" \t"));
+            v.erase(v.find_last_not_of(" \t\r") + 1);
+            return v;
+        };
+        std::string line, name;
+        int dim = 0, capacity = 0;
+        bool coords = false;
+        while (std::getline(f, line)) {
+            if (line.find("NODE_COORD_SECTION") != std::string::npos) {
+                coords = true;
+                break;
+            }
+            if (line.find("NAME") != std::string::npos && line.find(':') != std::string::npos)
+                name = value_after_colon(line);
+            else if (line.find("DIMENSION") != std::string::npos)
+                dim = std::stoi(value_after_colon(line));
+            else if (line.find("CAPACITY") != std::string::npos)
+                capacity = std::stoi(value_after_colon(line));
+        }
+        if (!coords || dim < 2) throw std::runtime_error("VRP file without NODE_COORD_SECTION: " + filename);
+        std::vector<Customer> nodes(dim, Customer{0, T(0), T(0), 0});
+        for (int i = 0; i < dim; ++i) {
+            int id;
+            T x, y;
+            if (!(f >> id >> x >> y) || id < 1 || id > dim) throw std::runtime_error("bad coordinate line in " + filename);
+            nodes[id - 1] = Customer{id - 1, x, y, 0};
+        }
+        bool demands = false;
+        while (std::getline(f, line))
+            if (line.find("DEMAND_SECTION") != std::string::npos) {
+                demands = true;
+                break;
+            }
+        if (demands)
+            for (int i = 0; i < dim; ++i) {
+                int id, dem;
+                if (!(f >> id >> dem) || id < 1 || id > dim) throw std::runtime_error("bad demand line in " + filename);
+                nodes[id - 1].demand = dem;
+            }
+        const size_t k = name.find("-k");
+        const int vehicles = (k != std::string::npos) ? std::stoi(name.substr(k + 2)) : std::max(3, (dim - 1) / 6);
+        return std::make_unique<MultiObjectiveVRPConfig<T>>(nodes, capacity, vehicles, name);
+    }
+    // configs/multi_objective_vrp_config.hpp:190-211
+    static void configure_for_size(MultiObjectiveVRPConfig<T>* c, int num_customers) {
+        if (num_customers <= 50) {
+            c->population_size = 1000, c->max_generations = 1500;
+        } else if (num_customers <= 100) {
+            c->population_size = 1500, c->max_generations = 2000;
+        } else {
+            c->population_size = 2000, c->max_generations = 2500;
+        }
+        c->elite_size = c->population_size / 5;
+        c->mutant_size = c->population_size / 6;
+        c->elite_prob = 0.10;
+        c->update_cuda_grid_size();
+    }
+    int get_num_customers() const { return (int)customers_.size() - 1; }
+    int get_num_vehicles() const { return vehicles_; }
+    int get_vehicle_capacity() const { return capacity_; }
+    const std::vector<Customer>& get_customers() const { return customers_; }
+    const std::string& get_instance_name() const { return name_; }
+    // the routes (customers 1..n in visiting order) of a device-decoded order such as
+    // Solver::get_best_permutation() -- the split of decode_routes (:236-264), for reports
+    std::vector<std::vector<int>> routes_of(const std::vector<int>& perm) const {
+        std::vector<std::vector<int>> routes;
+        std::vector<int> cur;
+        int load = 0;
+        for (int g : perm) {
+            const int c = g + 1, dem = customers_[c].demand;
+            if (load + dem > capacity_ && !cur.empty()) {
+                routes.push_back(cur);
+                cur.clear();
+                load = 0;
+            }
+            cur.push_back(c);
+            load += dem;
+        }
+        if (!cur.empty()) routes.push_back(cur);
+        return routes;
+    }
+
+private:
+    std::vector<Customer> customers_;
+    int capacity_, vehicles_;
+    std::string name_;
+};
+
 template <typename T>
 class JobSchedulingGPUConfig : public DeviceProblemConfig<T> {
 public:
@@ -664,7 +801,7 @@ public:
         brkga_params_default(&p);
         p.population_size = config_->population_size;
         p.elite_size = config_->elite_size;
-        p.mutant_size = config_->mutant_size;
+        p.mutant_size = config_->num_objectives > 1 ? config_->nsga2_random_offspring : config_->mutant_size;
         p.elite_prob = config_->elite_prob;
         p.max_generations = config_->max_generations;
         p.seed = config_->seed;

@@ -148,6 +148,27 @@ int32_t make_problem(const brkga_problem_desc* d, int device, std::shared_ptr<Pr
         pd->lo = d->lower;
         pd->hi = d->upper;
         break;
+    case BRKGA_MOVRP: {
+        // MultiObjectiveVRPConfig (configs/multi_objective_vrp_config.hpp:78-165): the depot and n
+        // customers; integer demands and capacity; two objectives
+        pd->m = 2;
+        if (!d->coords || !d->demands) return fail(BRKGA_ERR_INVALID, "MO-VRP needs coords and demands");
+        if (d->vehicle_capacity < 1 || d->vehicle_capacity > (1 << 30) || d->vehicles < 1)
+            return fail(BRKGA_ERR_INVALID, "MO-VRP needs 1 <= vehicle_capacity <= 2^30 and vehicles >= 1");
+        for (int i = 0; i <= n; ++i)
+            if (d->demands[i] < 0 || d->demands[i] > (1 << 30))
+                return fail(BRKGA_ERR_INVALID, "MO-VRP demands must lie in [0, 2^30]");
+        if (row_needs_global(n, n + 1, BRKGA_MOVRP))
+            return fail(BRKGA_ERR_UNSUPPORTED, "MO-VRP with " + std::to_string(n) +
+                                                   " customers: rows must fit the shared-memory row kernel");
+        pd->capi = d->vehicle_capacity;
+        pd->machines = d->vehicles;
+        st = upload(*pd, d->coords, (size_t)(n + 1) * 8, &p);
+        pd->xy = (float*)p;
+        if (st == BRKGA_OK) st = upload(*pd, d->demands, (size_t)(n + 1) * 4, &p);
+        pd->w = (int32_t*)p;
+        break;
+    }
     default:
         return fail(BRKGA_ERR_INVALID, "unknown problem kind " + std::to_string(d->kind));
     }
@@ -178,7 +199,9 @@ void fill_instance(PopDesc& d, const ProblemData& pd) {
     d.maximize = pd.maximize;
 }
 
-int points_of(const ProblemData& pd) { return (pd.kind == BRKGA_BITSP_COORDS) ? pd.n + 1 : pd.n; }
+int points_of(const ProblemData& pd) {
+    return (pd.kind == BRKGA_BITSP_COORDS || pd.kind == BRKGA_MOVRP) ? pd.n + 1 : pd.n;
+}
 
 bool stage_fits(const RowTile& t, int n, int pts, int kind) {
     return row_smem_bytes(t, n, pts, kind, true) <= kMaxSmem;

@@ -21,6 +21,7 @@ enum Kind : int32_t {
     TSPJ = 7,
     JOBSCHED = 8,
     CONTINUOUS = 9,
+    MOVRP = 10,  // xy = depot + customers, w = demands, capi = vehicle capacity, machines = vehicles
 };
 
 enum Function : int32_t { FN_SPHERE = 0, FN_RASTRIGIN = 1, FN_ROSENBROCK = 2 };

@@ -1203,6 +1203,300 @@ __global__ void migrate_kernel(PopDesc* descs, int k, int mig) {
 }
 
 // ---------------------------------------------------------------------------------------
+// MO-VRP rows (MultiObjectiveVRPConfig, configs/multi_objective_vrp_config.hpp).  A kernel of
+// their own, so the other kinds' row kernel keeps its registers: it builds rows exactly as
+// the row kernel does in the modes an NSGA-II population uses (initial keys, offspring,
+// diversity refill, given keys), then decodes and scores them:
+//   1. h = the FP32 sum of key_i * (i + 1) in index order (one warp, keys staged in shared
+//      memory); the sort value of gene i is key_i + (i * 1e-5 + h * 1e-5)  (:219-230);
+//   2. a stable argsort of the values, ties to the lower index (std::sort over (value,
+//      customer) pairs);
+//   3. one warp walks the order, closing a route when the next demand would take a
+//      non-empty route over capacity, and forms both objectives with the overload and
+//      fleet penalties in the reference's order of float additions (:233-313).
+// ---------------------------------------------------------------------------------------
+
+// the bucket argsort of row_argsort with buckets over (value - lo) * inv, lo = h * 1e-5 and
+// inv = 1 / (1 + n * 1e-5): the values span about [lo, lo + 1 + n * 1e-5], and any
+// non-decreasing bucket map gives the same (value, index) order
+template <int BLOCK, int G>
+__device__ void movrp_argsort(const float (&v)[G][4], int n, float lo, float inv, const RowSmem& s,
+                              uint32_t* warp_tot) {
+    constexpr int NB = 4 * G * BLOCK;
+    const int t = threadIdx.x;
+    uint32_t bs[G][4];
+#pragma unroll
+    for (int g = 0; g < G; ++g)
+#pragma unroll
+        for (int l = 0; l < 4; ++l) {
+            const int i = 4 * (t + g * BLOCK) + l;
+            if (i < n) {
+                const int b = bucket_of(__fmul_rn(__fsub_rn(v[g][l], lo), inv), (float)NB, NB);
+                bs[g][l] = ((uint32_t)b << 16) | atomicAdd(&s.cnt[b], 1u);
+            }
+        }
+    __syncthreads();
+    uint4 c[G];
+    uint32_t sum = 0;
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+        c[g] = reinterpret_cast<const uint4*>(s.cnt)[t * G + g];
+        sum += c[g].x + c[g].y + c[g].z + c[g].w;
+    }
+    uint32_t run = block_exclusive_scan<BLOCK>(sum, warp_tot, nullptr);
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+        const uint4 o = make_uint4(run, run + c[g].x, run + c[g].x + c[g].y, run + c[g].x + c[g].y + c[g].z);
+        run = o.w + c[g].w;
+        reinterpret_cast<uint4*>(s.cnt)[t * G + g] = o;
+    }
+    if (t == 0) s.cnt[NB] = (uint32_t)n;
+    __syncthreads();
+#pragma unroll
+    for (int g = 0; g < G; ++g)
+#pragma unroll
+        for (int l = 0; l < 4; ++l) {
+            const int i = 4 * (t + g * BLOCK) + l;
+            if (i < n)
+                s.sc[s.cnt[bs[g][l] >> 16] + (bs[g][l] & 0xFFFFu)] =
+                    ((unsigned long long)okey(v[g][l]) << 32) | (uint32_t)i;
+        }
+    __syncthreads();
+#pragma unroll
+    for (int g = 0; g < G; ++g)
+#pragma unroll
+        for (int l = 0; l < 4; ++l) {
+            const int i = 4 * (t + g * BLOCK) + l;
+            if (i < n) {
+                const uint32_t b = bs[g][l] >> 16, b0 = s.cnt[b], b1 = s.cnt[b + 1];
+                const unsigned long long me = ((unsigned long long)okey(v[g][l]) << 32) | (uint32_t)i;
+                uint32_t r = b0;
+                for (uint32_t q = b0; q < b1; ++q) r += (s.sc[q] < me) ? 1u : 0u;
+                s.perm[r] = i;
+            }
+        }
+    __syncthreads();
+}
+
+// routes and objectives of the sorted customers perm[j] + 1.  Lanes fetch 32 positions' legs
+// (from the previous customer, and to the depot) and demands; every lane then replays them in
+// order, so all lanes hold the same state.  d(a, b) = d(b, a) bit for bit (dx and -dx have
+// the same square), so the depot leg into a route's first customer is its leg to the depot.
+__device__ void movrp_objectives(const int32_t* perm, int n, const float* __restrict__ xy,
+                                 const int32_t* __restrict__ dem, int cap, int vehicles, float* red, float* out) {
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+        float dist = 0.0f, total = 0.0f, longest = 0.0f, pen = 0.0f, lastdep = 0.0f;
+        int load = 0, size = 0, routes = 0;
+        for (int c0 = 0; c0 < n; c0 += 32) {
+            const int j = c0 + lane;
+            float e = 0.0f, dep = 0.0f;
+            int dm = 0;
+            if (j < n) {
+                const int cust = perm[j] + 1;
+                e = edge_xy(xy, (j == 0) ? 0 : perm[j - 1] + 1, cust);
+                dep = edge_xy(xy, cust, 0);
+                dm = __ldg(dem + cust);
+            }
+            const int cnt = min(32, n - c0);
+            for (int q = 0; q < cnt; ++q) {
+                const float eq = __shfl_sync(0xffffffffu, e, q);
+                const float dq = __shfl_sync(0xffffffffu, dep, q);
+                const int mq = __shfl_sync(0xffffffffu, dm, q);
+                if (load + mq > cap && size > 0) {  // close the route: back to the depot
+                    dist = __fadd_rn(dist, lastdep);
+                    total = __fadd_rn(total, dist);
+                    longest = (dist > longest) ? dist : longest;
+                    if (load > cap) pen = __fadd_rn(pen, __fmul_rn((float)(load - cap), 100.0f));
+                    ++routes;
+                    dist = 0.0f;
+                    load = 0;
+                    size = 0;
+                }
+                dist = __fadd_rn(dist, (size == 0) ? dq : eq);
+                load += mq;
+                ++size;
+                lastdep = dq;
+            }
+        }
+        if (size > 0) {
+            dist = __fadd_rn(dist, lastdep);
+            total = __fadd_rn(total, dist);
+            longest = (dist > longest) ? dist : longest;
+            if (load > cap) pen = __fadd_rn(pen, __fmul_rn((float)(load - cap), 100.0f));
+            ++routes;
+        }
+        float o0 = __fadd_rn(total, pen), o1 = longest;
+        if (routes > vehicles) {
+            const float vp = __fmul_rn((float)(routes - vehicles), 500.0f);
+            o0 = __fadd_rn(o0, vp);
+            o1 = __fadd_rn(o1, vp);
+        }
+        if (lane == 0) {
+            red[0] = o0;
+            red[1] = o1;
+        }
+    }
+    __syncthreads();
+    out[0] = red[0];
+    out[1] = red[1];
+    __syncthreads();
+}
+
+template <int BLOCK, int G>
+__global__ void __launch_bounds__(BLOCK, RowResidency<BLOCK, G>::value) movrp_row_kernel(RowLaunch L) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ PopDesc sd;
+    __shared__ uint32_t warp_tot[32];
+    __shared__ float red_f[32];
+    const int t = threadIdx.x;
+    const RowSmem s = carve(smem_raw, BLOCK, G, L.max_n, L.max_points);
+    int cur_pid = -1;
+    zero_counters<BLOCK, G>(s);
+
+    for (int task = blockIdx.x; task < L.ntasks; task += gridDim.x) {
+        int pid = 0, r = task;
+        if (L.tasks) {
+            const Task tk = L.tasks[task];
+            pid = tk.pid;
+            r = tk.row;
+        }
+        if (pid != cur_pid) {
+            __syncthreads();
+            if (t == 0) sd = L.descs ? L.descs[pid] : L.single;
+            __syncthreads();
+            cur_pid = pid;
+        }
+        const int n = sd.n, ld = sd.ld, P = sd.P, m = sd.m, cur = sd.cur;
+        if (L.mode == MODE_NSGA_OFF && at_limit(sd)) continue;
+        if (L.mode == MODE_NSGA_REFILL && (!sd.advanced || r < __ldg(sd.nu))) continue;
+        const float* src = sd.keys[cur];
+        float* dst = nullptr;
+        float* dfit = nullptr;
+        enum { LOAD, RANDOM, NSGA } build = RANDOM;
+        uint32_t gdraw = 0, tag = 0;
+        int pa = 0, pb = 0;
+        if (L.mode == MODE_INIT) {  // core/population.hpp:107-110
+            dst = sd.keys[cur];
+            dfit = sd.fit[cur];
+            tag = (sd.island << 8) | TAG_INIT;
+        } else if (L.mode == MODE_NSGA_OFF) {  // core/solver.hpp:1019-1091, pool rows [P, 2P)
+            dst = sd.keys[cur] + (size_t)P * ld;
+            dfit = sd.fit[cur] + (size_t)P * m;
+            gdraw = sd.gen + 1;
+            if (r >= P - sd.Mn) {
+                tag = TAG_MUTANT;
+            } else {
+                build = NSGA;
+                tag = TAG_NSGA_COIN;
+                const uint4 pk = draw4(sd.seed, 0u, (uint32_t)r, gdraw, TAG_NSGA_TOUR);
+                pa = tourn(pick(pk.x, P), pick(pk.y, P), sd.nrank, sd.ncd);
+                pb = tourn(pick(pk.z, P), pick(pk.w, P), sd.nrank, sd.ncd);
+            }
+        } else if (L.mode == MODE_NSGA_REFILL) {  // core/population.hpp:166-171
+            dst = sd.keys[cur];
+            dfit = sd.fit[cur];
+            gdraw = sd.gen;
+            tag = TAG_NSGA_REFILL;
+        } else if (L.mode == MODE_EVAL) {
+            dfit = sd.fit[cur];
+            build = LOAD;
+        } else {
+            continue;  // single-objective modes do not apply
+        }
+
+        float k[G][4];
+        const float* row = src + (size_t)r * ld;
+        const bool vec = ((ld & 3) == 0) && ((reinterpret_cast<uintptr_t>(src) & 15) == 0);
+#pragma unroll
+        for (int gg = 0; gg < G; ++gg) {
+            const int q = t + gg * BLOCK;
+#pragma unroll
+            for (int l = 0; l < 4; ++l) k[gg][l] = 0.0f;
+            if (build == LOAD) {
+                if (vec && 4 * q + 3 < ld) {
+                    const float4 a = __ldg(reinterpret_cast<const float4*>(row) + q);
+                    k[gg][0] = a.x, k[gg][1] = a.y, k[gg][2] = a.z, k[gg][3] = a.w;
+                } else {
+#pragma unroll
+                    for (int l = 0; l < 4; ++l) k[gg][l] = (4 * q + l < n) ? __ldg(row + 4 * q + l) : 0.0f;
+                }
+            } else if (4 * q < n) {
+                const uint4 x = draw4(sd.seed, (uint32_t)q, (uint32_t)r, gdraw, tag);
+                if (build == RANDOM) {
+                    k[gg][0] = u24(x.x), k[gg][1] = u24(x.y), k[gg][2] = u24(x.z), k[gg][3] = u24(x.w);
+                } else {
+                    const float4 a = __ldg(reinterpret_cast<const float4*>(src + (size_t)pa * ld) + q);
+                    const float4 b = __ldg(reinterpret_cast<const float4*>(src + (size_t)pb * ld) + q);
+                    const uint32_t T = sd.rhoT, MT = sd.mutT;
+                    k[gg][0] = ((x.x >> 8) < T) ? a.x : b.x;
+                    k[gg][1] = ((x.y >> 8) < T) ? a.y : b.y;
+                    k[gg][2] = ((x.z >> 8) < T) ? a.z : b.z;
+                    k[gg][3] = ((x.w >> 8) < T) ? a.w : b.w;
+                    const uint4 mp = draw4(sd.seed, (uint32_t)q, (uint32_t)r, gdraw, TAG_NSGA_MUTP);
+                    const uint4 mk = draw4(sd.seed, (uint32_t)q, (uint32_t)r, gdraw, TAG_NSGA_MUTK);
+                    if ((mp.x >> 8) < MT) k[gg][0] = u24(mk.x);
+                    if ((mp.y >> 8) < MT) k[gg][1] = u24(mk.y);
+                    if ((mp.z >> 8) < MT) k[gg][2] = u24(mk.z);
+                    if ((mp.w >> 8) < MT) k[gg][3] = u24(mk.w);
+                }
+            }
+            if (build != LOAD && 4 * q < ld) {
+                float4 o;
+                o.x = (4 * q + 0 < n) ? k[gg][0] : 0.0f;
+                o.y = (4 * q + 1 < n) ? k[gg][1] : 0.0f;
+                o.z = (4 * q + 2 < n) ? k[gg][2] : 0.0f;
+                o.w = (4 * q + 3 < n) ? k[gg][3] : 0.0f;
+                reinterpret_cast<float4*>(dst + (size_t)r * ld)[q] = o;
+            }
+        }
+
+        // 1. the row hash and the sort values
+        float* sk = reinterpret_cast<float*>(s.sc);
+#pragma unroll
+        for (int gg = 0; gg < G; ++gg)
+#pragma unroll
+            for (int l = 0; l < 4; ++l) {
+                const int i = 4 * (t + gg * BLOCK) + l;
+                if (i < n) sk[i] = k[gg][l];
+            }
+        __syncthreads();
+        if (t < 32) {
+            float h = 0.0f;
+            for (int c0 = 0; c0 < n; c0 += 32) {
+                const int i = c0 + t;
+                const float term = (i < n) ? __fmul_rn(sk[i], (float)(i + 1)) : 0.0f;
+                const int cnt = min(32, n - c0);
+                for (int q = 0; q < cnt; ++q) h = __fadd_rn(h, __shfl_sync(0xffffffffu, term, q));
+            }
+            if (t == 0) red_f[0] = h;
+        }
+        __syncthreads();
+        const float hb = __fmul_rn(red_f[0], 1.0e-5f);
+#pragma unroll
+        for (int gg = 0; gg < G; ++gg)
+#pragma unroll
+            for (int l = 0; l < 4; ++l) {
+                const int i = 4 * (t + gg * BLOCK) + l;
+                k[gg][l] = (i < n) ? __fadd_rn(k[gg][l], __fadd_rn(__fmul_rn((float)i, 1.0e-5f), hb)) : 0.0f;
+            }
+        __syncthreads();  // red_f[0] and the staged keys are read
+        // 2. the visiting order
+        movrp_argsort<BLOCK, G>(k, n, hb, __frcp_rn(__fadd_rn(1.0f, __fmul_rn((float)n, 1.0e-5f))), s, warp_tot);
+        zero_counters<BLOCK, G>(s);  // ready for the next row (separated by the row-end barrier)
+        // 3. routes and objectives
+        float res[2];
+        movrp_objectives(s.perm, n, sd.xy, sd.w, (int)sd.capi, sd.machines, red_f, res);
+        if (L.perm_out) {
+            int32_t* po = L.perm_out + (size_t)r * n;
+            for (int i = t; i < n; i += BLOCK) po[i] = s.perm[i];
+        }
+        if (t < 2) dfit[(size_t)r * m + t] = res[t];
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------------------
 int device_sm_count() {
@@ -1279,6 +1573,29 @@ static RowFn row_fn(const RowTile& t) {
     return nullptr;
 }
 
+static RowFn movrp_fn(const RowTile& t) {
+#define BK_TILE(B, G) \
+    if (t.block == B && t.groups == G) return movrp_row_kernel<B, G>;
+    BK_TILE(32, 1)
+    BK_TILE(64, 1)
+    BK_TILE(64, 2)
+    BK_TILE(128, 1)
+    BK_TILE(128, 2)
+    BK_TILE(128, 4)
+    BK_TILE(256, 1)
+    BK_TILE(256, 2)
+    BK_TILE(256, 4)
+    BK_TILE(512, 1)
+    BK_TILE(512, 2)
+    BK_TILE(512, 4)
+    BK_TILE(1024, 1)
+    BK_TILE(1024, 2)
+    BK_TILE(1024, 3)
+    BK_TILE(1024, 4)
+#undef BK_TILE
+    return nullptr;
+}
+
 // the dynamic shared-memory limit of a kernel is only ever raised, so a later launch
 // that needs less never takes it away from a live engine that needs more
 static std::mutex g_attr_mu;
@@ -1299,6 +1616,8 @@ cudaError_t prepare_rows(const RowTile& tile, size_t smem, int* per_sm) {
     RowFn fn = row_fn(tile);
     if (!fn) return cudaErrorInvalidValue;
     cudaError_t e = raise_smem_limit(reinterpret_cast<const void*>(fn), smem);
+    // the MO-VRP kernel has the same launch bounds and shared memory
+    if (e == cudaSuccess) e = raise_smem_limit(reinterpret_cast<const void*>(movrp_fn(tile)), smem);
     if (e != cudaSuccess) return e;
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, fn, tile.block, smem);
 }
@@ -1306,12 +1625,13 @@ cudaError_t prepare_rows(const RowTile& tile, size_t smem, int* per_sm) {
 cudaError_t launch_rows(const RowLaunch& L, int kind, const RowTile& tile, int grid, cudaStream_t s) {
     if (tile.block == 0) {  // rows beyond shared memory: global-scratch kernel
         if (!L.gscratch || L.gstride < row_global_stride(L.max_n)) return cudaErrorInvalidValue;
+        if (kind == MOVRP) return cudaErrorInvalidValue;  // MO-VRP rows fit in shared memory only
         if (L.ntasks <= 0 || grid <= 0) return cudaSuccess;
         if (grid > L.ntasks) grid = L.ntasks;
         row_kernel_big<<<grid, kBigBlock, 0, s>>>(L);
         return cudaGetLastError();
     }
-    RowFn fn = row_fn(tile);
+    RowFn fn = (kind == MOVRP) ? movrp_fn(tile) : row_fn(tile);
     if (!fn) return cudaErrorInvalidValue;
     if (L.ntasks <= 0 || grid <= 0) return cudaSuccess;
     if (grid > L.ntasks) grid = L.ntasks;

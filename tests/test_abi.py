@@ -62,3 +62,36 @@ def test_product_does_not_reference_the_oracle():
             if f.endswith((".py", ".cu", ".h", ".cuh", ".hpp", ".cpp")):
                 txt = open(os.path.join(root, f)).read()
                 assert "liboracle" not in txt and "orc_" not in txt and "libref" not in txt, f
+
+
+def test_problem_desc_layout_matches_header():
+    """the ctypes mirror of brkga_problem_desc has the C struct's size and field offsets"""
+    hdr = os.path.dirname(B.HEADER_PATH)
+    fields = [f[0] for f in B.ProblemDesc._fields_]
+    src = ('#include <stdio.h>\n#include <stddef.h>\n#include "brkga_b200.h"\nint main(void){ printf("%zu", '
+           'sizeof(brkga_problem_desc));' + "".join(
+               f' printf(" %zu", offsetof(brkga_problem_desc, {f}));' for f in fields) + " return 0; }\n")
+    exe = os.path.join(os.environ.get("TMPDIR", "/tmp"), f"desc_layout_{os.getpid()}")
+    r = subprocess.run(["gcc", "-std=c99", "-I", hdr, "-x", "c", "-", "-o", exe], input=src, capture_output=True,
+                       text=True)
+    assert r.returncode == 0, r.stderr
+    out = [int(x) for x in subprocess.run([exe], capture_output=True, text=True).stdout.split()]
+    os.remove(exe)
+    assert out[0] == C.sizeof(B.ProblemDesc)
+    assert out[1:] == [getattr(B.ProblemDesc, f).offset for f in fields]
+
+
+def test_movrp_route_listing():
+    """movrp_routes (report formatting of a device-decoded order) splits routes where the
+    reference's decode_routes does"""
+    import instances as I
+    import oracle as O
+    for n, V, ov in ((1, None, False), (31, 5, False), (60, 2, True)):
+        xy, dem, cap, Vv = I.movrp_instance(n, n, V, ov)
+        po = O.OracleProblem(O.MOVRP, n, xy=xy, w=dem, machines=Vv, vcap=cap)
+        for perm in O.decode_problem(po, I.keys(4, n, n + 1)):
+            routes = B.movrp_routes(perm, dem, cap)
+            route_of, count = O.movrp_routes(po, perm)
+            assert len(routes) == count
+            assert [r for r, rt in enumerate(routes) for _ in rt] == route_of.tolist()
+            assert [c for rt in routes for c in rt] == (perm + 1).tolist()
