@@ -664,13 +664,14 @@ __global__ void __cluster_dims__(kPeelCluster, 1, 1) __launch_bounds__(kPeelThre
         __syncthreads();
         if (nf == 0) break;  // every CTA sees the same front
         // column sums over the front's rows: thread (word t % 16, slice t / 16); the member
-        // rows' words are loaded eight at a time into 4-plane counters
+        // rows' words are loaded sixteen at a time (one L2 round trip for fronts of up to
+        // 256 members) into 5-plane counters
         const int wl = t % kPeelWords, sl = t / kPeelWords, w = w0 + wl;
         uint32_t acc[kDB];
 #pragma unroll
         for (int b = 0; b < kDB; ++b) acc[b] = 0u;
         if (w < W) {
-            constexpr int kBatch = 8;
+            constexpr int kBatch = 16, kSP = 5;  // a batch counts up to 16: 5 planes
             for (int j0 = sl; j0 < (int)nf; j0 += kBatch * kPeelSlices) {
                 uint32_t xs[kBatch];
 #pragma unroll
@@ -678,27 +679,28 @@ __global__ void __cluster_dims__(kPeelCluster, 1, 1) __launch_bounds__(kPeelThre
                     const int j = j0 + u * kPeelSlices;
                     xs[u] = (j < (int)nf) ? __ldg(S + (size_t)list[j] * Wmax + w) : 0u;
                 }
-                uint32_t s0 = 0u, s1 = 0u, s2 = 0u, s3 = 0u;
+                uint32_t sv[kSP];
+#pragma unroll
+                for (int b = 0; b < kSP; ++b) sv[b] = 0u;
 #pragma unroll
                 for (int u = 0; u < kBatch; ++u) {
-                    const uint32_t c0 = s0 & xs[u];
-                    s0 ^= xs[u];
-                    const uint32_t c1 = s1 & c0;
-                    s1 ^= c0;
-                    const uint32_t c2 = s2 & c1;
-                    s2 ^= c1;
-                    s3 ^= c2;
+                    uint32_t c = xs[u];
+#pragma unroll
+                    for (int b = 0; b < kSP; ++b) {
+                        const uint32_t nc = sv[b] & c;
+                        sv[b] ^= c;
+                        c = nc;
+                    }
                 }
                 uint32_t cy = 0u;
-                const uint32_t sv[4] = {s0, s1, s2, s3};
 #pragma unroll
-                for (int b = 0; b < 4; ++b) {
+                for (int b = 0; b < kSP; ++b) {
                     const uint32_t x = acc[b], y = sv[b];
                     acc[b] = x ^ y ^ cy;
                     cy = (x & y) | (cy & (x ^ y));
                 }
 #pragma unroll
-                for (int b = 4; b < kDB; ++b) {
+                for (int b = kSP; b < kDB; ++b) {
                     const uint32_t x = acc[b];
                     acc[b] = x ^ cy;
                     cy = x & cy;
