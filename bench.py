@@ -546,6 +546,121 @@ def workload_serve(args):
             "generations": gens, "max_active": args.max_active, "tick": args.tick}
 
 
+def workload_operators(args):
+    """Each hot-path operator alone on the headline sizes (TSP n=1000, P=2048; Pareto ranks on
+    a 2P = 4096 pool), device-resident buffers, CUDA events with L2 flushed before every
+    launch; beside it the reference's own CPU code for the same operator (oracle/_ref, CUDA
+    hidden, one thread)"""
+    import torch
+    import brkga_b200 as B
+    dev = torch.device("cuda:0")
+    xy = instance()
+    pb = B.tsp(xy)
+    n, P = N_CITIES, POP
+    rng = np.random.default_rng(7)
+    keys = (rng.integers(0, 1 << 24, (P, n)) / float(1 << 24)).astype(np.float32)
+    d_pop = torch.from_numpy(keys).to(dev)
+    d_fit = torch.zeros(P, dtype=torch.float32, device=dev)
+    d_srt = torch.zeros(P, dtype=torch.int32, device=dev)
+    d_next = torch.zeros_like(d_pop)
+    d_nfit = torch.zeros_like(d_fit)
+    N2 = 2 * P
+    obj = rng.random((N2, 2), dtype=np.float32)
+    d_obj = torch.from_numpy(obj).to(dev)
+    d_rank = torch.zeros(N2, dtype=torch.int32, device=dev)
+    d_cd = torch.zeros(N2, dtype=torch.float32, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    cur = torch.cuda.current_stream()
+    pb.evaluate_population(d_pop, d_fit, P, n, stream=cur)
+    B.sort_fitness(d_fit, P, 1, False, d_srt, stream=cur)
+
+    def timed(fn, reps=30):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        tot = 0.0
+        for i in range(reps):
+            flush.fill_(float(i))
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(cur)
+            fn()
+            b.record(cur)
+            b.synchronize()
+            tot += a.elapsed_time(b)
+        return 1e3 * tot / reps  # us
+
+    gen = [0]
+
+    def generation():
+        gen[0] += 1
+        B.generation_step(pb, d_pop, d_fit, d_srt, d_next, d_nfit, P, ELITE, MUTANTS, RHO, n, SEED_GA, gen[0],
+                          stream=cur)
+        B.sort_fitness(d_nfit, P, 1, False, d_srt, stream=cur)
+
+    gpu = {
+        "decode + tour length": timed(lambda: pb.evaluate_population(d_pop, d_fit, P, n, stream=cur)),
+        "elite partition": timed(lambda: B.sort_fitness(d_fit, P, 1, False, d_srt, stream=cur)),
+        "generation (crossover, mutants, decode, tour length, partition)": timed(generation),
+        "Pareto ranks + crowding (4096 points)": timed(lambda: (B.pareto_rank(d_obj, N2, 2, d_rank, stream=cur),
+                                                               B.crowding(d_obj, d_rank, N2, 2, d_cd, stream=cur))),
+    }
+    fit_sorted = np.sort(O_free_fitness(d_fit))
+    cpu = _cpu_operators(xy, keys, fit_sorted, obj)
+    rows = []
+    for k, g_us in gpu.items():
+        c = cpu.get(k) if cpu else None
+        rows.append({"operator": k, "gpu_us": round(g_us, 2), "reference_cpu_us": None if c is None else round(c, 1),
+                     "ratio": None if c is None else round(c / g_us, 1)})
+    return {"metric": "hot-path operators, device time vs the reference's CPU code", "unit": "us per call",
+            "sizes": f"TSP n={n} P={P}; Pareto pool {N2} x 2 objectives", "operators": rows,
+            "reference_cores": 1, "l2": "flushed before every timed launch"}
+
+
+def O_free_fitness(d_fit):
+    return d_fit.cpu().numpy().astype(np.float32)
+
+
+def _cpu_operators(xy, keys, fit_sorted, obj):
+    """the reference's CPU operators in a child process with CUDA hidden (its CPU path)"""
+    import tempfile
+    with tempfile.TemporaryDirectory() as td:
+        np.save(os.path.join(td, "xy.npy"), xy)
+        np.save(os.path.join(td, "keys.npy"), keys)
+        np.save(os.path.join(td, "fit.npy"), fit_sorted)
+        np.save(os.path.join(td, "obj.npy"), obj)
+        code = f"""
+import json, sys, time
+sys.path[:0] = [{os.path.join(ROOT, 'oracle')!r}]
+import numpy as np
+import oracle as O
+if not O.ref_available():
+    print(json.dumps(None)); sys.exit(0)
+R = O.ref()
+td = {td!r}
+xy = np.load(td + '/xy.npy'); keys = np.load(td + '/keys.npy'); fit = np.load(td + '/fit.npy'); obj = np.load(td + '/obj.npy')
+P, n = keys.shape
+def ev(rows):  # the call also builds the config's distance matrix: timed apart by difference
+    f = np.zeros(rows, np.float32)
+    k = np.ascontiguousarray(keys[:rows])
+    t0 = time.perf_counter(); R.ref_tsp_eval(xy.ctypes.data, None, n, k, rows, f, None)
+    return time.perf_counter() - t0
+out = {{}}
+out['decode + tour length'] = 1e6 * (min(ev(160) for _ in range(2)) - min(ev(32) for _ in range(2))) / 128 * P
+out['elite partition'] = 1e6 * R.ref_population_sort_seconds(fit, P, n, 5)
+g = [R.ref_generation_seconds(xy, n, P, {ELITE}, {MUTANTS}, {RHO}, 1 + i, np.ascontiguousarray(keys), fit) for i in range(2)]
+out['generation (crossover, mutants, decode, tour length, partition)'] = 1e6 * min(g)
+N = obj.shape[0]; rank = np.zeros(N, np.int32); cd = np.zeros(N, np.float32)
+t0 = time.perf_counter(); R.ref_pareto(np.ascontiguousarray(obj), N, rank, cd); t1 = time.perf_counter()
+out['Pareto ranks + crowding (4096 points)'] = 1e6 * (t1 - t0)
+print(json.dumps(out))
+"""
+        env = dict(os.environ, CUDA_VISIBLE_DEVICES="")
+        r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=900)
+    if r.returncode != 0:
+        return None
+    return json.loads(r.stdout.strip().splitlines()[-1])
+
+
 def reference_quality(xy, runs, gens, P=256, E=51, M=25):
     """best tour length of `runs` runs of the reference's own Solver on its CPU path
     (oracle/_ref, CUDA hidden); the reference seeds each run from the clock"""
@@ -699,6 +814,8 @@ def run_workload(args):
                               dict(population_size=1500, elite_size=300, mutant_size=0, elite_prob=0.10,
                                    max_generations=100000, seed=12), args.generations, "movrp",
                               dict(seed=12, movrp=True, n=100, P=1500, cap=cap, V=V))
+    elif w == "operators":
+        out = workload_operators(args)
     elif w == "batch":
         out = workload_batch(args)
     elif w == "serve":
@@ -744,7 +861,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--profile-op", action="store_true", help="operator kernels only (profiler captures)")
     ap.add_argument("--workload", default="tsp1000",
-                    choices=["tsp1000", "tsp52", "nsga", "tspj", "movrp", "batch", "serve", "quality"])
+                    choices=["tsp1000", "tsp52", "nsga", "tspj", "movrp", "operators", "batch", "serve", "quality"])
     ap.add_argument("--generations", type=int, default=500)
     ap.add_argument("--instances", type=int, default=256)
     ap.add_argument("--rate", type=float, default=200.0)

@@ -330,6 +330,11 @@ def ref():
                                            _f32p, _f32p, _f32p, _f32p, _i32p, _i32p, _u8p, _f32p]
         R.ref_nsga2_offspring.argtypes = [_f32p, _f32p, C.c_int, C.c_int, C.c_double, C.c_uint32, _f32p, _i32p,
                                           _f32p, _f32p, _i32p, _u8p, _u8p, _f32p]
+        R.ref_generation_seconds.restype = C.c_double
+        R.ref_generation_seconds.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_uint32,
+                                             _f32p, _f32p]
+        R.ref_population_sort_seconds.restype = C.c_double
+        R.ref_population_sort_seconds.argtypes = [_f32p, C.c_int, C.c_int, C.c_int]
         R.ref_solver_create.restype = C.c_void_p
         R.ref_solver_create_movrp.restype = C.c_void_p
         R.ref_solver_create_movrp.argtypes = [_f32p, _i32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double]

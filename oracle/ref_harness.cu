@@ -290,6 +290,34 @@ int ref_pareto(const float* obj, int N, int32_t* rank, float* cd) {
     }
 }
 
+// Population::sort (core/population.hpp:660-676), the reference's elite partition, on P
+// single-objective individuals of n keys with the given fitness values: mean seconds of one
+// sort over `reps` sorts of the same unsorted population
+double ref_population_sort_seconds(const float* fit, int P, int n, int reps) {
+    try {
+        std::vector<float> xy(2 * (size_t)n, 0.0f);
+        auto cfg = std::make_unique<TSPConfig<float>>(coords_to_matrix(xy.data(), n), "ref");
+        cfg->population_size = P;
+        Population<float> pop(cfg.get());
+        std::vector<Individual<float>> base(P, Individual<float>(n));
+        for (int i = 0; i < P; i++) {
+            base[i].fitness = fit[i];
+            base[i].evaluated = true;
+        }
+        auto& inds = pop.get_individuals();
+        double total = 0.0;
+        for (int r = 0; r < reps; r++) {
+            inds = base;
+            const auto t0 = std::chrono::steady_clock::now();
+            pop.sort();
+            total += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        }
+        return total / (reps > 0 ? reps : 1);
+    } catch (...) {
+        return -1.0;
+    }
+}
+
 // select_next_generation_nsga2 (core/population.hpp:491-517): pool indices of survivors
 int ref_nsga2_select(const float* obj, int N, int P, int32_t* sel) {
     try {
@@ -361,6 +389,34 @@ int ref_brkga_generation(const float* xy, int n, int P, int E, int M, double rho
         return 0;
     } catch (...) {
         return -1;
+    }
+}
+
+// seconds of one Solver::evolve_generation on the CPU path (core/solver.hpp:213-273: the
+// non-elites' evaluation, sort, crossover and mutants) from a population in sorted order
+double ref_generation_seconds(const float* xy, int n, int P, int E, int M, double rho, uint32_t seed,
+                              const float* keys_sorted, const float* fit_sorted) {
+    try {
+        auto cfg = std::make_unique<TSPConfig<float>>(coords_to_matrix(xy, n), "ref");
+        cfg->population_size = P;
+        cfg->elite_size = E;
+        cfg->mutant_size = M;
+        cfg->elite_prob = rho;
+        cfg->max_generations = 1;
+        Solver<float> solver(std::move(cfg), false, 1000000);
+        if (solver.execution_mode != "cpu") return -2.0;
+        auto& inds = solver.population->get_individuals();
+        for (int r = 0; r < P; r++) {
+            set_keys(inds[r], keys_sorted + (size_t)r * n, n);
+            inds[r].fitness = fit_sorted[r];
+            inds[r].evaluated = true;
+        }
+        solver.rng.seed(seed);
+        const auto t0 = std::chrono::steady_clock::now();
+        solver.evolve_generation();
+        return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    } catch (...) {
+        return -1.0;
     }
 }
 
