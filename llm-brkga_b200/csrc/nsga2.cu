@@ -1373,9 +1373,10 @@ int32_t brkga_pareto_rank_bitmatrix(const float* d_obj, int32_t N, int32_t m, in
     cudaStream_t st = (cudaStream_t)stream;
     const int W = (N + 31) / 32;
     const size_t sbytes = (size_t)N * W * 4, cbytes = (size_t)N * 4;
+    const size_t doff = ((sbytes + cbytes + 255) / 256) * 256;  // a descriptor for the cluster peel
     std::lock_guard<std::mutex> lk(g_op_mu);
     void* buf = nullptr;
-    int32_t rc = op_scratch(sbytes + cbytes, &buf);
+    int32_t rc = op_scratch(doff + sizeof(PopDesc), &buf);
     if (rc != BRKGA_OK) return rc;
     DomArgs a;
     std::memset(&a, 0, sizeof(a));
@@ -1393,11 +1394,30 @@ int32_t brkga_pareto_rank_bitmatrix(const float* d_obj, int32_t N, int32_t m, in
         e = cudaGetLastError();
     }
     if (e != cudaSuccess) return cuda_fail(e, "dominance launch");
-    const size_t smem = (((size_t)N * 2 + 15) / 16) * 16 + peel_smem_bytes(N);
-    if ((e = raise_smem_limit(reinterpret_cast<const void*>(peel_op_kernel), smem)) != cudaSuccess)
-        return cuda_fail(e, "peel set-up");
-    peel_op_kernel<<<1, kNsgaBlock, smem, st>>>(N, a.S, a.cnt, W, d_rank);
-    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "peel launch");
+    if (N <= kMaxPool) {
+        // the engine's peel on a cluster of CTAs (ranks left in the counts), as for a
+        // population of N rows in mode 1
+        PopDesc hd;
+        std::memset(&hd, 0, sizeof(hd));
+        hd.P = N;
+        hd.m = m;
+        hd.domS = a.S;
+        hd.domW = W;
+        hd.domcnt = a.cnt;
+        PopDesc* dd = reinterpret_cast<PopDesc*>((char*)buf + doff);
+        if ((e = cudaMemcpyAsync(dd, &hd, sizeof(hd), cudaMemcpyHostToDevice, st)) != cudaSuccess)
+            return cuda_fail(e, "peel descriptor");
+        nsga_peel_cluster_kernel<<<kPeelCluster, kPeelThreads, 0, st>>>(dd, 1);
+        if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "peel launch");
+        if ((e = cudaMemcpyAsync(d_rank, a.cnt, cbytes, cudaMemcpyDeviceToDevice, st)) != cudaSuccess)
+            return cuda_fail(e, "rank copy");
+    } else {
+        const size_t smem = (((size_t)N * 2 + 15) / 16) * 16 + peel_smem_bytes(N);
+        if ((e = raise_smem_limit(reinterpret_cast<const void*>(peel_op_kernel), smem)) != cudaSuccess)
+            return cuda_fail(e, "peel set-up");
+        peel_op_kernel<<<1, kNsgaBlock, smem, st>>>(N, a.S, a.cnt, W, d_rank);
+        if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "peel launch");
+    }
     // the scratch is shared by later calls: finish before returning
     if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(e, "peel");
     return BRKGA_OK;
