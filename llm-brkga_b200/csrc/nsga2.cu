@@ -465,24 +465,6 @@ __device__ __forceinline__ unsigned long long order_key(int rank, float v, int i
     return ((unsigned long long)rank << 48) | ((unsigned long long)okey(v) << 16) | (unsigned long long)i;
 }
 
-// crowding with an in-CTA bitonic sort per objective (operator entry point)
-template <int T>
-__device__ void crowding_ref(int N, const SelSmem& s) {
-    const int t = threadIdx.x;
-    const int N2 = npow2(N);
-    for (int i = t; i < N; i += T) s.cd[i] = 0.0f;
-    for (int o = 0; o < 2; ++o) {
-        __syncthreads();
-        for (int i = t; i < N2; i += T) s.key[i] = (i < N) ? order_key(s.rank[i], s.obj[2 * i + o], i) : ~0ull;
-        __syncthreads();
-        bitonic_u64<T>(s.key, N2);
-        front_bounds<T>(N, s);
-        __syncthreads();
-        crowding_pass<T>(N, o, s);
-    }
-    __syncthreads();
-}
-
 // crowding from the orders nsga_order_kernel computed (ord[o * ostride + position]); leaves
 // s.key holding the objective-1 order and s.fs / s.fe its front bounds
 template <int T>
@@ -840,17 +822,6 @@ __global__ void __launch_bounds__(kNsgaBlock) peel_op_kernel(int N, const uint32
     peel_ranks<kNsgaBlock>(N, S, Wmax, cnt, r16, ps, wt32);
     __syncthreads();
     for (int i = threadIdx.x; i < N; i += kNsgaBlock) rank[i] = r16[i];
-}
-
-// crowding from given ranks (op API, two objectives): one CTA
-__global__ void __launch_bounds__(kNsgaBlock) crowd_op_kernel(const float* obj, const int32_t* rank, int N, float* cd) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    const SelSmem s = sel_carve(smem, N);
-    for (int i = threadIdx.x; i < 2 * N; i += kNsgaBlock) s.obj[i] = obj[i];
-    for (int i = threadIdx.x; i < N; i += kNsgaBlock) s.rank[i] = (uint16_t)rank[i];
-    __syncthreads();
-    crowding_ref<kNsgaBlock>(N, s);
-    for (int i = threadIdx.x; i < N; i += kNsgaBlock) cd[i] = s.cd[i];
 }
 
 // survivors -> the other pool buffer, rows [0, P); population blockIdx.y
@@ -1461,11 +1432,33 @@ int32_t brkga_crowding(const float* d_obj, const int32_t* d_rank, int32_t N, int
     if (m != 2) return fail(BRKGA_ERR_UNSUPPORTED, "crowding kernel handles two objectives");
     if (N < 0 || N > kMaxPool) return fail(BRKGA_ERR_UNSUPPORTED, "N outside [0, 4096]");
     if (N == 0) return BRKGA_OK;
-    cudaError_t e;
-    if ((e = raise_smem_limit(reinterpret_cast<const void*>(crowd_op_kernel), sel_smem_bytes(N))) != cudaSuccess)
-        return cuda_fail(e, "crowding set-up");
-    crowd_op_kernel<<<1, kNsgaBlock, sel_smem_bytes(N), (cudaStream_t)stream>>>(d_obj, d_rank, N, d_cd);
-    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "crowding launch");
+    cudaStream_t st = (cudaStream_t)stream;
+    // the engine's crowding: orders by (rank, objective, index) on the grid, then the crowding
+    // over them, as for a population of N points in mode 1; scratch from the stream-ordered
+    // pool (orders [2][2N], ranks [N], the descriptor), returned behind the launches
+    const size_t doff = (((size_t)5 * N * 4 + 255) / 256) * 256;
+    void* p = nullptr;
+    int32_t rc = dev_alloc(&p, doff + sizeof(PopDesc), st);
+    if (rc != BRKGA_OK) return rc;
+    PopDesc hd;
+    std::memset(&hd, 0, sizeof(hd));
+    hd.P = N;
+    hd.m = 2;
+    hd.fit[0] = const_cast<float*>(d_obj);
+    hd.domcnt = const_cast<int32_t*>(d_rank);
+    hd.nord = static_cast<int32_t*>(p);
+    hd.nrank = static_cast<int32_t*>(p) + 4 * (size_t)N;
+    hd.ncd = d_cd;
+    PopDesc* dd = reinterpret_cast<PopDesc*>(static_cast<char*>(p) + doff);
+    cudaError_t e = nsga_prepare((N + 1) / 2);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dd, &hd, sizeof(hd), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) {
+        nsga_order_kernel<<<dim3((N + kOrdPerCta - 1) / kOrdPerCta, 2, 1), kOrdThreads, (size_t)N * 8, st>>>(dd, 1);
+        nsga_select_kernel<<<1, kNsgaBlock, sel_smem_bytes(N), st>>>(dd, 1);
+        e = cudaGetLastError();
+    }
+    dev_free(p, st);
+    if (e != cudaSuccess) return cuda_fail(e, "crowding launch");
     return BRKGA_OK;
 }
 
