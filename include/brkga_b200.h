@@ -184,10 +184,11 @@ int32_t brkga_local_search(brkga_problem* pb, float* d_pop, float* d_fitness, in
 /* Pareto ranks of N points with m objectives (minimisation), d_obj [N][m].  Replaces
  * Population::fast_non_dominated_sort (core/population.hpp:409-440). */
 int32_t brkga_pareto_rank(const float* d_obj, int32_t N, int32_t m, int32_t* d_rank, void* stream);
-/* The same ranks through the bit-packed dominance matrix for any m: row i, bit j set when
- * point j dominates point i, built 32 columns per __ballot_sync; domination counts and
- * front peeling by __popc of row & front-mask words.  Uses an internal device scratch of
- * N*ceil(N/32)*4 bytes and returns after the ranks are written. */
+/* The same ranks through the bit-packed dominance matrix for any m: bit j of row i set when
+ * point i dominates point j, built 32 columns per __ballot_sync; fronts peeled by
+ * bit-sliced column sums of the front's rows (for N <= 4096 on a cluster of eight CTAs,
+ * the front exchanged through distributed shared memory).  Uses an internal device scratch
+ * of about N*ceil(N/32)*4 bytes and returns after the ranks are written. */
 int32_t brkga_pareto_rank_bitmatrix(const float* d_obj, int32_t N, int32_t m, int32_t* d_rank, void* stream);
 /* Pareto ranks exactly like brkga_pareto_rank, but the call allocates no device memory:
  * for callers that cannot call cudaMalloc -- code running under a framework whose
@@ -201,7 +202,9 @@ int32_t brkga_pareto_rank_bitmatrix(const float* d_obj, int32_t N, int32_t m, in
  * the same array: calls whose work overlaps on the GPU (different streams, or another
  * thread) race and must be ordered by the caller. */
 int32_t brkga_pareto_rank_noalloc(const float* d_obj, int32_t N, int32_t m, int32_t* d_rank, void* stream);
-/* Crowding distance per front (core/population.hpp:453-489), fronts from d_rank. */
+/* Crowding distance per front (core/population.hpp:453-489), fronts from d_rank; two
+ * objectives, N <= 4096.  Asynchronous on `stream`; its scratch comes from the library's
+ * stream-ordered pool. */
 int32_t brkga_crowding(const float* d_obj, const int32_t* d_rank, int32_t N, int32_t m, float* d_cd,
                        void* stream);
 
