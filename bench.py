@@ -604,7 +604,7 @@ def workload_operators(args):
         "Pareto ranks + crowding (4096 points)": timed(lambda: (B.pareto_rank(d_obj, N2, 2, d_rank, stream=cur),
                                                                B.crowding(d_obj, d_rank, N2, 2, d_cd, stream=cur))),
     }
-    fit_sorted = np.sort(O_free_fitness(d_fit))
+    fit_sorted = np.sort(d_fit.cpu().numpy().astype(np.float32))
     cpu = _cpu_operators(xy, keys, fit_sorted, obj)
     rows = []
     for k, g_us in gpu.items():
@@ -614,10 +614,6 @@ def workload_operators(args):
     return {"metric": "hot-path operators, device time vs the reference's CPU code", "unit": "us per call",
             "sizes": f"TSP n={n} P={P}; Pareto pool {N2} x 2 objectives", "operators": rows,
             "reference_cores": 1, "l2": "flushed before every timed launch"}
-
-
-def O_free_fitness(d_fit):
-    return d_fit.cpu().numpy().astype(np.float32)
 
 
 def _cpu_operators(xy, keys, fit_sorted, obj):
