@@ -225,3 +225,27 @@ def test_cpp_knapsack_files(cuda, tmp_path):
     best = s.get_best_individual()[2]
     assert np.float32(out["txt"]) == best and np.float32(out["csv"]) == best
     s.close()
+
+
+def test_engines_on_host_threads(cuda):
+    """solvers driven from several host threads at once (the reference's callers use
+    OpenMP / std::async) give the runs they give one at a time; one problem is shared"""
+    from concurrent.futures import ThreadPoolExecutor
+    xy = I.tsp_coords(80, seed=21)
+    pb = B().tsp(xy)
+
+    def run(seed):
+        s = B().Solver(pb, B().params(128, 20, 12, 0.7, 30, seed=seed))
+        s.run()
+        keys, fit = s.get_population()
+        hist = s.get_fitness_history()
+        s.close()
+        return keys, fit, hist
+
+    alone = [run(sd) for sd in range(6)]
+    with ThreadPoolExecutor(6) as ex:
+        together = list(ex.map(run, range(6)))
+    for a, b in zip(alone, together):
+        for x, y in zip(a, b):
+            np.testing.assert_array_equal(x, y)
+    pb.close()
