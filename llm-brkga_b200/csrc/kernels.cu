@@ -246,26 +246,34 @@ __device__ __forceinline__ long long block_excl_scan_ll(long long v, long long* 
 }
 
 // knapsack greedy in key order: prefix of the sorted items that fits, then a
-// first-fit scan of the rest by warp 0 (weights must be >= 0)
+// first-fit scan of the rest by warp 0 (weights must be >= 0).  The items' (weight, value)
+// pairs are first gathered in key order into wv ([n], free scratch after the argsort) by
+// the whole block, so the scans read on-chip data instead of one dependent round of loads
+// per 32 items.
 template <int BLOCK>
 __device__ float knap_greedy(const int32_t* perm, int n, const int32_t* __restrict__ w,
                              const int32_t* __restrict__ v, long long C, long long* red,
-                             long long* shared_misc) {
+                             long long* shared_misc, int2* wv) {
     const int t = threadIdx.x;
+    for (int p = t; p < n; p += BLOCK) {
+        const int it = perm[p];
+        wv[p] = make_int2(__ldg(w + it), __ldg(v + it));
+    }
+    __syncthreads();
     const int ch = (n + BLOCK - 1) / BLOCK;
     const int p0 = t * ch, p1 = min(n, p0 + ch);
     long long ws = 0;
-    for (int p = p0; p < p1; ++p) ws += __ldg(w + perm[p]);
+    for (int p = p0; p < p1; ++p) ws += wv[p].x;
     long long tot;
     const long long base = block_excl_scan_ll<BLOCK>(ws, red, &tot);
     // positions whose inclusive prefix weight stays <= C
     long long S = base, cnt = 0, val = 0, lastS = -1;
     for (int p = p0; p < p1; ++p) {
-        const int it = perm[p];
-        S += __ldg(w + it);
+        const int2 x = wv[p];
+        S += x.x;
         if (S <= C) {
             ++cnt;
-            val += __ldg(v + it);
+            val += x.y;
             lastS = S;
         }
     }
@@ -279,8 +287,9 @@ __device__ float knap_greedy(const int32_t* perm, int n, const int32_t* __restri
         long long r = C - shared_misc[0];
         for (int b = (int)f + 1; b < n; b += 32) {
             const int pos = b + t;
-            const long long wl = (pos < n) ? (long long)__ldg(w + perm[pos]) : LLONG_MAX;
-            const long long vl = (pos < n) ? (long long)__ldg(v + perm[pos]) : 0ll;
+            const int2 x = (pos < n) ? wv[pos] : make_int2(0, 0);
+            const long long wl = (pos < n) ? (long long)x.x : LLONG_MAX;
+            const long long vl = (long long)x.y;
             int cur = 0;
             for (;;) {
                 const unsigned mask = __ballot_sync(0xffffffffu, pos < n && t >= cur && wl <= r);
@@ -294,6 +303,15 @@ __device__ float knap_greedy(const int32_t* perm, int n, const int32_t* __restri
     }
     __syncthreads();
     return (float)(v0 + vt);
+}
+
+// the same, called rather than inlined: in the one-group row kernels (48 registers) an
+// inlined copy spills registers on every kind's path
+template <int BLOCK>
+__device__ __noinline__ float knap_greedy_call(const int32_t* perm, int n, const int32_t* __restrict__ w,
+                                               const int32_t* __restrict__ v, long long C, long long* red,
+                                               long long* shared_misc, int2* wv) {
+    return knap_greedy<BLOCK>(perm, n, w, v, C, red, shared_misc, wv);
 }
 
 // TSPJ makespan (configs/tspj_config.hpp:555-585): the city tour from the depot (node 0)
@@ -763,7 +781,12 @@ __global__ void __launch_bounds__(BLOCK, RowResidency<BLOCK, G>::value) row_kern
                         d[1] = __ldg(m1 + (size_t)a * np1 + b);
                     }, red_f, res);
                 } else if (kind == KNAP_GREEDY) {
-                    res[0] = knap_greedy<BLOCK>(s.perm, n, sd.w, sd.v, sd.capi, red_ll, misc);
+                    if constexpr (G == 1)
+                        res[0] = knap_greedy_call<BLOCK>(s.perm, n, sd.w, sd.v, sd.capi, red_ll, misc,
+                                                         reinterpret_cast<int2*>(s.sc));
+                    else
+                        res[0] = knap_greedy<BLOCK>(s.perm, n, sd.w, sd.v, sd.capi, red_ll, misc,
+                                                    reinterpret_cast<int2*>(s.sc));
                 } else if (kind == TSPJ) {
                     res[0] = tspj_makespan<BLOCK>(perm, n / 2, sd.mat, sd.mat2, red_f);
                 }
@@ -1064,7 +1087,7 @@ __global__ void __launch_bounds__(kBigBlock) row_kernel_big(RowLaunch L) {
                     d[1] = __ldg(m1 + (size_t)a * np1 + b);
                 }, red_f, res);
             } else if (kind == KNAP_GREEDY) {
-                res[0] = knap_greedy<BLOCK>(perm, n, sd.w, sd.v, sd.capi, red_ll, misc);
+                res[0] = knap_greedy<BLOCK>(perm, n, sd.w, sd.v, sd.capi, red_ll, misc, reinterpret_cast<int2*>(sc));
             } else if (kind == TSPJ) {
                 res[0] = tspj_makespan<BLOCK>(perm, n / 2, sd.mat, sd.mat2, red_f);
             }
