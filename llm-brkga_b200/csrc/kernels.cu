@@ -353,6 +353,50 @@ __device__ float tspj_makespan(const int32_t* perm, int nc, const float* __restr
     return v;
 }
 
+// The same for tours of up to 128 cities, called rather than inlined (one-group row
+// kernels): every lane issues the loads of all its positions before the first sequential
+// step, so the walk waits for one round of loads instead of one per 32 cities.
+template <int BLOCK>
+__device__ __noinline__ float tspj_makespan_call(const int32_t* perm, int nc, const float* __restrict__ travel,
+                                                 const float* __restrict__ jobs, float* red) {
+    constexpr int kChunks = 4;
+    if (nc > 32 * kChunks) return tspj_makespan<BLOCK>(perm, nc, travel, jobs, red);
+    const int lane = threadIdx.x & 31;
+    if (threadIdx.x < 32) {
+        const size_t D = (size_t)nc + 1;
+        float e[kChunks], jd[kChunks];
+#pragma unroll
+        for (int c = 0; c < kChunks; ++c) {
+            const int i = 32 * c + lane;
+            e[c] = 0.0f;
+            jd[c] = 0.0f;
+            if (i < nc) {
+                const int city = perm[i] + 1;
+                const int prev = (i == 0) ? 0 : perm[i - 1] + 1;
+                const int job = perm[nc + i] - nc + 1;
+                e[c] = __ldg(travel + (size_t)prev * D + city);
+                jd[c] = __ldg(jobs + (size_t)city * D + job);
+            }
+        }
+        float run = 0.0f, mjc = 0.0f;
+#pragma unroll
+        for (int c = 0; c < kChunks; ++c) {
+            const int cnt = min(32, nc - 32 * c);
+            for (int q = 0; q < cnt; ++q) {
+                run = __fadd_rn(run, __shfl_sync(0xffffffffu, e[c], q));
+                const float jc = __fadd_rn(run, __shfl_sync(0xffffffffu, jd[c], q));
+                mjc = (mjc < jc) ? jc : mjc;
+            }
+        }
+        const float tt = __fadd_rn(run, __ldg(travel + (size_t)(perm[nc - 1] + 1) * D));
+        if (lane == 0) red[0] = (tt < mjc) ? mjc : tt;
+    }
+    __syncthreads();
+    const float v = red[0];
+    __syncthreads();
+    return v;
+}
+
 // ContinuousOptGPUConfig (configs/continuous_opt_gpu_config.hpp:114-173): x = key * (upper -
 // lower) + lower; sphere sum x^2; Rastrigin 10 n + sum (x^2 - 10 cos(2 pi x)); Rosenbrock
 // sum 100 (x_{i+1} - x_i^2)^2 + (1 - x_i)^2.  keys in index order (shared or global memory).
@@ -788,7 +832,10 @@ __global__ void __launch_bounds__(BLOCK, RowResidency<BLOCK, G>::value) row_kern
                         res[0] = knap_greedy<BLOCK>(s.perm, n, sd.w, sd.v, sd.capi, red_ll, misc,
                                                     reinterpret_cast<int2*>(s.sc));
                 } else if (kind == TSPJ) {
-                    res[0] = tspj_makespan<BLOCK>(perm, n / 2, sd.mat, sd.mat2, red_f);
+                    if constexpr (G == 1)
+                        res[0] = tspj_makespan_call<BLOCK>(perm, n / 2, sd.mat, sd.mat2, red_f);
+                    else
+                        res[0] = tspj_makespan<BLOCK>(perm, n / 2, sd.mat, sd.mat2, red_f);
                 }
                 if (L.perm_out) {
                     int32_t* po = L.perm_out + (size_t)r * n;
@@ -1301,45 +1348,56 @@ __device__ void movrp_argsort(const float (&v)[G][4], int n, float lo, float inv
     __syncthreads();
 }
 
-// routes and objectives of the sorted customers perm[j] + 1.  Lanes fetch 32 positions' legs
-// (from the previous customer, and to the depot) and demands; every lane then replays them in
-// order, so all lanes hold the same state.  d(a, b) = d(b, a) bit for bit (dx and -dx have
-// the same square), so the depot leg into a route's first customer is its leg to the depot.
+// routes and objectives of the sorted customers perm[j] + 1.  Lanes fetch the legs (from the
+// previous customer, and to the depot) and demands of 128 positions at a time, loads first;
+// every lane then replays them in order, so all lanes hold the same state.  d(a, b) = d(b, a)
+// bit for bit (dx and -dx have the same square), so the depot leg into a route's first
+// customer is its leg to the depot.
 __device__ void movrp_objectives(const int32_t* perm, int n, const float* __restrict__ xy,
                                  const int32_t* __restrict__ dem, int cap, int vehicles, float* red, float* out) {
+    constexpr int kChunks = 4;
     if (threadIdx.x < 32) {
         const int lane = threadIdx.x;
         float dist = 0.0f, total = 0.0f, longest = 0.0f, pen = 0.0f, lastdep = 0.0f;
         int load = 0, size = 0, routes = 0;
-        for (int c0 = 0; c0 < n; c0 += 32) {
-            const int j = c0 + lane;
-            float e = 0.0f, dep = 0.0f;
-            int dm = 0;
-            if (j < n) {
-                const int cust = perm[j] + 1;
-                e = edge_xy(xy, (j == 0) ? 0 : perm[j - 1] + 1, cust);
-                dep = edge_xy(xy, cust, 0);
-                dm = __ldg(dem + cust);
-            }
-            const int cnt = min(32, n - c0);
-            for (int q = 0; q < cnt; ++q) {
-                const float eq = __shfl_sync(0xffffffffu, e, q);
-                const float dq = __shfl_sync(0xffffffffu, dep, q);
-                const int mq = __shfl_sync(0xffffffffu, dm, q);
-                if (load + mq > cap && size > 0) {  // close the route: back to the depot
-                    dist = __fadd_rn(dist, lastdep);
-                    total = __fadd_rn(total, dist);
-                    longest = (dist > longest) ? dist : longest;
-                    if (load > cap) pen = __fadd_rn(pen, __fmul_rn((float)(load - cap), 100.0f));
-                    ++routes;
-                    dist = 0.0f;
-                    load = 0;
-                    size = 0;
+        for (int g0 = 0; g0 < n; g0 += 32 * kChunks) {
+            float e[kChunks], dep[kChunks];
+            int dm[kChunks];
+#pragma unroll
+            for (int c = 0; c < kChunks; ++c) {
+                const int j = g0 + 32 * c + lane;
+                e[c] = 0.0f;
+                dep[c] = 0.0f;
+                dm[c] = 0;
+                if (j < n) {
+                    const int cust = perm[j] + 1;
+                    e[c] = edge_xy(xy, (j == 0) ? 0 : perm[j - 1] + 1, cust);
+                    dep[c] = edge_xy(xy, cust, 0);
+                    dm[c] = __ldg(dem + cust);
                 }
-                dist = __fadd_rn(dist, (size == 0) ? dq : eq);
-                load += mq;
-                ++size;
-                lastdep = dq;
+            }
+#pragma unroll
+            for (int c = 0; c < kChunks; ++c) {
+                const int cnt = min(32, n - (g0 + 32 * c));
+                for (int q = 0; q < cnt; ++q) {
+                    const float eq = __shfl_sync(0xffffffffu, e[c], q);
+                    const float dq = __shfl_sync(0xffffffffu, dep[c], q);
+                    const int mq = __shfl_sync(0xffffffffu, dm[c], q);
+                    if (load + mq > cap && size > 0) {  // close the route: back to the depot
+                        dist = __fadd_rn(dist, lastdep);
+                        total = __fadd_rn(total, dist);
+                        longest = (dist > longest) ? dist : longest;
+                        if (load > cap) pen = __fadd_rn(pen, __fmul_rn((float)(load - cap), 100.0f));
+                        ++routes;
+                        dist = 0.0f;
+                        load = 0;
+                        size = 0;
+                    }
+                    dist = __fadd_rn(dist, (size == 0) ? dq : eq);
+                    load += mq;
+                    ++size;
+                    lastdep = dq;
+                }
             }
         }
         if (size > 0) {
