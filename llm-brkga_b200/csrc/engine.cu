@@ -95,6 +95,9 @@ void Population::release(int device) {
 
 using namespace bk;
 
+// the longest captured run of plain generations is 2^kMaxRunLog
+constexpr int kMaxRunLog = 4;
+
 struct brkga_engine {
     std::mutex mu;
     int device = 0;
@@ -110,8 +113,10 @@ struct brkga_engine {
     bool stage = false;
     uint32_t gen = 0;
     bool initialized = false;
-    int chunk = 16;
-    cudaGraphExec_t gx_chunk = nullptr, gx_one = nullptr, gx_mig = nullptr;
+    // captured runs of 2^k plain generations (k <= kMaxRunLog), and one special generation
+    // (a migration for islands, the diversity pass for NSGA-II)
+    cudaGraphExec_t gx_run[kMaxRunLog + 1] = {};
+    cudaGraphExec_t gx_special = nullptr;
     int32_t* d_perm = nullptr;
     float* d_tmpfit = nullptr;
     NsgaState nsga;
@@ -134,9 +139,23 @@ static RowLaunch base_launch(brkga_engine* e, int mode) {
     return L;
 }
 
-static bool migration_due(const brkga_engine* e, uint32_t g) {
+// the next generation after the current one (counted from 1) that runs the special graph,
+// 0 when none does: islands migrate after generations g % interval == 0; NSGA-II runs its
+// diversity pass after generations (g - 1) % interval == 0.  Engines set no generation
+// limit, so the device's generation counter equals e->gen.
+static uint32_t next_special(const brkga_engine* e) {
+    const uint32_t g = e->gen;
+    if (e->pop.sh.mo) {
+        const int iv = e->nsga.div_interval;
+        if (iv <= 0) return 0;
+        return (g + (uint32_t)iv - 1u) / (uint32_t)iv * (uint32_t)iv + 1u;
+    }
     const auto& p = e->pop.prm;
-    return e->pop.sh.k > 1 && p.migration_interval > 0 && p.num_migrants > 0 && g % (uint32_t)p.migration_interval == 0;
+    if (e->pop.sh.k > 1 && p.migration_interval > 0 && p.num_migrants > 0) {
+        const uint32_t iv = (uint32_t)p.migration_interval;
+        return (g / iv + 1u) * iv;
+    }
+    return 0;
 }
 
 // one single-objective generation: fused rows + elite partition (+ migration, re-sort)
@@ -169,16 +188,16 @@ static cudaError_t enqueue_brkga_gen(brkga_engine* e, bool mig) {
     return err;
 }
 
-static cudaError_t enqueue_gen(brkga_engine* e, bool mig) {
-    if (e->pop.sh.mo) return nsga_enqueue_generation(e->nsga, e->stream);
-    return enqueue_brkga_gen(e, mig);
+static cudaError_t enqueue_gen(brkga_engine* e, bool special) {
+    if (e->pop.sh.mo) return nsga_enqueue_generation(e->nsga, e->stream, special);
+    return enqueue_brkga_gen(e, special);
 }
 
-static cudaError_t capture(brkga_engine* e, int gens, bool mig, cudaGraphExec_t* out) {
+static cudaError_t capture(brkga_engine* e, int gens, bool special, cudaGraphExec_t* out) {
     cudaGraph_t g = nullptr;
     cudaError_t err = cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal);
     if (err != cudaSuccess) return err;
-    for (int i = 0; i < gens && err == cudaSuccess; ++i) err = enqueue_gen(e, mig && i == gens - 1);
+    for (int i = 0; i < gens && err == cudaSuccess; ++i) err = enqueue_gen(e, special && i == gens - 1);
     cudaError_t end = cudaStreamEndCapture(e->stream, &g);
     if (err != cudaSuccess) {
         if (g) cudaGraphDestroy(g);
@@ -226,9 +245,9 @@ static int32_t grow_history(brkga_engine* e, int need) {
 static void destroy_engine(brkga_engine* e) {
     DeviceGuard g(e->device);
     if (e->stream) cudaStreamSynchronize(e->stream);
-    if (e->gx_chunk) cudaGraphExecDestroy(e->gx_chunk);
-    if (e->gx_one) cudaGraphExecDestroy(e->gx_one);
-    if (e->gx_mig) cudaGraphExecDestroy(e->gx_mig);
+    for (cudaGraphExec_t x : e->gx_run)
+        if (x) cudaGraphExecDestroy(x);
+    if (e->gx_special) cudaGraphExecDestroy(e->gx_special);
     nsga_release(e->nsga);
     e->pop.release(e->device);
     if (e->stream) cudaStreamDestroy(e->stream);
@@ -460,32 +479,23 @@ int32_t brkga_evolve(brkga_engine* e, int32_t generations) {
     cudaError_t err = cudaSuccess;
     int left = generations;
     while (left > 0 && err == cudaSuccess) {
-        // generations until (and excluding) the next migration generation
-        int plain = left;
-        if (e->pop.sh.k > 1 && e->pop.prm.migration_interval > 0 && e->pop.prm.num_migrants > 0) {
-            const uint32_t iv = (uint32_t)e->pop.prm.migration_interval;
-            const uint32_t next = (e->gen / iv + 1) * iv;
-            plain = std::min<int>(left, (int)(next - e->gen - 1));
-        }
-        while (plain >= e->chunk && err == cudaSuccess) {
-            if (!e->gx_chunk) err = capture(e, e->chunk, false, &e->gx_chunk);
-            if (err == cudaSuccess) err = cudaGraphLaunch(e->gx_chunk, e->stream);
-            plain -= e->chunk;
-            left -= e->chunk;
-            e->gen += e->chunk;
-        }
+        // plain generations until (and excluding) the next special one, in captured runs of
+        // 16, then 8, 4, 2, 1
+        const uint32_t next = next_special(e);
+        int plain = next ? std::min<int>(left, (int)(next - e->gen - 1u)) : left;
         while (plain > 0 && err == cudaSuccess) {
-            if (!e->gx_one) err = capture(e, 1, false, &e->gx_one);
-            if (err == cudaSuccess) err = cudaGraphLaunch(e->gx_one, e->stream);
-            --plain;
-            --left;
-            ++e->gen;
+            int k = kMaxRunLog;
+            while ((1 << k) > plain) --k;
+            if (!e->gx_run[k]) err = capture(e, 1 << k, false, &e->gx_run[k]);
+            if (err == cudaSuccess) err = cudaGraphLaunch(e->gx_run[k], e->stream);
+            plain -= 1 << k;
+            left -= 1 << k;
+            e->gen += 1u << k;
         }
         if (left > 0 && err == cudaSuccess) {
-            const bool mig = migration_due(e, e->gen + 1);
-            cudaGraphExec_t* gx = mig ? &e->gx_mig : &e->gx_one;
-            if (!*gx) err = capture(e, 1, mig, gx);
-            if (err == cudaSuccess) err = cudaGraphLaunch(*gx, e->stream);
+            // here e->gen + 1 == next
+            if (!e->gx_special) err = capture(e, 1, true, &e->gx_special);
+            if (err == cudaSuccess) err = cudaGraphLaunch(e->gx_special, e->stream);
             --left;
             ++e->gen;
         }

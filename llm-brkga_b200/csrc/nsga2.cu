@@ -1138,14 +1138,18 @@ cudaError_t nsga_enqueue_init(NsgaState& s, cudaStream_t st) {
     return nsga_enqueue_select(s.dd, 1, s.P, 1, st);
 }
 
-cudaError_t nsga_enqueue_generation(NsgaState& s, cudaStream_t st) {
+bool nsga_diversity_due(const NsgaState& s, uint32_t g) {
+    return s.div_interval > 0 && g >= 1u && ((g - 1u) % (uint32_t)s.div_interval) == 0u;
+}
+
+cudaError_t nsga_enqueue_generation(NsgaState& s, cudaStream_t st, bool with_diversity) {
     // offspring into pool rows [P, 2P) (core/solver.hpp:1019-1032) + their objectives
     cudaError_t e = launch_rows(nsga_rows(s, MODE_NSGA_OFF), s.kind, s.tile, s.grid, st);
     if (e != cudaSuccess) return e;
     // ranks, crowding and survivors of the pool (core/population.hpp:409-517)
     if ((e = nsga_enqueue_select(s.dd, 1, s.P, 0, st)) != cudaSuccess) return e;
     if ((e = nsga_enqueue_gather_finish(s.dd, 1, s.P, s.ld, st)) != cudaSuccess) return e;
-    if (s.div_interval > 0) {
+    if (with_diversity && s.div_interval > 0) {
         // decided on the device: due this generation, and fewer than 70% unique
         if ((e = nsga_enqueue_diversity(s.dd, 1, s.P, st)) != cudaSuccess) return e;
         if ((e = launch_rows(nsga_rows(s, MODE_NSGA_REFILL), s.kind, s.tile, s.grid, st)) != cudaSuccess) return e;

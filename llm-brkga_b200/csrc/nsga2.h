@@ -39,7 +39,13 @@ cudaError_t nsga_enqueue_diversity(PopDesc* dd, int npops, int maxP, cudaStream_
 void nsga_release(NsgaState& s);
 void nsga_set_history(NsgaState& s, float* h, int cap);
 cudaError_t nsga_enqueue_init(NsgaState& s, cudaStream_t st);
-cudaError_t nsga_enqueue_generation(NsgaState& s, cudaStream_t st);
+// one generation; with_diversity = false leaves out the diversity pass's launches (they
+// exit at once unless the pass is due after this generation: nsga_diversity_due)
+cudaError_t nsga_enqueue_generation(NsgaState& s, cudaStream_t st, bool with_diversity = true);
+// the diversity pass runs after generation g (counted from 1) when (g - 1) % interval == 0
+// (core/population.hpp:130-182 via core/solver.hpp:751-817), for a population with no
+// generation limit
+bool nsga_diversity_due(const NsgaState& s, uint32_t g);
 int32_t nsga_get_population(NsgaState& s, cudaStream_t st, float* keys, float* obj);
 int32_t nsga_set_population(NsgaState& s, cudaStream_t st, const float* keys);
 int32_t nsga_get_best(NsgaState& s, cudaStream_t st, float* keys, int32_t* perm, float* obj);

@@ -171,6 +171,31 @@ def test_engine_nsga2_diversity_rebuild(cuda):
     assert rebuilt > 0
 
 
+@pytest.mark.parametrize("strides", [(1, 7, 3, 13, 20, 16), (60,)])
+def test_engine_nsga2_diversity_strides(cuda, strides):
+    # evolve() splits a call into captured runs of 16/8/4/2/1 plain generations and one
+    # generation with the diversity pass whenever (g - 1) % interval == 0; uneven calls
+    # must give the same populations as single generations
+    n, P = 4, 40
+    a, b = I.tsp_coords(n + 1, seed=15), I.tsp_coords(n + 1, seed=16)
+    pb, po = B().bitsp(a, b), O.OracleProblem(O.BITSP_COORDS, n, xy=a, xy2=b)
+    s = B().Solver(pb, B().params(P, 0, 0, 0.7, sum(strides), seed=3, diversity_interval=5))
+    s.initialize()
+    ld = 4
+    pr = O.nsga2_params(P, 0, 0.7, 5.0 / n, 3, 5)
+    pop, obj, rank, cd = O.nsga2_init(po, pr, ld)
+    g = 0
+    for k in strides:
+        s.evolve(k)
+        for _ in range(k):
+            g += 1
+            O.nsga2_generation(po, pr, g, ld, pop, obj, rank, cd)
+        gk, go = s.get_population()
+        np.testing.assert_array_equal(gk, pop[:, :n], err_msg=f"generation {g}")
+        np.testing.assert_array_equal(go, obj, err_msg=f"generation {g}")
+    assert s.generation == g
+
+
 def test_invalid_params_rejected(cuda):
     xy = I.tsp_coords(10, seed=1)
     pb = B().tsp(xy)
