@@ -137,11 +137,14 @@ __global__ void dom_build_kernel(DomArgs a) {
 // comparisons of a pair give both directions: i dominates j iff !(a0 > b0) && !(a1 > b1)
 // && (a0 < b0 || a1 < b1), the reference's Individual::dominates (core/individual.hpp:99-114)
 // with its NaN behaviour; padding columns are NaN, which dominates nothing either way.
-constexpr int kDom2Rows = 4;     // rows per warp
-constexpr int kDom2Warps = 4;    // warps per CTA
+constexpr int kDom2Rows = 4;       // rows per warp
+constexpr int kDom2RowWarps = 4;   // row groups per CTA
+constexpr int kDom2ColGroups = 4;  // column groups: warp g of a row group takes the 32-word blocks b % 4 == g
+constexpr int kDom2Warps = kDom2RowWarps * kDom2ColGroups;
 
 __global__ void __launch_bounds__(kDom2Warps * 32) dom2_build_kernel(DomArgs a) {
     extern __shared__ float2 so[];  // [32 * ceil(N / 32)] objectives
+    __shared__ int cpart[kDom2ColGroups][kDom2RowWarps * kDom2Rows];
     const float* obj;
     int N, Wmax;
     uint32_t* S;
@@ -162,7 +165,7 @@ __global__ void __launch_bounds__(kDom2Warps * 32) dom2_build_kernel(DomArgs a) 
         cnt = a.cnt;
         Wmax = a.Wmax;
     }
-    constexpr int RPC = kDom2Rows * kDom2Warps;  // rows per CTA
+    constexpr int RPC = kDom2Rows * kDom2RowWarps;  // rows per CTA
     const int row0 = blockIdx.x * RPC;
     if (row0 >= N) return;
     const int W = (N + 31) / 32;
@@ -170,39 +173,50 @@ __global__ void __launch_bounds__(kDom2Warps * 32) dom2_build_kernel(DomArgs a) 
     for (int j = threadIdx.x; j < 32 * W; j += blockDim.x) so[j] = (j < N) ? __ldg(o2 + j) : make_float2(NAN, NAN);
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int i0 = row0 + warp * kDom2Rows;
+    const int rg = warp % kDom2RowWarps, cg = warp / kDom2RowWarps;
+    const int i0 = row0 + rg * kDom2Rows;
     float2 oi[kDom2Rows];
     int c[kDom2Rows];
-    uint32_t buf[kDom2Rows];
 #pragma unroll
     for (int r = 0; r < kDom2Rows; ++r) {
         oi[r] = so[min(i0 + r, N - 1)];
         c[r] = 0;
-        buf[r] = 0u;
     }
-    for (int w = 0; w < W; ++w) {
-        const float2 oj = so[32 * w + lane];
+    const int nblk = (W + 31) / 32;
+    for (int b = cg; b < nblk; b += kDom2ColGroups) {
+        uint32_t buf[kDom2Rows];
 #pragma unroll
-        for (int r = 0; r < kDom2Rows; ++r) {
-            const bool gt0 = oi[r].x > oj.x, gt1 = oi[r].y > oj.y;
-            const bool lt0 = oi[r].x < oj.x, lt1 = oi[r].y < oj.y;
-            const uint32_t si = __ballot_sync(0xffffffffu, !gt0 && !gt1 && (lt0 || lt1));
-            const uint32_t di = __ballot_sync(0xffffffffu, !lt0 && !lt1 && (gt0 || gt1));
-            c[r] += __popc(di);
-            if (lane == (w & 31)) buf[r] = si;
-        }
-        if ((w & 31) == 31 || w == W - 1) {
-            // lane l holds word (w & ~31) + l of each row: one coalesced store per row
-            const int wl = (w & ~31) + lane;
+        for (int r = 0; r < kDom2Rows; ++r) buf[r] = 0u;
+        const int wend = min(W, 32 * b + 32);
+        for (int w = 32 * b; w < wend; ++w) {
+            const float2 oj = so[32 * w + lane];
 #pragma unroll
-            for (int r = 0; r < kDom2Rows; ++r)
-                if (i0 + r < N && wl <= w) S[(size_t)(i0 + r) * Wmax + wl] = buf[r];
+            for (int r = 0; r < kDom2Rows; ++r) {
+                const bool gt0 = oi[r].x > oj.x, gt1 = oi[r].y > oj.y;
+                const bool lt0 = oi[r].x < oj.x, lt1 = oi[r].y < oj.y;
+                const uint32_t si = __ballot_sync(0xffffffffu, !gt0 && !gt1 && (lt0 || lt1));
+                const uint32_t di = __ballot_sync(0xffffffffu, !lt0 && !lt1 && (gt0 || gt1));
+                c[r] += __popc(di);
+                if (lane == (w & 31)) buf[r] = si;
+            }
         }
-    }
-    if (lane == 0) {
+        // lane l holds word 32 b + l of each row: one coalesced store per row
+        const int wl = 32 * b + lane;
 #pragma unroll
         for (int r = 0; r < kDom2Rows; ++r)
-            if (i0 + r < N) cnt[i0 + r] = c[r];
+            if (i0 + r < N && wl < wend) S[(size_t)(i0 + r) * Wmax + wl] = buf[r];
+    }
+    // dominator counts: the column groups' partial counts, added in a fixed order
+    if (lane == 0) {
+#pragma unroll
+        for (int r = 0; r < kDom2Rows; ++r) cpart[cg][rg * kDom2Rows + r] = c[r];
+    }
+    __syncthreads();
+    if (threadIdx.x < RPC && row0 + (int)threadIdx.x < N) {
+        int sum = 0;
+#pragma unroll
+        for (int g = 0; g < kDom2ColGroups; ++g) sum += cpart[g][threadIdx.x];
+        cnt[row0 + threadIdx.x] = sum;
     }
 }
 
@@ -824,36 +838,46 @@ __global__ void __launch_bounds__(kNsgaBlock) peel_op_kernel(int N, const uint32
     for (int i = threadIdx.x; i < N; i += kNsgaBlock) rank[i] = r16[i];
 }
 
-// survivors -> the other pool buffer, rows [0, P); population blockIdx.y
-__global__ void nsga_gather_kernel(PopDesc* dd) {
-    const PopDesc& d = dd[blockIdx.y];
-    if (at_limit(d)) return;
-    const int P = d.P, ld4 = d.ld / 4, m = d.m;
-    const float4* src = reinterpret_cast<const float4*>(d.keys[d.cur]);
-    float4* dst = reinterpret_cast<float4*>(d.keys[d.cur ^ 1]);
-    const float* fs = d.fit[d.cur];
-    float* fd = d.fit[d.cur ^ 1];
-    const size_t total = (size_t)P * ld4;
-    for (size_t x = (size_t)blockIdx.x * blockDim.x + threadIdx.x; x < total; x += (size_t)gridDim.x * blockDim.x) {
-        const int q = (int)(x / ld4), c = (int)(x % ld4);
-        const size_t sq = (size_t)__ldg(d.nsel + q);
-        dst[x] = src[sq * ld4 + c];
-        if (c == 0)
-            for (int o = 0; o < m; ++o) fd[(size_t)q * m + o] = fs[sq * m + o];
-    }
-}
+// survivors -> the other pool buffer, rows [0, P), one warp per row (population
+// blockIdx.y); then the last CTA of the population (completion counter) swaps the pool
+// buffers and advances the generation.  A population at its generation limit only
+// records that it did not advance.
+constexpr int kGatherWarps = 8;
 
-// one thread per population: swap the pool buffers, advance the generation
-__global__ void nsga_finish_kernel(PopDesc* dd, int npops) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p < npops) {
-        if (at_limit(dd[p])) {
-            dd[p].advanced = 0;
-            return;
+__global__ void __launch_bounds__(kGatherWarps * 32) nsga_gather_kernel(PopDesc* dd) {
+    PopDesc& d = dd[blockIdx.y];
+    if (at_limit(d)) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) d.advanced = 0;
+        return;
+    }
+    const int P = d.P, ld4 = d.ld / 4, m = d.m, cur = d.cur;
+    const int lane = threadIdx.x & 31;
+    const int q = blockIdx.x * kGatherWarps + (threadIdx.x >> 5);
+    if (q < P) {
+        const size_t sq = (size_t)__ldg(d.nsel + q);
+        const float4* src = reinterpret_cast<const float4*>(d.keys[cur]) + sq * ld4;
+        float4* dst = reinterpret_cast<float4*>(d.keys[cur ^ 1]) + (size_t)q * ld4;
+        int c = lane;
+        for (; c + 96 < ld4; c += 128) {
+            const float4 a0 = src[c], a1 = src[c + 32], a2 = src[c + 64], a3 = src[c + 96];
+            dst[c] = a0;
+            dst[c + 32] = a1;
+            dst[c + 64] = a2;
+            dst[c + 96] = a3;
         }
-        dd[p].cur ^= 1;
-        dd[p].gen += 1;
-        dd[p].advanced = 1;
+        for (; c < ld4; c += 32) dst[c] = src[c];
+        if (lane < m) d.fit[cur ^ 1][(size_t)q * m + lane] = d.fit[cur][sq * m + lane];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(d.done, 1) == (int)gridDim.x - 1) {
+            d.cur = cur ^ 1;
+            d.gen += 1;
+            d.advanced = 1;
+            *d.done = 0;
+            __threadfence();
+        }
     }
 }
 
@@ -999,7 +1023,7 @@ cudaError_t nsga_prepare(int maxP) {
 
 // two-objective dominance rows of up to maxN points per population (grid.y)
 static cudaError_t launch_dom2(const DomArgs& a, int maxN, int npops, cudaStream_t st) {
-    constexpr int RPC = kDom2Rows * kDom2Warps;
+    constexpr int RPC = kDom2Rows * kDom2RowWarps;
     const size_t smem = (size_t)((maxN + 31) / 32) * 32 * sizeof(float2);
     cudaError_t e = raise_smem_limit(reinterpret_cast<const void*>(dom2_build_kernel), smem);
     if (e != cudaSuccess) return e;
@@ -1031,11 +1055,8 @@ cudaError_t nsga_enqueue_select(PopDesc* dd, int npops, int maxP, int mode, cuda
 }
 
 cudaError_t nsga_enqueue_gather_finish(PopDesc* dd, int npops, int maxP, int maxld, cudaStream_t st) {
-    const int blocks = std::max(1, std::min(256, (maxP * (maxld / 4) + 255) / 256));
-    nsga_gather_kernel<<<dim3(blocks, npops), 256, 0, st>>>(dd);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    nsga_finish_kernel<<<(npops + 127) / 128, 128, 0, st>>>(dd, npops);
+    (void)maxld;
+    nsga_gather_kernel<<<dim3((maxP + kGatherWarps - 1) / kGatherWarps, npops), kGatherWarps * 32, 0, st>>>(dd);
     return cudaGetLastError();
 }
 
