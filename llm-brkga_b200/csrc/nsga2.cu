@@ -597,6 +597,12 @@ __device__ __forceinline__ bool select_active(const PopDesc& d, int mode) {
 // sum of the member rows' words over those columns.  The front masks are exchanged through
 // distributed shared memory with one cluster barrier per front, so the dominance rows are
 // read by eight SMs instead of one.  Ranks -> domcnt[0, N).
+//
+// The pool of a generation (mode 0) is peeled only up to the front where the survivors
+// (rank-0 points counted twice) first exceed P: that front is cut by crowding, and no
+// later front is selected.  The points left then get that front's rank + 1 as one last
+// front.  Selection, crowding of every selected point and the ranks kept for the next
+// generation are the same as with every front peeled.
 constexpr int kPeelCluster = 8, kPeelWords = 16, kPeelThreads = 256;
 constexpr int kPeelSlices = kPeelThreads / kPeelWords, kPeelWarps = kPeelThreads / 32;
 
@@ -645,6 +651,7 @@ __global__ void __cluster_dims__(kPeelCluster, 1, 1) __launch_bounds__(kPeelThre
     }
     cluster.sync();
     constexpr int NW = kPeelCluster * kPeelWords;
+    int survivors = 0, rest = 0;
     for (int k = 0; k < N; ++k) {
         // the whole front k, gathered from every CTA of the cluster
         if (t < NW) {
@@ -659,6 +666,13 @@ __global__ void __cluster_dims__(kPeelCluster, 1, 1) __launch_bounds__(kPeelThre
             for (uint32_t x = Ffull[t]; x; x &= x - 1) list[base++] = (uint16_t)(32 * t + __ffs(x) - 1);
         __syncthreads();
         if (nf == 0) break;  // every CTA sees the same front
+        if (mode == 0) {
+            survivors += (k == 0) ? 2 * (int)nf : (int)nf;
+            if (survivors > d.P) {
+                rest = k + 1;
+                break;
+            }
+        }
         // column sums over the front's rows: thread (word t % 16, slice t / 16); the member
         // rows' words are loaded sixteen at a time (one L2 round trip for fronts of up to
         // 256 members) into 5-plane counters
@@ -764,7 +778,7 @@ __global__ void __cluster_dims__(kPeelCluster, 1, 1) __launch_bounds__(kPeelThre
     cluster.sync();  // no CTA leaves while another may still read its front words
     for (int x = t; x < kPeelWords * 32; x += kPeelThreads) {
         const int i = 32 * w0 + x;
-        if (i < N) d.domcnt[i] = r16[x];
+        if (i < N) d.domcnt[i] = ((A[x >> 5] >> (x & 31)) & 1u) ? r16[x] : (uint16_t)rest;
     }
 }
 
