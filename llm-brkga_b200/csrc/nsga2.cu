@@ -137,6 +137,22 @@ __global__ void dom_build_kernel(DomArgs a) {
 // comparisons of a pair give both directions: i dominates j iff !(a0 > b0) && !(a1 > b1)
 // && (a0 < b0 || a1 < b1), the reference's Individual::dominates (core/individual.hpp:99-114)
 // with its NaN behaviour; padding columns are NaN, which dominates nothing either way.
+// Element i of [0, count) for i = threadIdx.x + k * T: a thread issues the loads of K of
+// its elements before the first store, so staging takes one memory round trip per K
+// elements instead of one per element.
+template <int T, int K, typename Ld, typename St>
+__device__ __forceinline__ void staged(int count, Ld ld, St st) {
+    for (int i0 = (int)threadIdx.x; i0 < count; i0 += T * K) {
+        decltype(ld(0)) v[K];
+#pragma unroll
+        for (int u = 0; u < K; ++u)
+            if (i0 + u * T < count) v[u] = ld(i0 + u * T);
+#pragma unroll
+        for (int u = 0; u < K; ++u)
+            if (i0 + u * T < count) st(i0 + u * T, v[u]);
+    }
+}
+
 constexpr int kDom2Rows = 4;       // rows per warp
 constexpr int kDom2RowWarps = 4;   // row groups per CTA
 constexpr int kDom2ColGroups = 4;  // column groups: warp g of a row group takes the 32-word blocks b % 4 == g
@@ -170,7 +186,9 @@ __global__ void __launch_bounds__(kDom2Warps * 32) dom2_build_kernel(DomArgs a) 
     if (row0 >= N) return;
     const int W = (N + 31) / 32;
     const float2* o2 = reinterpret_cast<const float2*>(obj);
-    for (int j = threadIdx.x; j < 32 * W; j += blockDim.x) so[j] = (j < N) ? __ldg(o2 + j) : make_float2(NAN, NAN);
+    staged<kDom2Warps * 32, 8>(
+        32 * W, [&](int j) { return (j < N) ? __ldg(o2 + j) : make_float2(NAN, NAN); },
+        [&](int j, float2 v) { so[j] = v; });
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int rg = warp % kDom2RowWarps, cg = warp / kDom2RowWarps;
@@ -487,10 +505,9 @@ __device__ void crowding_given(int N, const SelSmem& s, const int32_t* __restric
     for (int i = t; i < N; i += T) s.cd[i] = 0.0f;
     for (int o = 0; o < 2; ++o) {
         __syncthreads();
-        for (int p = t; p < N; p += T) {
-            const int i = __ldg(ord + (size_t)o * ostride + p);
-            s.key[p] = order_key(s.rank[i], s.obj[2 * i + o], i);
-        }
+        staged<T, 4>(
+            N, [&](int p) { return __ldg(ord + (size_t)o * ostride + p); },
+            [&](int p, int i) { s.key[p] = order_key(s.rank[i], s.obj[2 * i + o], i); });
         __syncthreads();
         front_bounds<T>(N, s);
         __syncthreads();
@@ -796,7 +813,9 @@ __global__ void __launch_bounds__(kOrdThreads) nsga_order_kernel(PopDesc* dd, in
     if (base >= N) return;
     const int o = blockIdx.y, t = threadIdx.x;
     const float* f = d.fit[d.cur];
-    for (int i = t; i < N; i += kOrdThreads) okeys[i] = order_key(__ldg(d.domcnt + i), __ldg(f + 2 * i + o), i);
+    staged<kOrdThreads, 4>(
+        N, [&](int i) { return make_int2(__ldg(d.domcnt + i), __float_as_int(__ldg(f + 2 * i + o))); },
+        [&](int i, int2 v) { okeys[i] = order_key(v.x, __int_as_float(v.y), i); });
     __syncthreads();
     const int lane = t & 31, i = base + (t >> 5);
     const unsigned long long me = (i < N) ? okeys[i] : 0ull;
@@ -820,8 +839,9 @@ __global__ void __launch_bounds__(kNsgaBlock) nsga_select_kernel(PopDesc* dd, in
     const int N = (mode == 0) ? 2 * P : P;
     const float* f = d.fit[d.cur];
     const SelSmem s = sel_carve(smem, N);
-    for (int i = t; i < 2 * N; i += kNsgaBlock) s.obj[i] = f[i];
-    for (int i = t; i < N; i += kNsgaBlock) s.rank[i] = (uint16_t)__ldg(d.domcnt + i);
+    staged<kNsgaBlock, 8>(2 * N, [&](int i) { return __ldg(f + i); }, [&](int i, float v) { s.obj[i] = v; });
+    staged<kNsgaBlock, 4>(N, [&](int i) { return __ldg(d.domcnt + i); },
+                          [&](int i, int v) { s.rank[i] = (uint16_t)v; });
     crowding_given<kNsgaBlock>(N, s, d.nord, 2 * P);
     float fmin = INFINITY;
     if (mode == 0) {
