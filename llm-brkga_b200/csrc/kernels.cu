@@ -1201,24 +1201,38 @@ __global__ void __launch_bounds__(RK_THREADS) rank_kernel(RankArgs a) {
     }
     const int base = blockIdx.x * RK_CH;
     if (base >= P) return;
-    // issue every global load of this thread before the first use (one HBM round trip)
-    constexpr int RK_BATCH = 8;
-    for (int i0 = t; i0 < P; i0 += RK_THREADS * RK_BATCH) {
-        float v[RK_BATCH];
-#pragma unroll
-        for (int u = 0; u < RK_BATCH; ++u) {
-            const int i = i0 + u * RK_THREADS;
-            v[u] = (i < P) ? __ldg(f + (size_t)i * m) : 0.0f;
-        }
-#pragma unroll
-        for (int u = 0; u < RK_BATCH; ++u) {
-            const int i = i0 + u * RK_THREADS;
-            if (i < P) rk_keys[i] = ((unsigned long long)fitkey(v[u], mx) << 32) | (uint32_t)i;
-        }
-    }
-    __syncthreads();
     const int e = t / RK_TPE, part = t % RK_TPE;
     const int i = base + e;
+    // a batch of this thread's global loads is issued before the first use (one round trip)
+    constexpr int RK_BATCH = 8;
+    float v[RK_BATCH];
+    auto load = [&](int i0) {
+#pragma unroll
+        for (int u = 0; u < RK_BATCH; ++u) {
+            const int j = i0 + u * RK_THREADS;
+            v[u] = (j < P) ? __ldg(f + (size_t)j * m) : 0.0f;
+        }
+    };
+    auto store = [&](int i0) {
+#pragma unroll
+        for (int u = 0; u < RK_BATCH; ++u) {
+            const int j = i0 + u * RK_THREADS;
+            if (j < P) rk_keys[j] = ((unsigned long long)fitkey(v[u], mx) << 32) | (uint32_t)j;
+        }
+    };
+    load(t);
+    if (d && part == 1 && d->parents && i >= d->E && i < P - d->M) {
+        // parent ranks of child row i of generation gen_new + 1 (core/solver.hpp:1117-1118);
+        // they do not depend on the fitness, so they are drawn while its loads are in flight
+        const uint4 pr = draw4(d->seed, 0u, (uint32_t)i, gen_new + 1, (d->island << 8) | TAG_PARENT);
+        d->parents[i] = make_int2((int)pick(pr.x, (uint32_t)d->E), d->E + (int)pick(pr.y, (uint32_t)(P - d->E)));
+    }
+    store(t);
+    for (int i0 = t + RK_THREADS * RK_BATCH; i0 < P; i0 += RK_THREADS * RK_BATCH) {
+        load(i0);
+        store(i0);
+    }
+    __syncthreads();
     const unsigned long long me = (i < P) ? rk_keys[i] : 0ull;
     // part p counts j = p, p + TPE, ...: the TPE parts of a warp read consecutive keys
     int cnt = 0;
@@ -1231,11 +1245,6 @@ __global__ void __launch_bounds__(RK_THREADS) rank_kernel(RankArgs a) {
         if (cnt == 0 && d && d->history && (int)gen_new < d->hist_cap) d->history[gen_new] = f[(size_t)i * m];
     }
     if (d) {
-        // parent ranks of child row i of generation gen_new + 1 (core/solver.hpp:1117-1118)
-        if (part == 1 && d->parents && i >= d->E && i < P - d->M) {
-            const uint4 pr = draw4(d->seed, 0u, (uint32_t)i, gen_new + 1, (d->island << 8) | TAG_PARENT);
-            d->parents[i] = make_int2((int)pick(pr.x, (uint32_t)d->E), d->E + (int)pick(pr.y, (uint32_t)(P - d->E)));
-        }
         if (a.flip) {
             __syncthreads();
             if (t == 0) {
