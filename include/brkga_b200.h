@@ -49,10 +49,17 @@ typedef enum {
     BRKGA_CONTINUOUS = 9,        /* ContinuousOptGPUConfig(n, lower, upper, function): x = key *
                                     (upper - lower) + lower; sphere / Rastrigin / Rosenbrock
                                     (configs/continuous_opt_gpu_config.hpp:37-57, 114-173)                  */
-    BRKGA_MOVRP = 10             /* MultiObjectiveVRPConfig: capacitated routes from one biased argsort;
+    BRKGA_MOVRP = 10,            /* MultiObjectiveVRPConfig: capacitated routes from one biased argsort;
                                     objectives total distance and longest route, with the reference's
                                     overload and fleet penalties (configs/multi_objective_vrp_config.hpp:
                                     214-313); two objectives, so runs take the NSGA-II path            */
+    BRKGA_EXTERNAL = 11          /* a config that brings its own fitness (BRKGAConfig::fitness_function, or
+                                    its own evaluate_population_gpu kernel; core/config.hpp:33-53): n
+                                    keys per row, one objective, direction from `maximize`.  The engine
+                                    builds rows and ranks them; the caller evaluates them between
+                                    brkga_external_begin and brkga_external_commit.  Engines only (one
+                                    island); the evaluation entry points, batches and the server
+                                    reject it                                                           */
 } brkga_problem_kind;
 
 /* functions of BRKGA_CONTINUOUS (the reference's OptimizationFunction) */
@@ -89,6 +96,9 @@ typedef struct {
     const int32_t* demands;      /* MO-VRP                                                    */
     int32_t vehicle_capacity;
     int32_t vehicles;
+    int32_t maximize;            /* BRKGA_EXTERNAL: 1 = larger fitness is better (the
+                                    reference's comparator, core/config.hpp:36); other kinds
+                                    fix their own direction and ignore it                     */
 } brkga_problem_desc;
 
 /* GA parameters (BRKGAConfig fields, core/config.hpp:17-30, plus the engine's own). */
@@ -246,6 +256,34 @@ int32_t brkga_set_population(brkga_engine* e, const float* keys);
 /* Solver::get_pareto_front (core/solver.hpp:1629): rank-0 members; objectives [cap][m],
  * keys [cap][n] (may be NULL); *count receives the front size (may exceed cap). */
 int32_t brkga_get_pareto_front(brkga_engine* e, float* objectives, float* keys, int32_t cap, int32_t* count);
+
+/* ---- external fitness (BRKGA_EXTERNAL engines) -------------------------------------------
+ * One generation of Solver::evolve_generation (core/solver.hpp:234-273) with the fitness
+ * from the caller, as the reference evaluates a config's fitness_function or its own
+ * evaluate_population_gpu (core/population.hpp:567-595, core/config.hpp:50-53):
+ *   brkga_external_begin   builds the rows on the device (the initial population on the
+ *                          first call, and on the first call after brkga_initialize; the
+ *                          next generation's rows after that), waits for them and returns the device
+ *                          buffers: *d_keys rows of *ld floats, *d_fitness one float per
+ *                          row.  Rows [*first, P) need a fitness: all rows at
+ *                          initialisation, the non-elite rows of a generation (elite rows
+ *                          keep theirs, as the reference's evaluated flag does).  With
+ *                          dense = 1 the keys are a packed [P][n] copy (*ld = n), the
+ *                          layout evaluate_population_gpu expects.
+ *   brkga_external_get_rows  the pending rows [first, P) into host keys [P - first][n].
+ *   brkga_external_set_fitness  host fitness [P - first] for those rows.
+ *   brkga_external_commit  waits for the device (so fitness that the caller's kernels
+ *                          wrote on any stream is in place), ranks the population (elite
+ *                          partition, best-fitness history) and completes the generation;
+ *                          waits for the engine.  On these engines brkga_initialize only restarts (the next
+ * begin builds a new initial population); brkga_evolve, brkga_run and
+ * brkga_set_population return BRKGA_ERR_UNSUPPORTED; brkga_get_best gives keys and
+ * fitness, not a permutation (the engine does not decode an external problem). */
+int32_t brkga_external_begin(brkga_engine* e, int32_t dense, float** d_keys, float** d_fitness, int32_t* ld,
+                             int32_t* first);
+int32_t brkga_external_get_rows(brkga_engine* e, float* keys);
+int32_t brkga_external_set_fitness(brkga_engine* e, const float* fitness);
+int32_t brkga_external_commit(brkga_engine* e);
 
 /* ---- batched solving (many independent instances advanced together) --------------------- */
 typedef struct brkga_batch brkga_batch;

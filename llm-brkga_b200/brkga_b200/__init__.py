@@ -24,6 +24,7 @@ HEADER_PATH = os.path.join(REPO_DIR, "include", "brkga_b200.h")
 TSP_COORDS, TSP_MATRIX, KNAP_THRESHOLD, KNAP_GREEDY, BITSP_COORDS, BITSP_MATRIX, TSPJ = 1, 2, 3, 4, 5, 6, 7
 JOBSCHED, CONTINUOUS = 8, 9
 MOVRP = 10
+EXTERNAL = 11
 SPHERE, RASTRIGIN, ROSENBROCK = 0, 1, 2
 
 STATUS = {0: "OK", -1: "INVALID", -2: "OOM", -3: "CUDA", -4: "TIMEOUT", -5: "CANCELLED",
@@ -41,7 +42,8 @@ class ProblemDesc(C.Structure):
                 ("matrix", C.c_void_p), ("matrix2", C.c_void_p), ("weights", C.c_void_p),
                 ("values", C.c_void_p), ("capacity", C.c_float), ("job_times", C.c_void_p),
                 ("machines", C.c_int32), ("function", C.c_int32), ("lower", C.c_float), ("upper", C.c_float),
-                ("demands", C.c_void_p), ("vehicle_capacity", C.c_int32), ("vehicles", C.c_int32)]
+                ("demands", C.c_void_p), ("vehicle_capacity", C.c_int32), ("vehicles", C.c_int32),
+                ("maximize", C.c_int32)]
 
 
 class Params(C.Structure):
@@ -108,6 +110,11 @@ def lib():
         "brkga_get_population": (_i32, [_vp, _vp, _vp]),
         "brkga_set_population": (_i32, [_vp, _vp]),
         "brkga_get_pareto_front": (_i32, [_vp, _vp, _vp, _i32, C.POINTER(_i32)]),
+        "brkga_external_begin": (_i32, [_vp, _i32, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_i32),
+                                        C.POINTER(_i32)]),
+        "brkga_external_get_rows": (_i32, [_vp, _vp]),
+        "brkga_external_set_fitness": (_i32, [_vp, _vp]),
+        "brkga_external_commit": (_i32, [_vp]),
         "brkga_batch_create": (_i32, [C.POINTER(_vp), C.POINTER(Params), _i32, C.POINTER(_vp)]),
         "brkga_batch_destroy": (_i32, [_vp]),
         "brkga_batch_evolve": (_i32, [_vp, _i32]),
@@ -169,7 +176,7 @@ class Problem:
 
     def __init__(self, kind, n, coords=None, coords2=None, matrix=None, matrix2=None, weights=None, values=None,
                  capacity=0.0, device=0, job_times=None, machines=0, function=0, lower=0.0, upper=0.0,
-                 demands=None, vehicle_capacity=0, vehicles=0):
+                 demands=None, vehicle_capacity=0, vehicles=0, maximize=False):
         keep = []
 
         def arr(a, dt):
@@ -182,7 +189,7 @@ class Problem:
         d = ProblemDesc(kind, n, arr(coords, np.float32), arr(coords2, np.float32), arr(matrix, np.float32),
                         arr(matrix2, np.float32), arr(weights, np.int32), arr(values, np.int32), float(capacity),
                         arr(job_times, np.float32), int(machines), int(function), float(lower), float(upper),
-                        arr(demands, np.int32), int(vehicle_capacity), int(vehicles))
+                        arr(demands, np.int32), int(vehicle_capacity), int(vehicles), int(bool(maximize)))
         h = C.c_void_p()
         check(lib().brkga_problem_create(C.byref(d), device, C.byref(h)))
         # n is the chromosome length (genes); a TSPJ instance of c cities has 2c genes
@@ -264,6 +271,12 @@ def movrp(coords, demands, vehicle_capacity, vehicles, device=0):
     coords = np.asarray(coords, np.float32)
     return Problem(MOVRP, coords.shape[0] - 1, coords=coords, demands=demands, vehicle_capacity=vehicle_capacity,
                    vehicles=vehicles, device=device)
+
+
+def external(n, maximize=False, device=0):
+    """A problem whose fitness the caller computes (a BRKGAConfig with its own
+    fitness_function, core/config.hpp:33-53): n keys per row, one objective."""
+    return Problem(EXTERNAL, n, device=device, maximize=maximize)
 
 
 def movrp_routes(perm, demands, vehicle_capacity):
@@ -356,10 +369,44 @@ class Solver:
 
     def get_best_individual(self):
         keys = np.zeros(self.n, np.float32)
-        perm = np.zeros(self.n, np.int32)
         fit = np.zeros(2, np.float32)
+        if self.problem.kind == EXTERNAL:  # not decoded by the engine
+            check(lib().brkga_get_best(self.h, _ptr(keys), None, _ptr(fit)))
+            return keys, None, fit[0]
+        perm = np.zeros(self.n, np.int32)
         check(lib().brkga_get_best(self.h, _ptr(keys), _ptr(perm), _ptr(fit)))
         return keys, perm, (fit[0] if self.m == 1 else fit[:2].copy())
+
+    # external fitness (Problem of kind EXTERNAL): the engine builds and ranks the rows, the
+    # caller evaluates rows [first, P) between begin and commit
+    def external_begin(self, dense=False):
+        """(keys address, fitness address, row stride in floats, first row to evaluate)"""
+        k, f, ld, first = C.c_void_p(), C.c_void_p(), C.c_int32(), C.c_int32()
+        check(lib().brkga_external_begin(self.h, int(bool(dense)), C.byref(k), C.byref(f), C.byref(ld),
+                                         C.byref(first)))
+        self._ext_first = first.value
+        return k.value, f.value, ld.value, first.value
+
+    def external_rows(self):
+        keys = np.zeros((self.prm.population_size - self._ext_first, self.n), np.float32)
+        check(lib().brkga_external_get_rows(self.h, _ptr(keys)))
+        return keys
+
+    def external_set_fitness(self, fitness):
+        fitness = np.ascontiguousarray(fitness, np.float32)
+        if fitness.shape != (self.prm.population_size - self._ext_first,):
+            raise ValueError(f"need {self.prm.population_size - self._ext_first} fitness values")
+        check(lib().brkga_external_set_fitness(self.h, _ptr(fitness)))
+
+    def external_commit(self):
+        check(lib().brkga_external_commit(self.h))
+
+    def external_step(self, fitness_of_rows):
+        """one generation (the initial population on the first call): fitness_of_rows maps
+        keys [rows][n] (numpy) to their fitness [rows]"""
+        self.external_begin()
+        self.external_set_fitness(fitness_of_rows(self.external_rows()))
+        self.external_commit()
 
     def get_fitness_history(self):
         cap = self.generation + 1

@@ -8,9 +8,11 @@
 // prints and swallows are thrown here as std::runtime_error with the library's message.
 //
 // Scope: the problem configs the engine implements on the GPU (TSP from a matrix or from
-// TSPLIB coordinates, 0/1 knapsack, bi-objective TSP).  A config that only supplies a
-// host std::function fitness (no GPU kernel) is rejected by Solver, because the engine
-// has no host fitness path.
+// TSPLIB coordinates, knapsack, bi-objective TSP, TSPJ, job scheduling, continuous
+// functions, MO-VRP), and single-objective configs that bring their own fitness -- a host
+// fitness_function or their own evaluate_population_gpu kernel, as LLM-written configs do.
+// Those run on the engine's external-fitness path: keys, crossover, mutants and the elite
+// partition on the device, the config's fitness between them.
 #ifndef BRKGA_B200_HPP
 #define BRKGA_B200_HPP
 
@@ -795,8 +797,23 @@ public:
     Solver(std::unique_ptr<BRKGAConfig<T>> cfg, bool verbose = true, int print_freq = 50)
         : config_(std::move(cfg)), verbose_(verbose), print_freq_(print_freq) {
         if (!config_->is_valid()) throw std::runtime_error("Invalid configuration");
+        n_ = config_->get_total_chromosome_length();
         brkga_problem* pb = config_->problem_handle();
-        if (!pb) throw std::runtime_error("this config has no device problem; the engine has no host fitness path");
+        if (!pb) {
+            // a config with its own fitness: the engine's external-fitness path
+            if (config_->num_objectives > 1)
+                throw std::runtime_error("a multi-objective config needs a device problem (host objective_functions "
+                                         "are not evaluated by this engine)");
+            if (!config_->fitness_function && !config_->has_gpu_evaluation())
+                throw std::runtime_error("config has neither a fitness_function nor GPU evaluation");
+            brkga_problem_desc d{};
+            d.kind = BRKGA_EXTERNAL;
+            d.n = n_;
+            // the reference's comparator says which fitness is better (core/config.hpp:36)
+            d.maximize = (config_->comparator && config_->comparator(T(1), T(0))) ? 1 : 0;
+            brkga_b200_detail::check(brkga_problem_create(&d, config_->device, &ext_pb_), "Solver");
+            pb = ext_pb_;
+        }
         brkga_params p;
         brkga_params_default(&p);
         p.population_size = config_->population_size;
@@ -814,21 +831,48 @@ public:
             p.local_search_individuals = config_->local_search_individuals;
             p.local_search_moves = config_->local_search_moves;
         }
-        brkga_b200_detail::check(brkga_create(pb, &p, &e_), "Solver");
-        n_ = config_->get_total_chromosome_length();
+        const int32_t rc = brkga_create(pb, &p, &e_);
+        if (rc != BRKGA_OK) {
+            char buf[512];
+            brkga_last_error(buf, sizeof(buf));
+            if (ext_pb_) brkga_problem_destroy(ext_pb_);
+            ext_pb_ = nullptr;
+            throw std::runtime_error(std::string("Solver: ") + buf);
+        }
         best_ = Individual<T>(config_->component_lengths, config_->num_objectives > 1 ? config_->num_objectives : 0);
     }
     ~Solver() {
         if (e_) brkga_destroy(e_);
+        if (ext_pb_) brkga_problem_destroy(ext_pb_);
     }
     Solver(const Solver&) = delete;
     Solver& operator=(const Solver&) = delete;
 
-    void initialize() { brkga_b200_detail::check(brkga_initialize(e_), "initialize"); }
-    void evolve_generation() { brkga_b200_detail::check(brkga_evolve(e_, 1), "evolve_generation"); }
-    void evolve(int generations) { brkga_b200_detail::check(brkga_evolve(e_, generations), "evolve"); }
+    void initialize() {
+        brkga_b200_detail::check(brkga_initialize(e_), "initialize");
+        if (ext_pb_) external_generation();  // the initial population, evaluated by the config
+        initialized_ = true;
+    }
+    void evolve_generation() { evolve(1); }
+    void evolve(int generations) {
+        if (!ext_pb_) {
+            brkga_b200_detail::check(brkga_evolve(e_, generations), "evolve");
+            return;
+        }
+        if (!initialized_) initialize();
+        for (int g = 0; g < generations; ++g) {
+            external_generation();
+            if (verbose_ && print_freq_ > 0 && brkga_generation(e_) % print_freq_ == 0)
+                std::cout << "Generation " << brkga_generation(e_) << ": best fitness " << std::setprecision(6)
+                          << get_best_individual().fitness << std::endl;
+        }
+    }
+    // Solver::run (core/solver.hpp:1517-1556): initialize, then config->max_generations
+    // generations (read now, so a caller may change it after construction)
     void run() {
-        brkga_b200_detail::check(brkga_run(e_), "run");
+        initialize();
+        evolve(config_->max_generations);
+        brkga_b200_detail::check(brkga_synchronize(e_), "run");
         if (verbose_) {
             const auto& b = get_best_individual();
             std::cout << "Evolution completed: " << brkga_generation(e_) << " generations, best fitness "
@@ -890,9 +934,45 @@ public:
     }
 
 private:
+    // one generation (the initial population first) with the config's own fitness: its
+    // evaluate_population_gpu on dense device rows, or its fitness_function on each row
+    // (core/population.hpp:567-595; elite rows keep their fitness)
+    void external_generation() {
+        float* dk = nullptr;
+        float* df = nullptr;
+        int32_t ld = 0, first = 0;
+        const bool gpu = config_->has_gpu_evaluation();
+        brkga_b200_detail::check(brkga_external_begin(e_, gpu ? 1 : 0, &dk, &df, &ld, &first), "evolve_generation");
+        const int count = config_->population_size - first;
+        if (gpu) {
+            config_->evaluate_population_gpu(reinterpret_cast<T*>(dk + (size_t)first * ld),
+                                             reinterpret_cast<T*>(df + first), count, n_);
+        } else {
+            rows_.resize((size_t)count * n_);
+            fit_.resize((size_t)count);
+            brkga_b200_detail::check(brkga_external_get_rows(e_, rows_.data()), "evolve_generation");
+            Individual<T> ind(config_->component_lengths, 0);
+            for (int i = 0; i < count; ++i) {
+                size_t off = (size_t)i * n_;
+                for (size_t c = 0; c < ind.chromosomes.size(); ++c) {
+                    const size_t len = (size_t)config_->component_lengths[c];
+                    ind.chromosomes[c].assign(rows_.begin() + off, rows_.begin() + off + len);
+                    off += len;
+                }
+                ind.evaluated = false;
+                fit_[i] = (float)config_->fitness_function(ind);
+            }
+            brkga_b200_detail::check(brkga_external_set_fitness(e_, fit_.data()), "evolve_generation");
+        }
+        brkga_b200_detail::check(brkga_external_commit(e_), "evolve_generation");
+    }
+
     std::unique_ptr<BRKGAConfig<T>> config_;
     bool verbose_;
     int print_freq_;
+    brkga_problem* ext_pb_ = nullptr;  // the external-fitness problem this Solver made
+    bool initialized_ = false;
+    std::vector<float> rows_, fit_;
     brkga_engine* e_ = nullptr;
     int n_ = 0;
     Individual<T> best_;

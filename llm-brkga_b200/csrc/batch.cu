@@ -337,6 +337,8 @@ static int32_t make_member(std::shared_ptr<ProblemData> pd, const brkga_params& 
         return fail(BRKGA_ERR_UNSUPPORTED, "local search runs in brkga_create engines, not in batches or the server");
     if (pd->kind == BRKGA_MOVRP)
         return fail(BRKGA_ERR_UNSUPPORTED, "MO-VRP runs in brkga_create engines, not in batches or the server");
+    if (pd->kind == BRKGA_EXTERNAL)
+        return fail(BRKGA_ERR_UNSUPPORTED, "external-fitness problems run in brkga_create engines");
     if (row_needs_global(pd->n, points_of(*pd), pd->kind))
         return fail(BRKGA_ERR_UNSUPPORTED, "batched and served rows must fit the shared-memory row kernel (n = " +
                                                std::to_string(pd->n) + " does not); solve it with brkga_create");
@@ -806,6 +808,8 @@ int32_t brkga_server_submit(brkga_server* s, const brkga_problem_desc* desc, con
     if (params->num_islands > 1) return fail(BRKGA_ERR_UNSUPPORTED, "served requests run one population each");
     if (desc->kind == BRKGA_MOVRP)
         return fail(BRKGA_ERR_UNSUPPORTED, "MO-VRP runs in brkga_create engines, not in batches or the server");
+    if (desc->kind == BRKGA_EXTERNAL)
+        return fail(BRKGA_ERR_UNSUPPORTED, "external-fitness problems run in brkga_create engines");
     const long long genes = (desc->kind == BRKGA_TSPJ) ? 2ll * desc->n : (long long)desc->n;
     if (desc->n < 1 || genes > row_max_n()) return fail(BRKGA_ERR_UNSUPPORTED, "chromosome length out of range");
     {

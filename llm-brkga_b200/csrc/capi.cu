@@ -148,6 +148,11 @@ int32_t make_problem(const brkga_problem_desc* d, int device, std::shared_ptr<Pr
         pd->lo = d->lower;
         pd->hi = d->upper;
         break;
+    case BRKGA_EXTERNAL:
+        // a config with its own fitness (core/config.hpp:33-53): no instance data on the device
+        pd->m = 1;
+        pd->maximize = d->maximize ? 1 : 0;
+        break;
     case BRKGA_MOVRP: {
         // MultiObjectiveVRPConfig (configs/multi_objective_vrp_config.hpp:78-165): the depot and n
         // customers; integer demands and capacity; two objectives
@@ -374,6 +379,8 @@ int32_t brkga_evaluate_population(brkga_problem* pb, const float* d_population, 
                                   void* stream) {
     if (!pb || !d_population || !d_fitness) return fail(BRKGA_ERR_INVALID, "null argument");
     const ProblemData& pd = *pb->d;
+    if (pd.kind == BRKGA_EXTERNAL)
+        return fail(BRKGA_ERR_UNSUPPORTED, "an external-fitness problem is evaluated by its caller");
     if (chrom_len != pd.n)
         return fail(BRKGA_ERR_INVALID, "chrom_len " + std::to_string(chrom_len) + " != problem size " +
                                            std::to_string(pd.n));
@@ -430,6 +437,8 @@ int32_t brkga_generation_step(brkga_problem* pb, const float* d_pop, const float
     if (!pb || !d_pop || !d_fitness || !d_sorted || !d_next || !d_next_fitness)
         return fail(BRKGA_ERR_INVALID, "null argument");
     const ProblemData& pd = *pb->d;
+    if (pd.kind == BRKGA_EXTERNAL)
+        return fail(BRKGA_ERR_UNSUPPORTED, "an external-fitness problem is evaluated by its caller");
     if (pd.m != 1) return fail(BRKGA_ERR_INVALID, "generation step is single-objective");
     if (P <= 0 || E <= 0 || M < 0 || E + M > P) return fail(BRKGA_ERR_INVALID, "need P > 0, E > 0, E + M <= P");
     if (!(elite_prob >= 0.0 && elite_prob <= 1.0)) return fail(BRKGA_ERR_INVALID, "elite_prob outside [0,1]");
@@ -468,6 +477,8 @@ int32_t brkga_local_search(brkga_problem* pb, float* d_pop, float* d_fitness, in
                            int32_t island, void* stream) {
     if (!pb || !d_pop || !d_fitness) return fail(BRKGA_ERR_INVALID, "null argument");
     const ProblemData& pd = *pb->d;
+    if (pd.kind == BRKGA_EXTERNAL)
+        return fail(BRKGA_ERR_UNSUPPORTED, "an external-fitness problem is evaluated by its caller");
     if (pd.kind != BRKGA_TSPJ) return fail(BRKGA_ERR_UNSUPPORTED, "local search is defined for TSPJ problems");
     if (chrom_len != pd.n)
         return fail(BRKGA_ERR_INVALID, "chrom_len " + std::to_string(chrom_len) + " != problem size " +
@@ -505,6 +516,8 @@ int32_t brkga_init_population(brkga_problem* pb, float* d_pop, float* d_fitness,
                               uint64_t seed, int32_t island, void* stream) {
     if (!pb || !d_pop || !d_fitness) return fail(BRKGA_ERR_INVALID, "null argument");
     const ProblemData& pd = *pb->d;
+    if (pd.kind == BRKGA_EXTERNAL)
+        return fail(BRKGA_ERR_UNSUPPORTED, "an external-fitness problem is evaluated by its caller");
     if (P <= 0) return fail(BRKGA_ERR_INVALID, "P must be > 0");
     if (ld <= 0) ld = round_up(pd.n, 4);
     if (ld % 4 != 0 || ld < pd.n) return fail(BRKGA_ERR_INVALID, "ld must be a multiple of 4 and >= n");

@@ -22,6 +22,7 @@ enum Kind : int32_t {
     JOBSCHED = 8,
     CONTINUOUS = 9,
     MOVRP = 10,  // xy = depot + customers, w = demands, capi = vehicle capacity, machines = vehicles
+    EXTERNAL = 11,  // fitness from the caller: rows are built, never evaluated on the device
 };
 
 enum Function : int32_t { FN_SPHERE = 0, FN_RASTRIGIN = 1, FN_ROSENBROCK = 2 };

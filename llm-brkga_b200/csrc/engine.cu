@@ -117,6 +117,13 @@ struct brkga_engine {
     // (a migration for islands, the diversity pass for NSGA-II)
     cudaGraphExec_t gx_run[kMaxRunLog + 1] = {};
     cudaGraphExec_t gx_special = nullptr;
+    // external fitness (BRKGA_EXTERNAL): rows pending the caller's fitness (0 none, 1 the
+    // initial population, 2 a generation), the buffer holding the ranked population, and
+    // the packed [P][n] copy of the keys for callers that want dense rows
+    bool external = false;
+    int ext_state = 0;
+    int ext_cur = 0;
+    float* ext_dense = nullptr;
     int32_t* d_perm = nullptr;
     float* d_tmpfit = nullptr;
     NsgaState nsga;
@@ -265,10 +272,13 @@ int32_t brkga_create(brkga_problem* pbh, const brkga_params* params, brkga_engin
     Shape sh;
     int32_t st = make_shape(*pd, *params, &sh);
     if (st != BRKGA_OK) return st;
+    if (pd->kind == BRKGA_EXTERNAL && sh.k > 1)
+        return fail(BRKGA_ERR_UNSUPPORTED, "external-fitness engines run one population (no islands)");
     DeviceGuard g(pd->device);
     if (!g.ok()) return fail(BRKGA_ERR_CUDA, "cannot select device");
     auto* e = new brkga_engine;
     e->device = pd->device;
+    e->external = pd->kind == BRKGA_EXTERNAL;
     e->pop.pd = pd;
     e->pop.prm = *params;
     e->pop.sh = sh;
@@ -441,6 +451,13 @@ int32_t brkga_initialize(brkga_engine* e) {
     if (!e) return fail(BRKGA_ERR_INVALID, "null engine");
     std::lock_guard<std::mutex> lk(e->mu);
     DeviceGuard g(e->device);
+    if (e->external) {
+        // the next brkga_external_begin builds a new initial population
+        e->initialized = false;
+        e->ext_state = 0;
+        e->gen = 0;
+        return BRKGA_OK;
+    }
     const Shape& sh = e->pop.sh;
     // reset generation counters / buffer index on the device
     for (auto& d : e->hd) {
@@ -468,6 +485,8 @@ int32_t brkga_initialize(brkga_engine* e) {
 int32_t brkga_evolve(brkga_engine* e, int32_t generations) {
     if (!e) return fail(BRKGA_ERR_INVALID, "null engine");
     if (generations < 0) return fail(BRKGA_ERR_INVALID, "negative generation count");
+    if (e->external)
+        return fail(BRKGA_ERR_UNSUPPORTED, "external-fitness engine: use brkga_external_begin / _commit");
     if (!e->initialized) {
         int32_t st = brkga_initialize(e);
         if (st != BRKGA_OK) return st;
@@ -514,6 +533,8 @@ int32_t brkga_synchronize(brkga_engine* e) {
 
 int32_t brkga_run(brkga_engine* e) {
     if (!e) return fail(BRKGA_ERR_INVALID, "null engine");
+    if (e->external)
+        return fail(BRKGA_ERR_UNSUPPORTED, "external-fitness engine: use brkga_external_begin / _commit");
     int32_t st = brkga_initialize(e);
     if (st != BRKGA_OK) return st;
     st = brkga_evolve(e, e->pop.prm.max_generations);
@@ -541,6 +562,8 @@ int32_t brkga_get_stream(brkga_engine* e, void** stream) {
 int32_t brkga_get_population(brkga_engine* e, float* keys, float* fitness) {
     if (!e) return fail(BRKGA_ERR_INVALID, "null engine");
     std::lock_guard<std::mutex> lk(e->mu);
+    if (e->external && (e->ext_state != 0 || !e->initialized))
+        return fail(BRKGA_ERR_INVALID, "no ranked population yet: commit the pending rows first");
     DeviceGuard g(e->device);
     if (e->pop.sh.mo) return nsga_get_population(e->nsga, e->stream, keys, fitness);
     int32_t st = sync_descs_to_host(e);
@@ -566,6 +589,7 @@ int32_t brkga_get_population(brkga_engine* e, float* keys, float* fitness) {
 
 int32_t brkga_set_population(brkga_engine* e, const float* keys) {
     if (!e || !keys) return fail(BRKGA_ERR_INVALID, "null argument");
+    if (e->external) return fail(BRKGA_ERR_UNSUPPORTED, "the engine cannot evaluate an external-fitness population");
     std::lock_guard<std::mutex> lk(e->mu);
     DeviceGuard g(e->device);
     if (e->pop.sh.mo) {
@@ -598,7 +622,10 @@ int32_t brkga_set_population(brkga_engine* e, const float* keys) {
 
 int32_t brkga_get_best(brkga_engine* e, float* keys, int32_t* perm, float* fitness) {
     if (!e) return fail(BRKGA_ERR_INVALID, "null engine");
+    if (e->external && perm) return fail(BRKGA_ERR_UNSUPPORTED, "an external-fitness problem is not decoded here");
     std::lock_guard<std::mutex> lk(e->mu);
+    if (e->external && (e->ext_state != 0 || !e->initialized))
+        return fail(BRKGA_ERR_INVALID, "no ranked population yet: commit the pending rows first");
     DeviceGuard g(e->device);
     if (e->pop.sh.mo) return nsga_get_best(e->nsga, e->stream, keys, perm, fitness);
     int32_t st = sync_descs_to_host(e);
@@ -684,6 +711,119 @@ int32_t brkga_get_pareto_front(brkga_engine* e, float* objectives, float* keys, 
     DeviceGuard g(e->device);
     if (!e->pop.sh.mo) return fail(BRKGA_ERR_INVALID, "not a multi-objective problem");
     return nsga_get_front(e->nsga, e->stream, objectives, keys, cap, count);
+}
+
+// ---- external fitness --------------------------------------------------------------------
+// The rows are built by the global-memory row kernel, which stores them without evaluating
+// an external problem (elite copies keep their fitness); the caller fills the fitness of
+// rows [first, P); the commit is the rank kernel: initially on the current buffer, then
+// with the buffer swap and generation advance of an ordinary generation.
+int32_t brkga_external_begin(brkga_engine* e, int32_t dense, float** d_keys, float** d_fitness, int32_t* ld,
+                             int32_t* first) {
+    if (!e || !d_keys || !d_fitness || !ld || !first) return fail(BRKGA_ERR_INVALID, "null argument");
+    if (!e->external) return fail(BRKGA_ERR_INVALID, "not an external-fitness engine");
+    std::lock_guard<std::mutex> lk(e->mu);
+    DeviceGuard g(e->device);
+    if (e->ext_state != 0) return fail(BRKGA_ERR_INVALID, "rows are pending: call brkga_external_commit first");
+    const Shape& sh = e->pop.sh;
+    cudaError_t err = cudaSuccess;
+    int buf = 0, from = 0;
+    if (!e->initialized) {
+        // Population::initialize (core/population.hpp:107-124)
+        for (auto& d : e->hd) {
+            d.cur = 0;
+            d.gen = 0;
+        }
+        err = cudaMemcpyAsync(e->dd, e->hd.data(), sizeof(PopDesc) * e->hd.size(), cudaMemcpyHostToDevice, e->stream);
+        RowLaunch L = base_launch(e, MODE_INIT);
+        L.ntasks = e->nt_all;
+        if (err == cudaSuccess) err = launch_rows(L, e->pop.pd->kind, e->tile, e->grid, e->stream);
+        e->ext_cur = 0;
+        e->gen = 0;
+        buf = 0;
+        from = 0;
+    } else {
+        int32_t st = grow_history(e, (int)e->gen + 2);
+        if (st != BRKGA_OK) return st;
+        RowLaunch L = base_launch(e, MODE_GEN);
+        L.ntasks = e->nt_gen;
+        err = launch_rows(L, e->pop.pd->kind, e->tile, e->grid, e->stream);
+        buf = e->ext_cur ^ 1;
+        from = sh.Ei;
+    }
+    float* keys = e->pop.keys[buf];
+    int stride = sh.ld;
+    if (err == cudaSuccess && dense && sh.ld != sh.n) {
+        if (!e->ext_dense) {
+            void* p = nullptr;
+            int32_t st = dalloc(e->pop, &p, (size_t)sh.Pi * sh.n * 4);
+            if (st != BRKGA_OK) return st;
+            e->ext_dense = (float*)p;
+        }
+        err = cudaMemcpy2DAsync(e->ext_dense, (size_t)sh.n * 4, keys, (size_t)sh.ld * 4, (size_t)sh.n * 4,
+                                (size_t)sh.Pi, cudaMemcpyDeviceToDevice, e->stream);
+        keys = e->ext_dense;
+        stride = sh.n;
+    }
+    if (err == cudaSuccess) err = cudaStreamSynchronize(e->stream);
+    if (err != cudaSuccess) return cuda_fail(err, "external rows");
+    e->ext_state = e->initialized ? 2 : 1;
+    *d_keys = keys;
+    *d_fitness = e->pop.fit[buf];
+    *ld = stride;
+    *first = from;
+    return BRKGA_OK;
+}
+
+int32_t brkga_external_get_rows(brkga_engine* e, float* keys) {
+    if (!e || !keys) return fail(BRKGA_ERR_INVALID, "null argument");
+    std::lock_guard<std::mutex> lk(e->mu);
+    DeviceGuard g(e->device);
+    if (!e->external || e->ext_state == 0) return fail(BRKGA_ERR_INVALID, "no rows pending");
+    const Shape& sh = e->pop.sh;
+    const int buf = (e->ext_state == 1) ? 0 : (e->ext_cur ^ 1);
+    const int from = (e->ext_state == 1) ? 0 : sh.Ei;
+    cudaError_t err = cudaMemcpy2D(keys, (size_t)sh.n * 4, e->pop.keys[buf] + (size_t)from * sh.ld,
+                                   (size_t)sh.ld * 4, (size_t)sh.n * 4, (size_t)(sh.Pi - from), cudaMemcpyDeviceToHost);
+    if (err != cudaSuccess) return cuda_fail(err, "external rows read-back");
+    return BRKGA_OK;
+}
+
+int32_t brkga_external_set_fitness(brkga_engine* e, const float* fitness) {
+    if (!e || !fitness) return fail(BRKGA_ERR_INVALID, "null argument");
+    std::lock_guard<std::mutex> lk(e->mu);
+    DeviceGuard g(e->device);
+    if (!e->external || e->ext_state == 0) return fail(BRKGA_ERR_INVALID, "no rows pending");
+    const Shape& sh = e->pop.sh;
+    const int buf = (e->ext_state == 1) ? 0 : (e->ext_cur ^ 1);
+    const int from = (e->ext_state == 1) ? 0 : sh.Ei;
+    cudaError_t err = cudaMemcpy(e->pop.fit[buf] + from, fitness, (size_t)(sh.Pi - from) * 4, cudaMemcpyHostToDevice);
+    if (err != cudaSuccess) return cuda_fail(err, "external fitness upload");
+    return BRKGA_OK;
+}
+
+int32_t brkga_external_commit(brkga_engine* e) {
+    if (!e) return fail(BRKGA_ERR_INVALID, "null engine");
+    std::lock_guard<std::mutex> lk(e->mu);
+    DeviceGuard g(e->device);
+    if (!e->external || e->ext_state == 0) return fail(BRKGA_ERR_INVALID, "no rows pending");
+    const Shape& sh = e->pop.sh;
+    // fitness the caller's own kernels wrote, on any stream, is in place before the ranking
+    cudaError_t err = cudaDeviceSynchronize();
+    if (err != cudaSuccess) return cuda_fail(err, "external fitness");
+    const bool initial = e->ext_state == 1;
+    err = launch_sort_pops(e->dd, sh.k, sh.Pi, initial ? 0 : 1, e->stream);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(e->stream);
+    if (err != cudaSuccess) return cuda_fail(err, "external commit");
+    if (initial) {
+        e->initialized = true;
+        e->gen = 0;
+    } else {
+        e->ext_cur ^= 1;
+        ++e->gen;
+    }
+    e->ext_state = 0;
+    return BRKGA_OK;
 }
 
 }  // extern "C"

@@ -1046,6 +1046,7 @@ __global__ void __launch_bounds__(kBigBlock) row_kernel_big(RowLaunch L) {
             row = dst + (size_t)r * ld;
         }
         __syncthreads();  // the row's keys are visible to the whole block
+        if (sd.kind == EXTERNAL) continue;  // the caller computes the fitness
 
         float res[2] = {0.0f, 0.0f};
         const int kind = sd.kind;
@@ -1624,6 +1625,9 @@ int row_max_n() { return 4 * 1024 * 4; }
 int row_max_n_global() { return 1 << 22; }
 
 bool row_needs_global(int n, int pts, int kind) {
+    // rows of an external-fitness problem are only built: the global kernel builds them
+    // without a sort buffer in shared memory
+    if (kind == EXTERNAL) return true;
     if (n > row_max_n()) return true;
     const RowTile t = pick_tile(n);
     return row_smem_bytes(t, n, pts, kind, false) > kRowSmemCap;
