@@ -260,7 +260,7 @@ int32_t brkga_get_pareto_front(brkga_engine* e, float* objectives, float* keys, 
 /* ---- external fitness (BRKGA_EXTERNAL engines) -------------------------------------------
  * One generation of Solver::evolve_generation (core/solver.hpp:234-273) with the fitness
  * from the caller, as the reference evaluates a config's fitness_function or its own
- * evaluate_population_gpu (core/population.hpp:567-595, core/config.hpp:50-53):
+ * evaluate_population_gpu (core/population.hpp:523-527, 567-595, 626-652; core/config.hpp:50-53):
  *   brkga_external_begin   builds the rows on the device (the initial population on the
  *                          first call, and on the first call after brkga_initialize; the
  *                          next generation's rows after that), waits for them and returns the device

@@ -936,7 +936,8 @@ public:
 private:
     // one generation (the initial population first) with the config's own fitness: its
     // evaluate_population_gpu on dense device rows, or its fitness_function on each row
-    // (core/population.hpp:567-595; elite rows keep their fitness)
+    // (Population::evaluate_all, core/population.hpp:523-527, 567-595, 626-652; elite rows keep
+    // their fitness)
     void external_generation() {
         float* dk = nullptr;
         float* df = nullptr;
