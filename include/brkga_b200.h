@@ -53,9 +53,10 @@ typedef enum {
                                     objectives total distance and longest route, with the reference's
                                     overload and fleet penalties (configs/multi_objective_vrp_config.hpp:
                                     214-313); two objectives, so runs take the NSGA-II path            */
-    BRKGA_EXTERNAL = 11          /* a config that brings its own fitness (BRKGAConfig::fitness_function, or
-                                    its own evaluate_population_gpu kernel; core/config.hpp:33-53): n
-                                    keys per row, one objective, direction from `maximize`.  The engine
+    BRKGA_EXTERNAL = 11          /* a config that brings its own fitness (BRKGAConfig::fitness_function /
+                                    objective_functions, or its own evaluate_population_gpu kernel;
+                                    core/config.hpp:33-53): n keys per row; one objective (BRKGA,
+                                    direction from `maximize`) or two (NSGA-II, minimised).  The engine
                                     builds rows and ranks them; the caller evaluates them between
                                     brkga_external_begin and brkga_external_commit.  Engines only (one
                                     island); the evaluation entry points, batches and the server
@@ -99,6 +100,7 @@ typedef struct {
     int32_t maximize;            /* BRKGA_EXTERNAL: 1 = larger fitness is better (the
                                     reference's comparator, core/config.hpp:36); other kinds
                                     fix their own direction and ignore it                     */
+    int32_t num_objectives;      /* BRKGA_EXTERNAL: 1 (0 reads as 1) or 2                     */
 } brkga_problem_desc;
 
 /* GA parameters (BRKGAConfig fields, core/config.hpp:17-30, plus the engine's own). */
@@ -258,29 +260,37 @@ int32_t brkga_set_population(brkga_engine* e, const float* keys);
 int32_t brkga_get_pareto_front(brkga_engine* e, float* objectives, float* keys, int32_t cap, int32_t* count);
 
 /* ---- external fitness (BRKGA_EXTERNAL engines) -------------------------------------------
- * One generation of Solver::evolve_generation (core/solver.hpp:234-273) with the fitness
- * from the caller, as the reference evaluates a config's fitness_function or its own
- * evaluate_population_gpu (core/population.hpp:523-527, 567-595, 626-652; core/config.hpp:50-53):
- *   brkga_external_begin   builds the rows on the device (the initial population on the
- *                          first call, and on the first call after brkga_initialize; the
- *                          next generation's rows after that), waits for them and returns the device
- *                          buffers: *d_keys rows of *ld floats, *d_fitness one float per
- *                          row.  Rows [*first, P) need a fitness: all rows at
- *                          initialisation, the non-elite rows of a generation (elite rows
- *                          keep theirs, as the reference's evaluated flag does).  With
- *                          dense = 1 the keys are a packed [P][n] copy (*ld = n), the
- *                          layout evaluate_population_gpu expects.
- *   brkga_external_get_rows  the pending rows [first, P) into host keys [P - first][n].
- *   brkga_external_set_fitness  host fitness [P - first] for those rows.
+ * One generation of Solver::evolve_generation (core/solver.hpp:234-273, 751-817) with the
+ * fitness from the caller, as the reference evaluates a config's fitness_function /
+ * objective_functions or its own evaluate_population_gpu (core/population.hpp:523-527,
+ * 567-595, 626-652; core/config.hpp:50-53):
+ *   brkga_external_begin   builds the rows that need a fitness on the device and waits
+ *                          for them: the initial population on the first call (and on the
+ *                          first call after brkga_initialize), then each generation's new
+ *                          rows -- the non-elite rows of a BRKGA generation (elite rows
+ *                          keep theirs, as the reference's evaluated flag does), the P
+ *                          offspring of an NSGA-II generation.  *d_keys points at the first
+ *                          of *count pending rows, *ld floats apart; *d_fitness at their
+ *                          fitness, num_objectives floats per row; *first is the first
+ *                          row's index in the engine's buffer.  With dense = 1 the keys are
+ *                          a packed [count][n] copy (*ld = n), the layout
+ *                          evaluate_population_gpu expects.
+ *   brkga_external_get_rows  the pending rows into host keys [count][n].
+ *   brkga_external_set_fitness  host fitness [count][num_objectives] for them.
  *   brkga_external_commit  waits for the device (so fitness that the caller's kernels
- *                          wrote on any stream is in place), ranks the population (elite
- *                          partition, best-fitness history) and completes the generation;
- *                          waits for the engine.  On these engines brkga_initialize only restarts (the next
- * begin builds a new initial population); brkga_evolve, brkga_run and
- * brkga_set_population return BRKGA_ERR_UNSUPPORTED; brkga_get_best gives keys and
- * fitness, not a permutation (the engine does not decode an external problem). */
+ *                          wrote on any stream is in place), ranks the population and
+ *                          completes the generation.  NSGA-II: when the generation's
+ *                          diversity pass (ensure_minimum_diversity, core/population.hpp:
+ *                          130-182) replaced rows with fresh keys, it returns
+ *                          BRKGA_ERR_NOT_READY instead: the next brkga_external_begin
+ *                          returns those rows, and the commit after them completes the
+ *                          generation.
+ * On these engines brkga_initialize only restarts (the next begin builds a new initial
+ * population); brkga_evolve, brkga_run and brkga_set_population return
+ * BRKGA_ERR_UNSUPPORTED; brkga_get_best gives keys and fitness, not a permutation (the
+ * engine does not decode an external problem). */
 int32_t brkga_external_begin(brkga_engine* e, int32_t dense, float** d_keys, float** d_fitness, int32_t* ld,
-                             int32_t* first);
+                             int32_t* first, int32_t* count);
 int32_t brkga_external_get_rows(brkga_engine* e, float* keys);
 int32_t brkga_external_set_fitness(brkga_engine* e, const float* fitness);
 int32_t brkga_external_commit(brkga_engine* e);

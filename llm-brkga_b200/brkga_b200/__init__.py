@@ -43,7 +43,7 @@ class ProblemDesc(C.Structure):
                 ("values", C.c_void_p), ("capacity", C.c_float), ("job_times", C.c_void_p),
                 ("machines", C.c_int32), ("function", C.c_int32), ("lower", C.c_float), ("upper", C.c_float),
                 ("demands", C.c_void_p), ("vehicle_capacity", C.c_int32), ("vehicles", C.c_int32),
-                ("maximize", C.c_int32)]
+                ("maximize", C.c_int32), ("num_objectives", C.c_int32)]
 
 
 class Params(C.Structure):
@@ -111,7 +111,7 @@ def lib():
         "brkga_set_population": (_i32, [_vp, _vp]),
         "brkga_get_pareto_front": (_i32, [_vp, _vp, _vp, _i32, C.POINTER(_i32)]),
         "brkga_external_begin": (_i32, [_vp, _i32, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_i32),
-                                        C.POINTER(_i32)]),
+                                        C.POINTER(_i32), C.POINTER(_i32)]),
         "brkga_external_get_rows": (_i32, [_vp, _vp]),
         "brkga_external_set_fitness": (_i32, [_vp, _vp]),
         "brkga_external_commit": (_i32, [_vp]),
@@ -176,7 +176,7 @@ class Problem:
 
     def __init__(self, kind, n, coords=None, coords2=None, matrix=None, matrix2=None, weights=None, values=None,
                  capacity=0.0, device=0, job_times=None, machines=0, function=0, lower=0.0, upper=0.0,
-                 demands=None, vehicle_capacity=0, vehicles=0, maximize=False):
+                 demands=None, vehicle_capacity=0, vehicles=0, maximize=False, num_objectives=1):
         keep = []
 
         def arr(a, dt):
@@ -189,7 +189,8 @@ class Problem:
         d = ProblemDesc(kind, n, arr(coords, np.float32), arr(coords2, np.float32), arr(matrix, np.float32),
                         arr(matrix2, np.float32), arr(weights, np.int32), arr(values, np.int32), float(capacity),
                         arr(job_times, np.float32), int(machines), int(function), float(lower), float(upper),
-                        arr(demands, np.int32), int(vehicle_capacity), int(vehicles), int(bool(maximize)))
+                        arr(demands, np.int32), int(vehicle_capacity), int(vehicles), int(bool(maximize)),
+                        int(num_objectives))
         h = C.c_void_p()
         check(lib().brkga_problem_create(C.byref(d), device, C.byref(h)))
         # n is the chromosome length (genes); a TSPJ instance of c cities has 2c genes
@@ -273,10 +274,11 @@ def movrp(coords, demands, vehicle_capacity, vehicles, device=0):
                    vehicles=vehicles, device=device)
 
 
-def external(n, maximize=False, device=0):
+def external(n, maximize=False, num_objectives=1, device=0):
     """A problem whose fitness the caller computes (a BRKGAConfig with its own
-    fitness_function, core/config.hpp:33-53): n keys per row, one objective."""
-    return Problem(EXTERNAL, n, device=device, maximize=maximize)
+    fitness_function / objective_functions, core/config.hpp:33-53): n keys per row; one
+    objective (BRKGA) or two (NSGA-II, minimised)."""
+    return Problem(EXTERNAL, n, device=device, maximize=maximize, num_objectives=num_objectives)
 
 
 def movrp_routes(perm, demands, vehicle_capacity):
@@ -372,41 +374,51 @@ class Solver:
         fit = np.zeros(2, np.float32)
         if self.problem.kind == EXTERNAL:  # not decoded by the engine
             check(lib().brkga_get_best(self.h, _ptr(keys), None, _ptr(fit)))
-            return keys, None, fit[0]
+            return keys, None, (fit[0] if self.m == 1 else fit[:2].copy())
         perm = np.zeros(self.n, np.int32)
         check(lib().brkga_get_best(self.h, _ptr(keys), _ptr(perm), _ptr(fit)))
         return keys, perm, (fit[0] if self.m == 1 else fit[:2].copy())
 
     # external fitness (Problem of kind EXTERNAL): the engine builds and ranks the rows, the
-    # caller evaluates rows [first, P) between begin and commit
+    # caller evaluates the pending rows between begin and commit
     def external_begin(self, dense=False):
-        """(keys address, fitness address, row stride in floats, first row to evaluate)"""
-        k, f, ld, first = C.c_void_p(), C.c_void_p(), C.c_int32(), C.c_int32()
+        """(address of the first pending row's keys, address of its fitness, row stride in
+        floats, its row index, number of pending rows)"""
+        k, f, ld, first, cnt = C.c_void_p(), C.c_void_p(), C.c_int32(), C.c_int32(), C.c_int32()
         check(lib().brkga_external_begin(self.h, int(bool(dense)), C.byref(k), C.byref(f), C.byref(ld),
-                                         C.byref(first)))
-        self._ext_first = first.value
-        return k.value, f.value, ld.value, first.value
+                                         C.byref(first), C.byref(cnt)))
+        self._ext_count = cnt.value
+        return k.value, f.value, ld.value, first.value, cnt.value
 
     def external_rows(self):
-        keys = np.zeros((self.prm.population_size - self._ext_first, self.n), np.float32)
+        keys = np.zeros((self._ext_count, self.n), np.float32)
         check(lib().brkga_external_get_rows(self.h, _ptr(keys)))
         return keys
 
     def external_set_fitness(self, fitness):
         fitness = np.ascontiguousarray(fitness, np.float32)
-        if fitness.shape != (self.prm.population_size - self._ext_first,):
-            raise ValueError(f"need {self.prm.population_size - self._ext_first} fitness values")
+        want = (self._ext_count,) if self.m == 1 else (self._ext_count, self.m)
+        if fitness.shape != want:
+            raise ValueError(f"need fitness of shape {want}")
         check(lib().brkga_external_set_fitness(self.h, _ptr(fitness)))
 
     def external_commit(self):
-        check(lib().brkga_external_commit(self.h))
+        """True when the generation is complete; False when an NSGA-II diversity pass left
+        refill rows that need fitness (call external_begin again)"""
+        rc = lib().brkga_external_commit(self.h)
+        if rc == -8:
+            return False
+        check(rc)
+        return True
 
     def external_step(self, fitness_of_rows):
         """one generation (the initial population on the first call): fitness_of_rows maps
-        keys [rows][n] (numpy) to their fitness [rows]"""
-        self.external_begin()
-        self.external_set_fitness(fitness_of_rows(self.external_rows()))
-        self.external_commit()
+        keys [rows][n] (numpy) to their fitness [rows] (or [rows][2])"""
+        while True:
+            self.external_begin()
+            self.external_set_fitness(fitness_of_rows(self.external_rows()))
+            if self.external_commit():
+                return
 
     def get_fitness_history(self):
         cap = self.generation + 1

@@ -801,16 +801,22 @@ public:
         brkga_problem* pb = config_->problem_handle();
         if (!pb) {
             // a config with its own fitness: the engine's external-fitness path
-            if (config_->num_objectives > 1)
-                throw std::runtime_error("a multi-objective config needs a device problem (host objective_functions "
-                                         "are not evaluated by this engine)");
-            if (!config_->fitness_function && !config_->has_gpu_evaluation())
-                throw std::runtime_error("config has neither a fitness_function nor GPU evaluation");
+            const bool mo = config_->num_objectives > 1;
+            if (config_->num_objectives > 2)
+                throw std::runtime_error("external-fitness configs have one or two objectives");
+            if (!config_->has_gpu_evaluation()) {
+                if (!mo && !config_->fitness_function) throw std::runtime_error("Fitness function not set");
+                if (mo && ((int)config_->objective_functions.size() < 2 || !config_->objective_functions[0] ||
+                           !config_->objective_functions[1]))
+                    throw std::runtime_error("Multi-objective mode but no objective functions defined");
+            }
             brkga_problem_desc d{};
             d.kind = BRKGA_EXTERNAL;
             d.n = n_;
-            // the reference's comparator says which fitness is better (core/config.hpp:36)
-            d.maximize = (config_->comparator && config_->comparator(T(1), T(0))) ? 1 : 0;
+            d.num_objectives = mo ? 2 : 1;
+            // the reference's comparator says which fitness is better (core/config.hpp:36);
+            // objectives are minimised (Individual::dominates)
+            d.maximize = (!mo && config_->comparator && config_->comparator(T(1), T(0))) ? 1 : 0;
             brkga_b200_detail::check(brkga_problem_create(&d, config_->device, &ext_pb_), "Solver");
             pb = ext_pb_;
         }
@@ -935,37 +941,45 @@ public:
 
 private:
     // one generation (the initial population first) with the config's own fitness: its
-    // evaluate_population_gpu on dense device rows, or its fitness_function on each row
-    // (Population::evaluate_all, core/population.hpp:523-527, 567-595, 626-652; elite rows keep
-    // their fitness)
+    // evaluate_population_gpu on dense device rows, or its fitness_function /
+    // objective_functions on each row (Population::evaluate_all, core/population.hpp:523-527,
+    // 567-595, 626-652); BRKGA elite rows keep their fitness.  An NSGA-II generation whose
+    // diversity pass replaced rows asks for those too (BRKGA_ERR_NOT_READY).
     void external_generation() {
-        float* dk = nullptr;
-        float* df = nullptr;
-        int32_t ld = 0, first = 0;
         const bool gpu = config_->has_gpu_evaluation();
-        brkga_b200_detail::check(brkga_external_begin(e_, gpu ? 1 : 0, &dk, &df, &ld, &first), "evolve_generation");
-        const int count = config_->population_size - first;
-        if (gpu) {
-            config_->evaluate_population_gpu(reinterpret_cast<T*>(dk + (size_t)first * ld),
-                                             reinterpret_cast<T*>(df + first), count, n_);
-        } else {
-            rows_.resize((size_t)count * n_);
-            fit_.resize((size_t)count);
-            brkga_b200_detail::check(brkga_external_get_rows(e_, rows_.data()), "evolve_generation");
-            Individual<T> ind(config_->component_lengths, 0);
-            for (int i = 0; i < count; ++i) {
-                size_t off = (size_t)i * n_;
-                for (size_t c = 0; c < ind.chromosomes.size(); ++c) {
-                    const size_t len = (size_t)config_->component_lengths[c];
-                    ind.chromosomes[c].assign(rows_.begin() + off, rows_.begin() + off + len);
-                    off += len;
+        const int m = config_->num_objectives > 1 ? 2 : 1;
+        for (;;) {
+            float* dk = nullptr;
+            float* df = nullptr;
+            int32_t ld = 0, first = 0, count = 0;
+            brkga_b200_detail::check(brkga_external_begin(e_, gpu ? 1 : 0, &dk, &df, &ld, &first, &count),
+                                     "evolve_generation");
+            if (gpu) {
+                if (count > 0) config_->evaluate_population_gpu(reinterpret_cast<T*>(dk), reinterpret_cast<T*>(df), count, n_);
+            } else {
+                rows_.resize((size_t)count * n_);
+                fit_.resize((size_t)count * m);
+                brkga_b200_detail::check(brkga_external_get_rows(e_, rows_.data()), "evolve_generation");
+                Individual<T> ind(config_->component_lengths, m > 1 ? m : 0);
+                for (int i = 0; i < count; ++i) {
+                    size_t off = (size_t)i * n_;
+                    for (size_t c = 0; c < ind.chromosomes.size(); ++c) {
+                        const size_t len = (size_t)config_->component_lengths[c];
+                        ind.chromosomes[c].assign(rows_.begin() + off, rows_.begin() + off + len);
+                        off += len;
+                    }
+                    ind.evaluated = false;
+                    if (m == 1)
+                        fit_[i] = (float)config_->fitness_function(ind);
+                    else
+                        for (int o = 0; o < m; ++o) fit_[(size_t)i * m + o] = (float)config_->objective_functions[o](ind);
                 }
-                ind.evaluated = false;
-                fit_[i] = (float)config_->fitness_function(ind);
+                brkga_b200_detail::check(brkga_external_set_fitness(e_, fit_.data()), "evolve_generation");
             }
-            brkga_b200_detail::check(brkga_external_set_fitness(e_, fit_.data()), "evolve_generation");
+            const int32_t rc = brkga_external_commit(e_);
+            if (rc == BRKGA_OK) return;
+            if (rc != BRKGA_ERR_NOT_READY) brkga_b200_detail::check(rc, "evolve_generation");
         }
-        brkga_b200_detail::check(brkga_external_commit(e_), "evolve_generation");
     }
 
     std::unique_ptr<BRKGAConfig<T>> config_;

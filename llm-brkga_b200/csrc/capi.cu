@@ -150,7 +150,11 @@ int32_t make_problem(const brkga_problem_desc* d, int device, std::shared_ptr<Pr
         break;
     case BRKGA_EXTERNAL:
         // a config with its own fitness (core/config.hpp:33-53): no instance data on the device
-        pd->m = 1;
+        if (d->num_objectives < 0 || d->num_objectives > 2)
+            return fail(BRKGA_ERR_UNSUPPORTED, "external problems have one or two objectives");
+        pd->m = d->num_objectives == 2 ? 2 : 1;
+        if (pd->m == 2 && d->maximize)
+            return fail(BRKGA_ERR_INVALID, "two objectives are minimised (Individual::dominates)");
         pd->maximize = d->maximize ? 1 : 0;
         break;
     case BRKGA_MOVRP: {

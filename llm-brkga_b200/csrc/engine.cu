@@ -118,11 +118,15 @@ struct brkga_engine {
     cudaGraphExec_t gx_run[kMaxRunLog + 1] = {};
     cudaGraphExec_t gx_special = nullptr;
     // external fitness (BRKGA_EXTERNAL): rows pending the caller's fitness (0 none, 1 the
-    // initial population, 2 a generation), the buffer holding the ranked population, and
-    // the packed [P][n] copy of the keys for callers that want dense rows
+    // initial population, 2 a generation's new rows, 3 NSGA-II refill rows after a
+    // diversity rebuild), where they are, the buffer holding the ranked population
+    // (BRKGA), and the packed [P][n] copy of the keys for callers that want dense rows
     bool external = false;
     int ext_state = 0;
     int ext_cur = 0;
+    float* ext_keys = nullptr;
+    float* ext_fit = nullptr;
+    int ext_first = 0, ext_count = 0;
     float* ext_dense = nullptr;
     int32_t* d_perm = nullptr;
     float* d_tmpfit = nullptr;
@@ -716,62 +720,96 @@ int32_t brkga_get_pareto_front(brkga_engine* e, float* objectives, float* keys, 
 // ---- external fitness --------------------------------------------------------------------
 // The rows are built by the global-memory row kernel, which stores them without evaluating
 // an external problem (elite copies keep their fitness); the caller fills the fitness of
-// rows [first, P); the commit is the rank kernel: initially on the current buffer, then
-// with the buffer swap and generation advance of an ordinary generation.
+// the pending rows; the commit is the elite partition (BRKGA: initially on the current
+// buffer, then with the buffer swap and generation advance of an ordinary generation) or
+// the NSGA-II selection, survivor gather and, when due, the diversity pass.
+
+// rows [first, first + count) of keys / fit (m values per row) are pending
+static void ext_pending(brkga_engine* e, int state, float* keys, float* fit, int first, int count) {
+    const Shape& sh = e->pop.sh;
+    const int m = e->pop.pd->m;
+    e->ext_state = state;
+    e->ext_keys = keys + (size_t)first * sh.ld;
+    e->ext_fit = fit + (size_t)first * m;
+    e->ext_first = first;
+    e->ext_count = count;
+}
+
 int32_t brkga_external_begin(brkga_engine* e, int32_t dense, float** d_keys, float** d_fitness, int32_t* ld,
-                             int32_t* first) {
-    if (!e || !d_keys || !d_fitness || !ld || !first) return fail(BRKGA_ERR_INVALID, "null argument");
+                             int32_t* first, int32_t* count) {
+    if (!e || !d_keys || !d_fitness || !ld || !first || !count) return fail(BRKGA_ERR_INVALID, "null argument");
     if (!e->external) return fail(BRKGA_ERR_INVALID, "not an external-fitness engine");
     std::lock_guard<std::mutex> lk(e->mu);
     DeviceGuard g(e->device);
-    if (e->ext_state != 0) return fail(BRKGA_ERR_INVALID, "rows are pending: call brkga_external_commit first");
+    if (e->ext_state != 0 && e->ext_state != 3)
+        return fail(BRKGA_ERR_INVALID, "rows are pending: call brkga_external_commit first");
     const Shape& sh = e->pop.sh;
     cudaError_t err = cudaSuccess;
-    int buf = 0, from = 0;
-    if (!e->initialized) {
+    if (e->ext_state == 3) {
+        // NSGA-II refill rows, built by the commit that reported them
+    } else if (!e->initialized) {
         // Population::initialize (core/population.hpp:107-124)
         for (auto& d : e->hd) {
             d.cur = 0;
             d.gen = 0;
         }
         err = cudaMemcpyAsync(e->dd, e->hd.data(), sizeof(PopDesc) * e->hd.size(), cudaMemcpyHostToDevice, e->stream);
-        RowLaunch L = base_launch(e, MODE_INIT);
-        L.ntasks = e->nt_all;
-        if (err == cudaSuccess) err = launch_rows(L, e->pop.pd->kind, e->tile, e->grid, e->stream);
+        if (err == cudaSuccess) {
+            if (sh.mo) {
+                err = nsga_enqueue_rows(e->nsga, MODE_INIT, e->stream);
+            } else {
+                RowLaunch L = base_launch(e, MODE_INIT);
+                L.ntasks = e->nt_all;
+                err = launch_rows(L, e->pop.pd->kind, e->tile, e->grid, e->stream);
+            }
+        }
         e->ext_cur = 0;
         e->gen = 0;
-        buf = 0;
-        from = 0;
+        ext_pending(e, 1, e->pop.keys[0], e->pop.fit[0], 0, sh.Pi);
+    } else if (sh.mo) {
+        // offspring into pool rows [P, 2P) of the current buffer (core/solver.hpp:1019-1091)
+        int32_t st = grow_history(e, (int)e->gen + 2);
+        if (st == BRKGA_OK) st = sync_descs_to_host(e);
+        if (st != BRKGA_OK) return st;
+        const int cur = e->hd[0].cur;
+        err = nsga_enqueue_rows(e->nsga, MODE_NSGA_OFF, e->stream);
+        ext_pending(e, 2, e->pop.keys[cur], e->pop.fit[cur], sh.Pi, sh.Pi);
     } else {
         int32_t st = grow_history(e, (int)e->gen + 2);
         if (st != BRKGA_OK) return st;
         RowLaunch L = base_launch(e, MODE_GEN);
         L.ntasks = e->nt_gen;
         err = launch_rows(L, e->pop.pd->kind, e->tile, e->grid, e->stream);
-        buf = e->ext_cur ^ 1;
-        from = sh.Ei;
+        const int buf = e->ext_cur ^ 1;
+        ext_pending(e, 2, e->pop.keys[buf], e->pop.fit[buf], sh.Ei, sh.Pi - sh.Ei);
     }
-    float* keys = e->pop.keys[buf];
+    float* keys = e->ext_keys;
     int stride = sh.ld;
-    if (err == cudaSuccess && dense && sh.ld != sh.n) {
+    if (err == cudaSuccess && dense && sh.ld != sh.n && e->ext_count > 0) {
         if (!e->ext_dense) {
             void* p = nullptr;
             int32_t st = dalloc(e->pop, &p, (size_t)sh.Pi * sh.n * 4);
-            if (st != BRKGA_OK) return st;
+            if (st != BRKGA_OK) {
+                e->ext_state = 0;
+                return st;
+            }
             e->ext_dense = (float*)p;
         }
-        err = cudaMemcpy2DAsync(e->ext_dense, (size_t)sh.n * 4, keys, (size_t)sh.ld * 4, (size_t)sh.n * 4,
-                                (size_t)sh.Pi, cudaMemcpyDeviceToDevice, e->stream);
+        err = cudaMemcpy2DAsync(e->ext_dense, (size_t)sh.n * 4, e->ext_keys, (size_t)sh.ld * 4, (size_t)sh.n * 4,
+                                (size_t)e->ext_count, cudaMemcpyDeviceToDevice, e->stream);
         keys = e->ext_dense;
         stride = sh.n;
     }
     if (err == cudaSuccess) err = cudaStreamSynchronize(e->stream);
-    if (err != cudaSuccess) return cuda_fail(err, "external rows");
-    e->ext_state = e->initialized ? 2 : 1;
+    if (err != cudaSuccess) {
+        e->ext_state = 0;
+        return cuda_fail(err, "external rows");
+    }
     *d_keys = keys;
-    *d_fitness = e->pop.fit[buf];
+    *d_fitness = e->ext_fit;
     *ld = stride;
-    *first = from;
+    *first = e->ext_first;
+    *count = e->ext_count;
     return BRKGA_OK;
 }
 
@@ -781,10 +819,9 @@ int32_t brkga_external_get_rows(brkga_engine* e, float* keys) {
     DeviceGuard g(e->device);
     if (!e->external || e->ext_state == 0) return fail(BRKGA_ERR_INVALID, "no rows pending");
     const Shape& sh = e->pop.sh;
-    const int buf = (e->ext_state == 1) ? 0 : (e->ext_cur ^ 1);
-    const int from = (e->ext_state == 1) ? 0 : sh.Ei;
-    cudaError_t err = cudaMemcpy2D(keys, (size_t)sh.n * 4, e->pop.keys[buf] + (size_t)from * sh.ld,
-                                   (size_t)sh.ld * 4, (size_t)sh.n * 4, (size_t)(sh.Pi - from), cudaMemcpyDeviceToHost);
+    if (e->ext_count == 0) return BRKGA_OK;
+    cudaError_t err = cudaMemcpy2D(keys, (size_t)sh.n * 4, e->ext_keys, (size_t)sh.ld * 4, (size_t)sh.n * 4,
+                                   (size_t)e->ext_count, cudaMemcpyDeviceToHost);
     if (err != cudaSuccess) return cuda_fail(err, "external rows read-back");
     return BRKGA_OK;
 }
@@ -794,10 +831,8 @@ int32_t brkga_external_set_fitness(brkga_engine* e, const float* fitness) {
     std::lock_guard<std::mutex> lk(e->mu);
     DeviceGuard g(e->device);
     if (!e->external || e->ext_state == 0) return fail(BRKGA_ERR_INVALID, "no rows pending");
-    const Shape& sh = e->pop.sh;
-    const int buf = (e->ext_state == 1) ? 0 : (e->ext_cur ^ 1);
-    const int from = (e->ext_state == 1) ? 0 : sh.Ei;
-    cudaError_t err = cudaMemcpy(e->pop.fit[buf] + from, fitness, (size_t)(sh.Pi - from) * 4, cudaMemcpyHostToDevice);
+    if (e->ext_count == 0) return BRKGA_OK;
+    cudaError_t err = cudaMemcpy(e->ext_fit, fitness, (size_t)e->ext_count * e->pop.pd->m * 4, cudaMemcpyHostToDevice);
     if (err != cudaSuccess) return cuda_fail(err, "external fitness upload");
     return BRKGA_OK;
 }
@@ -811,18 +846,56 @@ int32_t brkga_external_commit(brkga_engine* e) {
     // fitness the caller's own kernels wrote, on any stream, is in place before the ranking
     cudaError_t err = cudaDeviceSynchronize();
     if (err != cudaSuccess) return cuda_fail(err, "external fitness");
-    const bool initial = e->ext_state == 1;
-    err = launch_sort_pops(e->dd, sh.k, sh.Pi, initial ? 0 : 1, e->stream);
+    const int state = e->ext_state;
+    e->ext_state = 0;
+    if (!sh.mo) {
+        err = launch_sort_pops(e->dd, sh.k, sh.Pi, state == 1 ? 0 : 1, e->stream);
+        if (err == cudaSuccess) err = cudaStreamSynchronize(e->stream);
+        if (err != cudaSuccess) return cuda_fail(err, "external commit");
+        if (state == 1) {
+            e->initialized = true;
+            e->gen = 0;
+        } else {
+            e->ext_cur ^= 1;
+            ++e->gen;
+        }
+        return BRKGA_OK;
+    }
+    // NSGA-II (core/population.hpp:409-517; ensure_minimum_diversity :130-182)
+    if (state == 1) {
+        err = nsga_enqueue_select(e->dd, 1, sh.Pi, 1, e->stream);
+    } else if (state == 3) {
+        err = nsga_enqueue_select(e->dd, 1, sh.Pi, 2, e->stream);  // re-rank the rebuilt population
+    } else {
+        err = nsga_enqueue_select(e->dd, 1, sh.Pi, 0, e->stream);
+        if (err == cudaSuccess) err = nsga_enqueue_gather_finish(e->dd, 1, sh.Pi, sh.ld, e->stream);
+        if (err == cudaSuccess && nsga_diversity_due(e->nsga, e->gen + 1)) {
+            err = nsga_enqueue_diversity(e->dd, 1, sh.Pi, e->stream);
+            int32_t nu = sh.Pi;
+            if (err == cudaSuccess) err = cudaStreamSynchronize(e->stream);
+            if (err == cudaSuccess) err = cudaMemcpy(&nu, e->hd[0].nu, 4, cudaMemcpyDeviceToHost);
+            if (err == cudaSuccess && nu < sh.Pi) {
+                // kept rows were gathered into the other buffer, now current: rows [nu, P)
+                // take fresh keys and need the caller's objectives
+                ++e->gen;
+                int32_t st = sync_descs_to_host(e);
+                if (st != BRKGA_OK) return st;
+                const int cur = e->hd[0].cur;
+                err = nsga_enqueue_rows(e->nsga, MODE_NSGA_REFILL, e->stream);
+                if (err == cudaSuccess) err = cudaStreamSynchronize(e->stream);
+                if (err != cudaSuccess) return cuda_fail(err, "external refill rows");
+                ext_pending(e, 3, e->pop.keys[cur], e->pop.fit[cur], nu, sh.Pi - nu);
+                return fail(BRKGA_ERR_NOT_READY, "diversity refill rows pending: evaluate them and commit again");
+            }
+        }
+        if (err == cudaSuccess) ++e->gen;
+    }
     if (err == cudaSuccess) err = cudaStreamSynchronize(e->stream);
     if (err != cudaSuccess) return cuda_fail(err, "external commit");
-    if (initial) {
+    if (state == 1) {
         e->initialized = true;
         e->gen = 0;
-    } else {
-        e->ext_cur ^= 1;
-        ++e->gen;
     }
-    e->ext_state = 0;
     return BRKGA_OK;
 }
 

@@ -1187,6 +1187,10 @@ static RowLaunch nsga_rows(const NsgaState& s, int mode) {
     return L;
 }
 
+cudaError_t nsga_enqueue_rows(NsgaState& s, int mode, cudaStream_t st) {
+    return launch_rows(nsga_rows(s, mode), s.kind, s.tile, s.grid, st);
+}
+
 cudaError_t nsga_enqueue_init(NsgaState& s, cudaStream_t st) {
     cudaError_t e = launch_rows(nsga_rows(s, MODE_INIT), s.kind, s.tile, s.grid, st);
     if (e != cudaSuccess) return e;

@@ -39,6 +39,8 @@ cudaError_t nsga_enqueue_diversity(PopDesc* dd, int npops, int maxP, cudaStream_
 void nsga_release(NsgaState& s);
 void nsga_set_history(NsgaState& s, float* h, int cap);
 cudaError_t nsga_enqueue_init(NsgaState& s, cudaStream_t st);
+// one row launch of the population in the given mode (MODE_INIT, MODE_NSGA_OFF, ...)
+cudaError_t nsga_enqueue_rows(NsgaState& s, int mode, cudaStream_t st);
 // one generation; with_diversity = false leaves out the diversity pass's launches (they
 // exit at once unless the pass is due after this generation: nsga_diversity_due)
 cudaError_t nsga_enqueue_generation(NsgaState& s, cudaStream_t st, bool with_diversity = true);

@@ -66,16 +66,15 @@ def test_external_device_fitness_dense_rows(cuda, n):
     prm = B().params(P, E, M, 0.7, G, seed=9)
     keys_b, fit_b, _ = _builtin_run(xy, prm, G)
     s = B().Solver(B().external(n), prm)
-    for _ in range(G + 1):
-        kp, fp, ld, first = s.external_begin(dense=True)
-        assert ld == n
-        rows = torch.as_tensor(_Cai(kp, (P, n)), device="cuda")
-        host_rows = s.external_rows()
-        np.testing.assert_array_equal(rows[first:].cpu().numpy(), host_rows)
-        fit = torch.as_tensor(_Cai(fp, (P,)), device="cuda")
-        fit[first:] = torch.from_numpy(O.evaluate(po, rows[first:].cpu().numpy())).cuda()
+    for g in range(G + 1):
+        kp, fp, ld, first, cnt = s.external_begin(dense=True)
+        assert ld == n and (first, cnt) == ((0, P) if g == 0 else (E, P - E))
+        rows = torch.as_tensor(_Cai(kp, (cnt, n)), device="cuda")
+        np.testing.assert_array_equal(rows.cpu().numpy(), s.external_rows())
+        fit = torch.as_tensor(_Cai(fp, (cnt,)), device="cuda")
+        fit[:] = torch.from_numpy(O.evaluate(po, rows.cpu().numpy())).cuda()
         torch.cuda.synchronize()
-        s.external_commit()
+        assert s.external_commit()
     keys_e, fit_e = s.get_population()
     np.testing.assert_array_equal(keys_e, keys_b)
     np.testing.assert_array_equal(fit_e, fit_b)
@@ -105,7 +104,7 @@ def test_external_rejections(cuda):
         assert ei.value.code == -6
     with pytest.raises(B().BrkgaError):  # nothing ranked yet
         s.get_best_individual()
-    s.external_begin()
+    assert s.external_begin()[3:] == (0, 32)
     with pytest.raises(B().BrkgaError) as ei:  # rows already pending
         s.external_begin()
     assert ei.value.code == -1
@@ -132,11 +131,57 @@ def test_external_rejections(cuda):
     assert ei.value.code == -6
     # initialize restarts: the next begin builds a new initial population
     s.initialize()
-    _, _, _, first = s.external_begin()
-    assert first == 0
+    assert s.external_begin()[3:] == (0, 32)
     s.external_set_fitness(np.ones(32, np.float32))
     s.external_commit()
     assert s.generation == 0
+
+
+def _builtin_nsga(a, b, prm, G, per_generation=None):
+    s = B().Solver(B().bitsp(a, b), prm)
+    s.initialize()
+    out = []
+    for _ in range(G):
+        s.evolve(1)
+        if per_generation:
+            out.append(s.get_population())
+    return s, out
+
+
+@pytest.mark.parametrize("n,P,G,div", [(30, 64, 30, 25), (4, 40, 40, 5)])
+def test_external_nsga2_equals_builtin(cuda, n, P, G, div):
+    # two objectives from the host (the oracle's depot tours), NSGA-II on the device; the
+    # tiny instance converges to duplicates, so the diversity pass rebuilds the population
+    # and the commit asks for the refill rows' objectives
+    a, b = I.tsp_coords(n + 1, seed=n), I.tsp_coords(n + 1, seed=n + 1)
+    po = O.OracleProblem(O.BITSP_COORDS, n, xy=a, xy2=b)
+    prm = B().params(P, 0, 0, 0.7, G, seed=21, diversity_interval=div)
+    sb, per_gen = _builtin_nsga(a, b, prm, G, per_generation=True)
+    s = B().Solver(B().external(n, num_objectives=2), prm)
+    refills = 0
+
+    def objectives(rows):
+        return O.evaluate(po, rows)
+
+    s.external_step(objectives)
+    for g in range(G):
+        while True:
+            _, _, _, first, cnt = s.external_begin()
+            assert cnt == (P if first == P else P - first)
+            s.external_set_fitness(objectives(s.external_rows()))
+            if s.external_commit():
+                break
+            refills += 1
+        keys_e, obj_e = s.get_population()
+        np.testing.assert_array_equal(keys_e, per_gen[g][0], err_msg=f"generation {g + 1}")
+        np.testing.assert_array_equal(obj_e, per_gen[g][1], err_msg=f"generation {g + 1}")
+    if n == 4:
+        assert refills > 0
+    fo_e, fk_e = s.get_pareto_front()
+    fo_b, fk_b = sb.get_pareto_front()
+    np.testing.assert_array_equal(fo_e, fo_b)
+    np.testing.assert_array_equal(fk_e, fk_b)
+    np.testing.assert_array_equal(s.get_fitness_history(), sb.get_fitness_history())
 
 
 def test_external_cpp_program(cuda):
