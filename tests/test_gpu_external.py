@@ -201,3 +201,22 @@ def test_external_cpp_program(cuda):
     r = subprocess.run([exe, "host", "41", "3", "60"], capture_output=True, text=True, timeout=300,
                        env=dict(os.environ, QUICK_TEST="10"))
     assert r.returncode == 0 and json.loads(r.stdout.strip().splitlines()[-1])["history"] == 11
+
+
+def test_external_cpp_program_two_objectives(cuda):
+    """the same config with a second weight vector (objective_functions, NSGA-II): the host
+    objectives and the config's own two-objective kernel give the same Pareto front, and
+    no point of it dominates another"""
+    exe = os.path.join(os.path.dirname(B().LIB_PATH), "..", "build", "solve_external")
+    outs = {}
+    for mode in ("host2", "gpu2"):
+        r = subprocess.run([exe, mode, "37", "5", "40"], capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stderr
+        assert "Pareto front size:" in r.stdout
+        outs[mode] = json.loads(r.stdout.strip().splitlines()[-1])
+    assert outs["host2"] == outs["gpu2"]
+    pts = np.array(outs["host2"]["points"])
+    assert outs["host2"]["front"] == len(pts) > 0
+    for i in range(len(pts)):
+        dom = np.all(pts <= pts[i], axis=1) & np.any(pts < pts[i], axis=1)
+        assert not dom.any()
