@@ -427,6 +427,52 @@ print(json.dumps(dict(value=g / t, gens=g, seconds=t)))
             "sample": f"{d['gens']} generations ({d['seconds']:.1f} s) of the same workload"}
 
 
+def workload_external(args):
+    """a config that brings its own fitness, as the reference's LLM solver writes them
+    (cpp/examples/solve_external.cu: single-machine weighted completion time, n=40, P=256,
+    E=51, M=25, rho=0.7, generated-main flow): generations/s with its host
+    fitness_function and with its own CUDA kernel, and the reference's CPU solver on the
+    same config and instance"""
+    exe = os.path.join(ROOT, "llm-brkga_b200", "build", "solve_external")
+    gens = args.generations
+    out = {"metric": "gens/s LLM-style config, weighted completion time n=40 pop 256", "unit": "gens/s",
+           "generations": gens, "workload": "external fitness (BRKGA_EXTERNAL) through the drop-in Solver"}
+    for mode in ("host", "gpu"):
+        r = subprocess.run([exe, mode, "40", "1", str(gens)], capture_output=True, text=True, timeout=900)
+        if r.returncode != 0:
+            raise SystemExit(f"solve_external {mode} failed: {r.stderr[-500:]}")
+        d = json.loads(r.stdout.strip().splitlines()[-1])
+        key = "value" if mode == "host" else "gpu_fitness_value"
+        out[key] = gens / d["seconds"]
+        out["best_" + mode] = d["best"]
+    if not args.no_cpu:
+        code = f"""
+import json, sys
+sys.path[:0] = [{os.path.join(ROOT, 'oracle')!r}]
+import oracle as O
+if not O.ref_available():
+    print(json.dumps(dict(value=None))); sys.exit(0)
+R = O.ref()
+h = R.ref_solver_create_wct(40, 1, 256, 51, 25, 0.7)
+R.ref_solver_evolve(h, 1)
+g, t = 0, 0.0
+while t < 10.0 and g < {gens}:
+    t += R.ref_solver_evolve(h, 1); g += 1
+print(json.dumps(dict(value=g / t, gens=g, seconds=t, best=R.ref_solver_best(h))))
+"""
+        env = dict(os.environ, CUDA_VISIBLE_DEVICES="")
+        r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=900)
+        if r.returncode == 0:
+            d = json.loads(r.stdout.strip().splitlines()[-1])
+            if d.get("value") is not None:
+                out["cpu_baseline"] = {"value": d["value"], "unit": "gens/s", "cores": 1, "kind": "reference",
+                                       "sample": f"{d['gens']} generations ({d['seconds']:.1f} s) of the same config"}
+                out["best_reference"] = d["best"]
+        else:
+            out["cpu_baseline"] = {"error": r.stderr[-500:]}
+    return out
+
+
 def workload_batch(args):
     """256 TSP instances, n ~ U[100,2000], P in {256,512,1024}, 4 islands migrating the 2
     best every 50 generations, 500 generations, in one batch; against the same instances
@@ -814,6 +860,8 @@ def run_workload(args):
         out = workload_operators(args)
     elif w == "batch":
         out = workload_batch(args)
+    elif w == "external":
+        out = workload_external(args)
     elif w == "serve":
         out = workload_serve(args)
     elif w == "quality":
@@ -857,7 +905,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--profile-op", action="store_true", help="operator kernels only (profiler captures)")
     ap.add_argument("--workload", default="tsp1000",
-                    choices=["tsp1000", "tsp52", "nsga", "tspj", "movrp", "operators", "batch", "serve", "quality"])
+                    choices=["tsp1000", "tsp52", "nsga", "tspj", "movrp", "operators", "batch", "serve", "quality",
+                             "external"])
     ap.add_argument("--generations", type=int, default=500)
     ap.add_argument("--instances", type=int, default=256)
     ap.add_argument("--rate", type=float, default=200.0)

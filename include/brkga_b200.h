@@ -278,8 +278,9 @@ int32_t brkga_get_pareto_front(brkga_engine* e, float* objectives, float* keys, 
  *   brkga_external_get_rows  the pending rows into host keys [count][n].
  *   brkga_external_set_fitness  host fitness [count][num_objectives] for them.
  *   brkga_external_commit  waits for the device (so fitness that the caller's kernels
- *                          wrote on any stream is in place), ranks the population and
- *                          completes the generation.  NSGA-II: when the generation's
+ *                          wrote on any stream is in place), then ranks the population on
+ *                          the engine's stream, completing the generation (calls that read
+ *                          the population wait for it).  NSGA-II: when the generation's
  *                          diversity pass (ensure_minimum_diversity, core/population.hpp:
  *                          130-182) replaced rows with fresh keys, it returns
  *                          BRKGA_ERR_NOT_READY instead: the next brkga_external_begin

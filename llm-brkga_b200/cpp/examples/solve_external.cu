@@ -14,6 +14,7 @@
 // in the two-objective modes the Pareto front's size and its objective pairs.
 #include <cuda_runtime.h>
 
+#include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <numeric>
@@ -155,12 +156,14 @@ int main(int argc, char** argv) {
             if (config_ptr) config_ptr->max_generations = std::atoi(quick_test_env);
         }
         std::cout << "Running optimization..." << std::endl;
+        const auto t0 = std::chrono::steady_clock::now();
         solver.run();
+        const double seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         if (two) {
             // the generated main's multi-objective branch: the Pareto front
             auto pareto = solver.get_pareto_front();
             std::cout << "Pareto front size: " << pareto.size() << std::endl;
-            std::printf("{\"front\": %zu, \"points\": [", pareto.size());
+            std::printf("{\"seconds\": %.6f, \"front\": %zu, \"points\": [", seconds, pareto.size());
             for (size_t i = 0; i < pareto.size(); ++i)
                 std::printf("%s[%.9g, %.9g]", i ? ", " : "", (double)pareto[i].objectives[0],
                             (double)pareto[i].objectives[1]);
@@ -173,8 +176,9 @@ int main(int argc, char** argv) {
         if (config_ptr) config_ptr->print_solution(best);
         const auto& hist = solver.get_fitness_history();
         const float again = config_ptr->fitness_function(best);
-        std::printf("{\"best\": %.9g, \"check\": %.9g, \"history\": %zu, \"first\": %.9g, \"last\": %.9g}\n",
-                    (double)best.fitness, (double)again, hist.size(), (double)hist.front(), (double)hist.back());
+        std::printf("{\"seconds\": %.6f, \"best\": %.9g, \"check\": %.9g, \"history\": %zu, \"first\": %.9g, "
+                    "\"last\": %.9g}\n",
+                    seconds, (double)best.fitness, (double)again, hist.size(), (double)hist.front(), (double)hist.back());
     } catch (const std::exception& e) {
         std::cerr << "Error: " << e.what() << std::endl;
         return 1;

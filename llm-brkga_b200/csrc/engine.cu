@@ -848,9 +848,10 @@ int32_t brkga_external_commit(brkga_engine* e) {
     if (err != cudaSuccess) return cuda_fail(err, "external fitness");
     const int state = e->ext_state;
     e->ext_state = 0;
+    // the ranking is enqueued; every later call that reads the population (or builds the
+    // next rows) waits for the engine's stream first
     if (!sh.mo) {
         err = launch_sort_pops(e->dd, sh.k, sh.Pi, state == 1 ? 0 : 1, e->stream);
-        if (err == cudaSuccess) err = cudaStreamSynchronize(e->stream);
         if (err != cudaSuccess) return cuda_fail(err, "external commit");
         if (state == 1) {
             e->initialized = true;
@@ -890,7 +891,6 @@ int32_t brkga_external_commit(brkga_engine* e) {
         }
         if (err == cudaSuccess) ++e->gen;
     }
-    if (err == cudaSuccess) err = cudaStreamSynchronize(e->stream);
     if (err != cudaSuccess) return cuda_fail(err, "external commit");
     if (state == 1) {
         e->initialized = true;

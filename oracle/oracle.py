@@ -326,6 +326,8 @@ def ref():
         R.ref_cont_eval.argtypes = [C.c_int, C.c_float, C.c_float, C.c_int, _f32p, C.c_int, _f32p]
         R.ref_pareto.argtypes = [_f32p, C.c_int, _i32p, _f32p]
         R.ref_nsga2_select.argtypes = [_f32p, C.c_int, C.c_int, _i32p]
+        R.ref_solver_create_wct.restype = C.c_void_p
+        R.ref_solver_create_wct.argtypes = [C.c_int, C.c_uint, C.c_int, C.c_int, C.c_int, C.c_double]
         R.ref_brkga_generation.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_uint32,
                                            _f32p, _f32p, _f32p, _f32p, _i32p, _i32p, _u8p, _f32p]
         R.ref_nsga2_offspring.argtypes = [_f32p, _f32p, C.c_int, C.c_int, C.c_double, C.c_uint32, _f32p, _i32p,

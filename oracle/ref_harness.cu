@@ -521,6 +521,48 @@ void* ref_solver_create_movrp(const float* xy, const int32_t* demands, int n, in
     return nullptr;
 }
 
+// a config that brings only a host fitness_function, the kind the reference's LLM solver
+// writes: single-machine weighted completion time (jobs in key order, ties to the lower
+// job; sum of w_j * C_j, minimised), with the float arithmetic of the engine's external-
+// fitness example (llm-brkga_b200/cpp/examples/solve_external.cu) and its host
+// fitness_function, with the instance drawn as that example draws it (std::mt19937(seed):
+// processing times U[1, 100), then weights U[1, 10))
+// a subclass, as the LLM solver's configs are (a bare BRKGAConfig<float> given to the
+// reference's Solver crashed in this -O3 build; at -O1 it ran)
+struct RefWctConfig : public BRKGAConfig<float> {
+    explicit RefWctConfig(int n) : BRKGAConfig<float>(n) {}
+};
+
+void* ref_solver_create_wct(int n, unsigned seed, int P, int E, int M, double rho) {
+    try {
+        auto cfg = std::make_unique<RefWctConfig>(n);
+        std::mt19937 rng(seed);
+        std::uniform_real_distribution<float> up(1.0f, 100.0f), uw(1.0f, 10.0f);
+        std::vector<float> pv(n), wv(n);
+        for (int i = 0; i < n; ++i) {
+            pv[i] = up(rng);
+            wv[i] = uw(rng);
+        }
+        cfg->fitness_function = [pv, wv](const Individual<float>& ind) {
+            const std::vector<float>& keys = ind.chromosomes[0];
+            std::vector<int> order(keys.size());
+            std::iota(order.begin(), order.end(), 0);
+            std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return keys[a] < keys[b]; });
+            float c = 0.0f, total = 0.0f;
+            for (int job : order) {
+                c = c + pv[job];
+                const float prod = wv[job] * c;
+                total = total + prod;
+            }
+            return total;
+        };
+        cfg->comparator = [](float a, float b) { return a < b; };
+        return make_solver(std::move(cfg), P, E, M, rho);
+    } catch (...) {
+    }
+    return nullptr;
+}
+
 const char* ref_solver_mode(void* h) { return static_cast<RefSolver*>(h)->s->execution_mode.c_str(); }
 
 double ref_solver_evolve(void* h, int gens) {

@@ -195,6 +195,7 @@ def test_external_cpp_program(cuda):
         assert r.returncode == 0, r.stderr
         assert "Best fitness:" in r.stdout and "Weighted completion time:" in r.stdout
         outs[mode] = json.loads(r.stdout.strip().splitlines()[-1])
+        outs[mode].pop("seconds")
     assert outs["host"] == outs["gpu"]
     d = outs["host"]
     assert d["best"] == d["check"] and d["history"] == 61 and d["last"] <= d["first"]
@@ -214,6 +215,7 @@ def test_external_cpp_program_two_objectives(cuda):
         assert r.returncode == 0, r.stderr
         assert "Pareto front size:" in r.stdout
         outs[mode] = json.loads(r.stdout.strip().splitlines()[-1])
+        outs[mode].pop("seconds")
     assert outs["host2"] == outs["gpu2"]
     pts = np.array(outs["host2"]["points"])
     assert outs["host2"]["front"] == len(pts) > 0
