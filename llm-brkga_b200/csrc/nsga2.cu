@@ -41,11 +41,66 @@ __host__ __device__ inline int npow2(int x) {
     return p;
 }
 
+// Ascending bitonic sort of s[0, N2) (N2 a power of two) by the whole block.  Strides of 64
+// and more go through shared memory with a barrier each; strides 32 .. 1 run in registers:
+// warp w owns the 64-element blocks w, w + warps, ..., lane l holding elements l and l + 32
+// of a block (stride 32 inside the lane, strides 16 .. 1 by shuffles), so each k costs one
+// barrier for all of its small strides instead of six.
+__device__ __forceinline__ unsigned long long cx_keep(unsigned long long x, unsigned long long y, int g, int j,
+                                                      int k) {
+    // element g of the pair (g, g ^ j): the lower index keeps the minimum in an ascending
+    // run ((g & k) == 0), the maximum in a descending one
+    const bool keep_min = ((g & j) == 0) == ((g & k) == 0);
+    return keep_min ? (x < y ? x : y) : (x < y ? y : x);
+}
+
 template <int BLOCK>
 __device__ void bitonic_u64(unsigned long long* s, int N2) {
     const int t = threadIdx.x;
-    for (int k = 2; k <= N2; k <<= 1)
-        for (int j = k >> 1; j > 0; j >>= 1) {
+    if (N2 < 64) {
+        for (int k = 2; k <= N2; k <<= 1)
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                for (int p = t; p < (N2 >> 1); p += BLOCK) {
+                    const int i = ((p & ~(j - 1)) << 1) | (p & (j - 1));
+                    const int ixj = i + j;
+                    const bool up = (i & k) == 0;
+                    const unsigned long long a = s[i], b = s[ixj];
+                    if ((a > b) == up) {
+                        s[i] = b;
+                        s[ixj] = a;
+                    }
+                }
+                __syncthreads();
+            }
+        return;
+    }
+    constexpr int NW = BLOCK / 32;
+    const int lane = t & 31, warp = t >> 5;
+    // strides min(32, k / 2) .. 1 of step k on every 64-element block, in registers
+    auto small_strides = [&](int k, int jmax) {
+        for (int base = warp * 64; base < N2; base += NW * 64) {
+            const int g0 = base + lane, g1 = g0 + 32;
+            unsigned long long x0 = s[g0], x1 = s[g1];
+            if (jmax >= 32) {
+                const unsigned long long lo = x0 < x1 ? x0 : x1, hi = x0 < x1 ? x1 : x0;
+                const bool up = (g0 & k) == 0;
+                x0 = up ? lo : hi;
+                x1 = up ? hi : lo;
+            }
+            for (int j = (jmax >= 32 ? 16 : jmax); j > 0; j >>= 1) {
+                const unsigned long long y0 = __shfl_xor_sync(0xffffffffu, x0, j);
+                const unsigned long long y1 = __shfl_xor_sync(0xffffffffu, x1, j);
+                x0 = cx_keep(x0, y0, g0, j, k);
+                x1 = cx_keep(x1, y1, g1, j, k);
+            }
+            s[g0] = x0;
+            s[g1] = x1;
+        }
+        __syncthreads();
+    };
+    for (int k = 2; k <= 64; k <<= 1) small_strides(k, k >> 1);
+    for (int k = 128; k <= N2; k <<= 1) {
+        for (int j = k >> 1; j >= 64; j >>= 1) {
             for (int p = t; p < (N2 >> 1); p += BLOCK) {
                 const int i = ((p & ~(j - 1)) << 1) | (p & (j - 1));
                 const int ixj = i + j;
@@ -58,6 +113,8 @@ __device__ void bitonic_u64(unsigned long long* s, int N2) {
             }
             __syncthreads();
         }
+        small_strides(k, 32);
+    }
 }
 
 constexpr int kCB = 16;  // count planes (two's complement)
