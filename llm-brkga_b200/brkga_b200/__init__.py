@@ -324,6 +324,7 @@ class Solver:
         self.h = h
         self.n = problem.n
         self.m = problem.num_objectives
+        self._ext_count = 0  # rows pending an external fitness (set by external_begin)
 
     def close(self):
         if getattr(self, "h", None):
