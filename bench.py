@@ -9,11 +9,16 @@ tour length kernel + elite-partition sort) of the device-resident solver.
 
 N > 1 runs N independent replicas (one instance per GPU, no collective: islands and
 instances are independent units), launched one process per GPU by torch.distributed.run.
-The JSON line's `value` is whole-job generations per second with the population resident
-in HBM; `e2e` is the same metric through the C ABI from host buffers: each e2e step is one
-whole 1000-generation solve (problem upload from pinned memory, create, initialise,
-evolve, read the best tour back).  L2 is flushed (a 256 MiB write) before every timed
-generation, outside its CUDA-event bracket.
+One timed step is a stretch of GENS_PER_STEP generations of the device-resident solver
+(one evolve call: captured CUDA graphs of 16 generations each), with L2 flushed (a 256 MiB
+write) before every step, outside its CUDA-event bracket; inside a step the 16 MB
+population stays L2-resident as it does in a solver run.  The JSON line's `value` is
+whole-job generations per second with the population resident in HBM;
+`l2_flushed_gens_per_s` times single generations with L2 flushed before each.  `e2e` is the
+same metric through the C ABI from host buffers: each e2e step is one whole
+1000-generation solve (problem upload from pinned memory, create, initialise, evolve, read
+the best tour back).  At N = 1 the line also nests the batched (256 island instances),
+served (Poisson mixed stream) and 32-seed quality measurements.
 """
 from __future__ import annotations
 
@@ -37,9 +42,16 @@ for _p in (os.path.join(ROOT, "llm-brkga_b200"), os.path.join(ROOT, "oracle")):
 METRIC = "gens/s TSP n=1000 pop 2048"
 N_CITIES, POP, ELITE, MUTANTS, RHO = 1000, 2048, 307, 307, 0.7
 E2E_GENERATIONS = 1000
+GENS_PER_STEP = 4096  # generations per timed step (about 0.13 s of device work)
 SEED_INSTANCE, SEED_GA = 2026, 7
 PROFILE = os.path.join(ROOT, "profiles", "row_kernel_tsp_n1000_p2048.md")
 HOLD_CYCLES_PER_STEP = 400_000  # ~0.2 ms of device spin per queued step (host enqueue cost)
+
+
+def workload_config():
+    """the headline workload, identical in both arms' lines"""
+    return {"workload": f"TSP n={N_CITIES} pop={POP} elite={ELITE} mutants={MUTANTS} rho={RHO}",
+            "n": N_CITIES, "population": POP, "elite": ELITE, "mutants": MUTANTS, "rho": RHO}
 
 
 def instance():
@@ -198,32 +210,49 @@ def run_ours(args, rank, world):
     stream = torch.cuda.ExternalStream(s.stream, device=dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
 
+    gps = args.gens_per_step
     for _ in range(args.warmup):
         with torch.cuda.stream(stream):
             flush.fill_(1.0)
-        s.evolve(1)
+        s.evolve(gps)
     s.synchronize()
 
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     barrier()
     with ClockSampler(dev) as clocks:
-        # hold the stream while the host queues every timed step, so no host gap lands
+        # hold the stream while the host queues the first steps, so no host gap lands
         # inside an event bracket (the hold itself is outside every bracket)
         with torch.cuda.stream(stream):
-            torch.cuda._sleep(HOLD_CYCLES_PER_STEP * args.steps)
+            torch.cuda._sleep(HOLD_CYCLES_PER_STEP * 16)
         for i in range(args.steps):
             with torch.cuda.stream(stream):
                 flush.fill_(float(i))
                 starts[i].record(stream)
-            s.evolve(1)
+            s.evolve(gps)
             with torch.cuda.stream(stream):
                 ends[i].record(stream)
         s.synchronize()
         barrier()
     ms = reps.max(sum(a.elapsed_time(b) for a, b in zip(starts, ends)))
-    value = whole_job_rate(world, args.steps, ms / 1e3)
+    value = whole_job_rate(world, args.steps * gps, ms / 1e3)
     best = float(s.get_best_individual()[2])
+
+    # --- single generations with L2 flushed before each (the population re-read from HBM)
+    f_starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    f_ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    with torch.cuda.stream(stream):
+        torch.cuda._sleep(HOLD_CYCLES_PER_STEP * args.steps)
+    for i in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(float(i))
+            f_starts[i].record(stream)
+        s.evolve(1)
+        with torch.cuda.stream(stream):
+            f_ends[i].record(stream)
+    s.synchronize()
+    f_ms = reps.max(sum(a.elapsed_time(b) for a, b in zip(f_starts, f_ends)))
+    flushed_value = whole_job_rate(world, args.steps, f_ms / 1e3)
 
     # --- dominant kernel alone: the fused row kernel through the generation-step entry point
     ld = (N_CITIES + 3) // 4 * 4
@@ -256,19 +285,6 @@ def run_ours(args, rank, world):
     torch.cuda.synchronize()
     row_ms = sum(a.elapsed_time(b) for a, b in zip(kstarts, kends)) / args.steps
     sort_ms = sum(a.elapsed_time(b) for a, b in zip(sstarts, sends)) / args.steps
-
-    # --- for information: back-to-back generations with L2 left warm (one evolve call)
-    warm_gens = 200
-    s.synchronize()
-    w0, w1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with torch.cuda.stream(stream):
-        torch.cuda._sleep(HOLD_CYCLES_PER_STEP)
-        w0.record(stream)
-    s.evolve(warm_gens)
-    with torch.cuda.stream(stream):
-        w1.record(stream)
-    s.synchronize()
-    warm_gens_per_s = warm_gens / (w0.elapsed_time(w1) / 1e3)
 
     # --- end to end through the C ABI from host buffers: one whole solve per step
     e2e = None
@@ -315,10 +331,12 @@ def run_ours(args, rank, world):
             "metric": METRIC, "value": value, "unit": "gens/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded uniform coordinates)",
-            "config": {"workload": f"TSP n={N_CITIES} pop={POP} elite={ELITE} mutants={MUTANTS} rho={RHO}",
-                       "n": N_CITIES, "population": POP, "elite": ELITE, "mutants": MUTANTS, "rho": RHO,
-                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                       "l2": "flushed (256 MiB write) before every timed generation, outside the timing"},
+            "config": workload_config(),
+            "generations_per_step": gps,
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+            "l2": f"flushed (256 MiB write) before every timed step of {gps} generations, outside the timing; "
+                  "within a step the population stays L2-resident as in a solver run",
+            "l2_flushed_gens_per_s": flushed_value,
             "impl": "ours",
             "e2e": e2e,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -330,13 +348,12 @@ def run_ours(args, rank, world):
                                          "coords_in_smem": bool(s_info[3])},
                          "algorithmic_bytes_per_launch": alg, "kernel_ms": row_ms, "peak_kind": peak_kind,
                          "sort_kernel_ms": sort_ms},
-            "gpu_launches": 2 * args.steps,
+            "gpu_launches": 2 * args.steps * gps,
             # rows decoded and evaluated per generation: children and mutants (elites keep
             # their fitness, as the reference's host path does)
             "individual_evaluations_per_s": value * (POP - ELITE),
             "clocks": clocks.summary(),
             "best_tour": best,
-            "l2_warm_back_to_back_gens_per_s": warm_gens_per_s,
         }
     s.close()
     reps.close()
@@ -569,9 +586,12 @@ def workload_serve(args):
     makespan = time.perf_counter() - t0
     lat = np.array([done[r][3] for r in ids])
     srv.close()
-    # plain solver: one request at a time, alone on the GPU, on a sample
-    sample = list(range(0, len(reqs), max(1, len(reqs) // 24)))
-    tsum = 0.0
+    # plain solver (the drop-in, one request at a time, alone on the GPU) on every k-th
+    # request of the same stream; its best must equal the served one (results do not depend
+    # on what else shares the GPU)
+    every = max(1, args.plain_every)
+    sample = list(range(0, len(reqs), every))
+    tsum, same = 0.0, 0
     for i in sample:
         _, kw, prm = reqs[i]
         kw = dict(kw)
@@ -581,14 +601,24 @@ def workload_serve(args):
         t1 = time.perf_counter()
         s = B.Solver(pb, prm)
         s.run()
-        s.get_best_individual()
+        best = s.get_best_individual()[2]
         s.close()
         tsum += time.perf_counter() - t1
+        pb.close()
+        m = 2 if kind == B.BITSP_COORDS else 1
+        served_best = np.asarray(done[ids[i]][1], np.float32).reshape(-1)[:m]
+        same += int(np.array_equal(np.asarray(best, np.float32).reshape(-1)[:m], served_best))
     plain = len(sample) / tsum
+    kinds = {"tsp": 0, "knapsack": 0, "bitsp": 0}
+    for _, kw, _ in reqs:
+        kinds["tsp" if kw["kind"] == B.TSP_COORDS else "knapsack" if kw["kind"] == B.KNAP_GREEDY else "bitsp"] += 1
     return {"metric": "served solves/s mixed stream", "value": len(reqs) / makespan, "unit": "solves/s",
-            "requests": len(reqs), "arrival_rate": rate, "arrival_seconds": dur, "makespan_s": makespan,
+            "requests": len(reqs), "mix": kinds, "arrival_rate": rate, "arrival_seconds": dur,
+            "makespan_s": makespan,
             "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
-            "plain_solver_solves_per_s": plain, "speedup_vs_plain": (len(reqs) / makespan) / plain,
+            "plain_solver_solves_per_s": plain, "plain_solver_sample": f"every {every}th request ({len(sample)})",
+            "speedup_vs_plain": (len(reqs) / makespan) / plain,
+            "sample_results_identical_to_plain": f"{same}/{len(sample)}",
             "generations": gens, "max_active": args.max_active, "tick": args.tick}
 
 
@@ -735,7 +765,7 @@ def _stats(v):
     return {"mean": float(v.mean()), "std": float(v.std()), "min": float(v.min()), "max": float(v.max())}
 
 
-def workload_quality(args):
+def workload_quality(args, headline_scale=True):
     """Best tour over 32 seeds on the n=52 configuration (coordinates uniform in
     [0,1000)^2 from seed 1, population 256, elite 51, mutants 25, rho 0.7, 500
     generations): this engine (the 32 seeds as one batch, spot-checked against the plain
@@ -764,26 +794,27 @@ def workload_quality(args):
         s.run()
         same += int(np.float32(s.get_best_individual()[2]) == np.float32(ours[i]))
         s.close()
-    # the headline scale too, on fewer runs (the reference's CPU path takes about 0.09 s
-    # per generation there): TSP n=1000, P=2048, E=M=307, 100 generations, 4 runs each
-    xy2 = instance()
-    pb2 = B.tsp(xy2)
-    big = []
-    for sd in range(1, 5):
-        s = B.Solver(pb2, B.params(POP, ELITE, MUTANTS, RHO, 100, seed=sd))
-        s.run()
-        big.append(float(s.get_best_individual()[2]))
-        s.close()
-    out_big = {"ours_100_generations": _stats(big)}
     out = {"metric": "best tour over 32 seeds, TSP n=52 pop 256, 500 generations", "unit": "tour length",
-           "tsp1000_pop2048": out_big,
            "ours": _stats(ours), "ours_seconds_32_runs": secs, "ours_fp32_vs_fp64_max_rel": max(rel),
            "plain_solver_identical": f"{same}/{len(range(0, runs, 8))}", "generations": gens}
+    if headline_scale:
+        # the headline scale too, on fewer runs (the reference's CPU path takes about 0.09 s
+        # per generation there): TSP n=1000, P=2048, E=M=307, 100 generations, 4 runs each
+        xy2 = instance()
+        pb2 = B.tsp(xy2)
+        big = []
+        for sd in range(1, 5):
+            s = B.Solver(pb2, B.params(POP, ELITE, MUTANTS, RHO, 100, seed=sd))
+            s.run()
+            big.append(float(s.get_best_individual()[2]))
+            s.close()
+        out["tsp1000_pop2048"] = {"ours_100_generations": _stats(big)}
     if not args.no_cpu:
         ref = reference_quality(xy, runs, gens)
-        ref_big = reference_quality(xy2, 4, 100, P=POP, E=ELITE, M=MUTANTS)
-        if isinstance(ref_big, list):
-            out_big["reference_100_generations"] = _stats(ref_big)
+        if headline_scale:
+            ref_big = reference_quality(xy2, 4, 100, P=POP, E=ELITE, M=MUTANTS)
+            if isinstance(ref_big, list):
+                out["tsp1000_pop2048"]["reference_100_generations"] = _stats(ref_big)
         if isinstance(ref, list):
             out["reference"] = _stats(ref)
             out["mean_ours_minus_reference_rel"] = (out["ours"]["mean"] - out["reference"]["mean"]) / \
@@ -913,6 +944,11 @@ def main():
     ap.add_argument("--duration", type=float, default=10.0)
     ap.add_argument("--max-active", type=int, default=256)
     ap.add_argument("--tick", type=int, default=25)
+    ap.add_argument("--plain-every", type=int, default=20,
+                    help="served stream: the plain solver runs every k-th request")
+    ap.add_argument("--gens-per-step", type=int, default=GENS_PER_STEP)
+    ap.add_argument("--no-extras", action="store_true",
+                    help="headline only: skip the nested batched / served / quality measurements")
     args = ap.parse_args()
     if args.profile_op:
         profile_op(args)
@@ -932,9 +968,7 @@ def main():
         line = {"metric": METRIC, "value": cb["value"], "unit": "gens/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": 1e3 / cb["value"], "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded uniform coordinates)",
-                "config": {"workload": f"TSP n={N_CITIES} pop={POP} elite={ELITE} mutants={MUTANTS} rho={RHO}",
-                           "n": N_CITIES, "population": POP, "elite": ELITE, "mutants": MUTANTS, "rho": RHO},
-                "impl": "reference", "cpu_baseline": cb,
+                "config": workload_config(), "impl": "reference", "cpu_baseline": cb,
                 "e2e": {"value": cb["value"], "unit": "gens/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         return
@@ -943,6 +977,12 @@ def main():
     if rank == 0:
         if not args.no_cpu:
             out["cpu_baseline"] = cpu_baseline()
+        if world == 1 and not args.no_extras:
+            # BASELINE's batched-islands and served-stream configurations, and the 32-seed
+            # quality check, measured after the headline (outside its timed region)
+            out["batched"] = workload_batch(args)
+            out["served"] = workload_serve(args)
+            out["quality"] = workload_quality(args, headline_scale=False)
         print(json.dumps(out))
 
 

@@ -210,9 +210,10 @@ int32_t brkga_pareto_rank_bitmatrix(const float* d_obj, int32_t N, int32_t m, in
  * on every GPU that loads it, held until the process exits), so N is limited to 2048
  * points (larger N returns BRKGA_ERR_UNSUPPORTED); 1 <= m <= 4.  The first call on a
  * device looks up that array's address and raises a kernel's shared-memory limit; make
- * that first call before any stream capture.  Asynchronous on `stream`.  Every call uses
- * the same array: calls whose work overlaps on the GPU (different streams, or another
- * thread) race and must be ordered by the caller. */
+ * that first call before any stream capture.  The address is kept for the life of the
+ * process, so do not use this entry point on a device after cudaDeviceReset.  Asynchronous
+ * on `stream`.  Every call uses the same array: calls whose work overlaps on the GPU
+ * (different streams, or another thread) race and must be ordered by the caller. */
 int32_t brkga_pareto_rank_noalloc(const float* d_obj, int32_t N, int32_t m, int32_t* d_rank, void* stream);
 /* Crowding distance per front (core/population.hpp:453-489), fronts from d_rank; two
  * objectives, N <= 4096.  Asynchronous on `stream`; its scratch comes from the library's
@@ -278,7 +279,10 @@ int32_t brkga_get_pareto_front(brkga_engine* e, float* objectives, float* keys, 
  *   brkga_external_get_rows  the pending rows into host keys [count][n].
  *   brkga_external_set_fitness  host fitness [count][num_objectives] for them.
  *   brkga_external_commit  waits for the device (so fitness that the caller's kernels
- *                          wrote on any stream is in place), then ranks the population on
+ *                          wrote on any stream is in place: a cudaDeviceSynchronize, which
+ *                          also waits for every other engine's and thread's work on that
+ *                          device, so engines driven from several host threads serialise
+ *                          at each commit), then ranks the population on
  *                          the engine's stream, completing the generation (calls that read
  *                          the population wait for it).  NSGA-II: when the generation's
  *                          diversity pass (ensure_minimum_diversity, core/population.hpp:

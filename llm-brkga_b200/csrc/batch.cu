@@ -562,6 +562,7 @@ int32_t brkga_batch_evolve(brkga_batch* b, int32_t generations) {
     for (Member* m : b->g.members)
         if ((int)b->gen + generations + 1 > m->pop.hist_cap)
             return fail(BRKGA_ERR_INVALID, "batch evolved past a member's max_generations");
+    NvtxRange range("batch generations", b->gen + 1u, b->gen + (unsigned)generations);
     cudaError_t e = run_generations(b->g, b->gen, generations, true);
     if (e != cudaSuccess) return cuda_fail(e, "batch evolve");
     b->gen += generations;
@@ -851,6 +852,7 @@ int32_t brkga_server_step(brkga_server* s) {
     int32_t st;
     // 1. advance every active request by one tick (each stops at its own budget)
     if (!s->active.empty()) {
+        NvtxRange range("server tick");
         // membership changes often, so the tick launches directly instead of capturing
         e = run_generations(g, 0, tick, false);
         if (e != cudaSuccess) return cuda_fail(e, "server tick");
@@ -897,11 +899,23 @@ int32_t brkga_server_step(brkga_server* s) {
         }
         if (changed && (st = build_plan(g)) != BRKGA_OK) return st;
     }
-    // 3. admit queued requests while slots and memory allow
+    // 3. admit queued requests while slots and memory allow.  Besides the server's own
+    // budget, each admission round re-reads the device's free memory (other processes and
+    // engines come and go) plus what the library's pool holds unused, and keeps a reserve
+    // of 1/64 of the device free.
     std::vector<Member*> fresh;
+    size_t avail = 0;
+    if (!s->queue.empty() && (int)s->active.size() < s->cfg.max_active) {
+        size_t fr = 0, tot = 0;
+        if ((e = cudaMemGetInfo(&fr, &tot)) != cudaSuccess) return cuda_fail(e, "free memory");
+        const size_t spare = pool_spare(s->cfg.device), reserve = tot / 64;
+        avail = (fr + spare > reserve) ? fr + spare - reserve : 0;
+    }
     while (!s->queue.empty() && (int)s->active.size() < s->cfg.max_active) {
         Request* r = s->queue.front();
         if (s->in_use + r->bytes > s->budget) break;
+        if (r->bytes > avail) break;
+        avail -= r->bytes;
         s->queue.pop_front();
         std::shared_ptr<ProblemData> pd;
         Member* m = nullptr;

@@ -501,6 +501,7 @@ int32_t brkga_evolve(brkga_engine* e, int32_t generations) {
     if (st != BRKGA_OK) return st;
     cudaError_t err = cudaSuccess;
     int left = generations;
+    NvtxRange all("brkga_evolve", e->gen + 1u, e->gen + (unsigned)generations);
     while (left > 0 && err == cudaSuccess) {
         // plain generations until (and excluding) the next special one, in captured runs of
         // 16, then 8, 4, 2, 1
@@ -509,6 +510,7 @@ int32_t brkga_evolve(brkga_engine* e, int32_t generations) {
         while (plain > 0 && err == cudaSuccess) {
             int k = kMaxRunLog;
             while ((1 << k) > plain) --k;
+            NvtxRange run("generations", e->gen + 1u, e->gen + (1u << k));
             if (!e->gx_run[k]) err = capture(e, 1 << k, false, &e->gx_run[k]);
             if (err == cudaSuccess) err = cudaGraphLaunch(e->gx_run[k], e->stream);
             plain -= 1 << k;
@@ -517,6 +519,7 @@ int32_t brkga_evolve(brkga_engine* e, int32_t generations) {
         }
         if (left > 0 && err == cudaSuccess) {
             // here e->gen + 1 == next
+            NvtxRange run("generation (migration / diversity / local search)", e->gen + 1u, e->gen + 1u);
             if (!e->gx_special) err = capture(e, 1, true, &e->gx_special);
             if (err == cudaSuccess) err = cudaGraphLaunch(e->gx_special, e->stream);
             --left;

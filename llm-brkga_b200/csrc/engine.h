@@ -2,12 +2,14 @@
 #pragma once
 
 #include <cstdint>
+#include <cstdio>
 #include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include "../../include/brkga_b200.h"
 #include "kernels.h"
@@ -22,7 +24,24 @@ int32_t fail(int32_t code, const std::string& msg);
 int32_t dev_alloc(void** p, size_t bytes, cudaStream_t st);
 void dev_free(void* p, cudaStream_t st);
 size_t pool_reserved(int dev);
+size_t pool_spare(int dev);
 int32_t cuda_fail(cudaError_t e, const char* what);
+
+// An NVTX range around a stretch of host work (named like "generations 17-32").  With no
+// profiler attached NVTX calls return at once; under Nsight Systems the ranges line up with
+// the CUDA graphs each stretch launches.
+class NvtxRange {
+   public:
+    NvtxRange(const char* what, unsigned first, unsigned last) {
+        char buf[80];
+        snprintf(buf, sizeof buf, "%s %u-%u", what, first, last);
+        nvtxRangePushA(buf);
+    }
+    explicit NvtxRange(const char* what) { nvtxRangePushA(what); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 class DeviceGuard {
 public:

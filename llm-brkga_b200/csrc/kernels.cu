@@ -76,12 +76,73 @@ __device__ __forceinline__ int bucket_of(float key, float nbf, int nb) {
     return b < nb - 1 ? b : nb - 1;
 }
 
+// The exact rank inside a bucket scans the bucket, so its cost is the sum of the squared
+// bucket sizes.  Keys in [0,1) spread over about one per bucket; equal keys, keys outside
+// [0,1) (one bucket each side) or NaNs (the last bucket) pile into few buckets.  A row with
+// a bucket above kHeavyBucket keys is sorted instead by an ascending bitonic network over
+// its composites: O(n log^2 n) on any input, and the same (key, index) order.
+constexpr uint32_t kHeavyBucket = 32;
+
+// Ascending sort of a[0, n) (shared or global memory) by the whole block, any n: the
+// bitonic network in its one-direction form (each merge of size k first compares i with
+// its mirror inside the k-block, then half-cleaners of stride k/4 .. 1), with a[i] for
+// i >= n taken as +infinity.  Such an element is always the higher index of its pair and
+// would stay put, so pairs that reach past n are skipped and nothing is padded.
+template <int BLOCK>
+__device__ void block_sort_u64(unsigned long long* a, int n) {
+    const int t = threadIdx.x;
+    int n2 = 1;
+    while (n2 < n) n2 <<= 1;
+    const int half = n2 >> 1;
+    for (int k = 2; k <= n2; k <<= 1) {
+        const int hk = k >> 1;
+        for (int p = t; p < half; p += BLOCK) {
+            const int base = (p / hk) * k, x = p % hk;
+            const int i = base + x, j = base + k - 1 - x;
+            if (j < n) {
+                const unsigned long long u = a[i], v = a[j];
+                if (v < u) {
+                    a[i] = v;
+                    a[j] = u;
+                }
+            }
+        }
+        __syncthreads();
+        for (int st = k >> 2; st > 0; st >>= 1) {
+            for (int p = t; p < half; p += BLOCK) {
+                const int i = ((p & ~(st - 1)) << 1) | (p & (st - 1));
+                const int j = i + st;
+                if (j < n) {
+                    const unsigned long long u = a[i], v = a[j];
+                    if (v < u) {
+                        a[i] = v;
+                        a[j] = u;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// the permutation of a heavy row: each segment's composites sorted, then their indices;
+// called rather than inlined, so the row kernels keep their registers for the common path
+template <int BLOCK>
+__device__ __noinline__ void heavy_row_perm(unsigned long long* sc, int32_t* perm, int n, int split) {
+    block_sort_u64<BLOCK>(sc, split);
+    if (split < n) block_sort_u64<BLOCK>(sc + split, n - split);
+    for (int p = threadIdx.x; p < n; p += BLOCK) perm[p] = (int32_t)(uint32_t)sc[p];
+    __syncthreads();
+}
+
 // Counters must be zero on entry; they are left holding bucket offsets (the caller
 // re-zeroes them while it no longer needs them).  Bucket count NB = 4 * G * BLOCK >= n,
 // thread t owns the contiguous buckets [4Gt, 4Gt + 4G) for the scan.
 // Keys [split, n) form a second segment sorted on its own (TSPJ's job keys after its city
 // keys): it takes the upper half of the buckets, so no bucket mixes the segments and
-// positions [split, n) of the permutation hold the second segment's order.
+// positions [split, n) of the permutation hold the second segment's order.  A heavy row
+// sorts each segment's composites on its own: the scatter has put the first segment's in
+// [0, split).
 template <int BLOCK, int G>
 __device__ void row_argsort(const float (&k)[G][4], int n, int split, const RowSmem& s, uint32_t* warp_tot) {
     constexpr int KB = 4 * G, NB = KB * BLOCK;
@@ -102,11 +163,12 @@ __device__ void row_argsort(const float (&k)[G][4], int n, int split, const RowS
         }
     __syncthreads();
     uint4 c[G];
-    uint32_t sum = 0;
+    uint32_t sum = 0, big = 0;
 #pragma unroll
     for (int g = 0; g < G; ++g) {
         c[g] = reinterpret_cast<const uint4*>(s.cnt)[t * G + g];
         sum += c[g].x + c[g].y + c[g].z + c[g].w;
+        big = max(big, max(max(c[g].x, c[g].y), max(c[g].z, c[g].w)));
     }
     uint32_t run = block_exclusive_scan<BLOCK>(sum, warp_tot, nullptr);
 #pragma unroll
@@ -120,7 +182,7 @@ __device__ void row_argsort(const float (&k)[G][4], int n, int split, const RowS
         reinterpret_cast<uint4*>(s.cnt)[t * G + g] = o;
     }
     if (t == 0) s.cnt[NB] = (uint32_t)n;
-    __syncthreads();
+    const bool heavy = __syncthreads_or(big > kHeavyBucket) != 0;
     // scatter composites
 #pragma unroll
     for (int g = 0; g < G; ++g)
@@ -133,6 +195,10 @@ __device__ void row_argsort(const float (&k)[G][4], int n, int split, const RowS
             }
         }
     __syncthreads();
+    if (heavy) {
+        heavy_row_perm<BLOCK>(s.sc, s.perm, n, split);
+        return;
+    }
     // exact rank inside the bucket
 #pragma unroll
     for (int g = 0; g < G; ++g)
@@ -1074,10 +1140,15 @@ __global__ void __launch_bounds__(kBigBlock) row_kernel_big(RowLaunch L) {
             auto bucket = [&](float k, int i) { return bucket_of(k, nbf, nbs) + ((i >= split) ? nbs : 0); };
             for (int i = t; i < n; i += BLOCK) perm[i] = (int32_t)atomicAdd(&cnt[bucket(row[i], i)], 1u);
             __syncthreads();
+            bool heavy;
             {
                 const int ch = NB / BLOCK;
-                uint32_t sum = 0;
-                for (int j = t * ch; j < t * ch + ch; ++j) sum += cnt[j];
+                uint32_t sum = 0, big = 0;
+                for (int j = t * ch; j < t * ch + ch; ++j) {
+                    const uint32_t c = cnt[j];
+                    sum += c;
+                    big = max(big, c);
+                }
                 uint32_t run = block_exclusive_scan<BLOCK>(sum, warp_tot, nullptr);
                 for (int j = t * ch; j < t * ch + ch; ++j) {
                     const uint32_t c = cnt[j];
@@ -1085,21 +1156,26 @@ __global__ void __launch_bounds__(kBigBlock) row_kernel_big(RowLaunch L) {
                     run += c;
                 }
                 if (t == 0) cnt[NB] = (uint32_t)n;
+                heavy = __syncthreads_or(big > kHeavyBucket) != 0;
             }
-            __syncthreads();
             for (int i = t; i < n; i += BLOCK) {
                 const float k = row[i];
                 sc[cnt[bucket(k, i)] + (uint32_t)perm[i]] = ((unsigned long long)okey(k) << 32) | (uint32_t)i;
             }
             __syncthreads();
-            for (int i = t; i < n; i += BLOCK) {
-                const float k = row[i];
-                const int b = bucket(k, i);
-                const uint32_t b0 = cnt[b], b1 = cnt[b + 1];
-                const unsigned long long me = ((unsigned long long)okey(k) << 32) | (uint32_t)i;
-                uint32_t rk = b0;
-                for (uint32_t q = b0; q < b1; ++q) rk += (sc[q] < me) ? 1u : 0u;
-                perm[rk] = i;
+            if (heavy) {
+                // equal or extreme keys in few buckets: sort each segment's composites
+                heavy_row_perm<BLOCK>(sc, perm, n, split);
+            } else {
+                for (int i = t; i < n; i += BLOCK) {
+                    const float k = row[i];
+                    const int b = bucket(k, i);
+                    const uint32_t b0 = cnt[b], b1 = cnt[b + 1];
+                    const unsigned long long me = ((unsigned long long)okey(k) << 32) | (uint32_t)i;
+                    uint32_t rk = b0;
+                    for (uint32_t q = b0; q < b1; ++q) rk += (sc[q] < me) ? 1u : 0u;
+                    perm[rk] = i;
+                }
             }
             __syncthreads();
             for (int j = t; j <= NB; j += BLOCK) cnt[j] = 0u;  // for the next row
@@ -1317,11 +1393,12 @@ __device__ void movrp_argsort(const float (&v)[G][4], int n, float lo, float inv
         }
     __syncthreads();
     uint4 c[G];
-    uint32_t sum = 0;
+    uint32_t sum = 0, big = 0;
 #pragma unroll
     for (int g = 0; g < G; ++g) {
         c[g] = reinterpret_cast<const uint4*>(s.cnt)[t * G + g];
         sum += c[g].x + c[g].y + c[g].z + c[g].w;
+        big = max(big, max(max(c[g].x, c[g].y), max(c[g].z, c[g].w)));
     }
     uint32_t run = block_exclusive_scan<BLOCK>(sum, warp_tot, nullptr);
 #pragma unroll
@@ -1331,7 +1408,7 @@ __device__ void movrp_argsort(const float (&v)[G][4], int n, float lo, float inv
         reinterpret_cast<uint4*>(s.cnt)[t * G + g] = o;
     }
     if (t == 0) s.cnt[NB] = (uint32_t)n;
-    __syncthreads();
+    const bool heavy = __syncthreads_or(big > kHeavyBucket) != 0;
 #pragma unroll
     for (int g = 0; g < G; ++g)
 #pragma unroll
@@ -1342,6 +1419,10 @@ __device__ void movrp_argsort(const float (&v)[G][4], int n, float lo, float inv
                     ((unsigned long long)okey(v[g][l]) << 32) | (uint32_t)i;
         }
     __syncthreads();
+    if (heavy) {  // equal or extreme values in few buckets: sort the composites instead
+        heavy_row_perm<BLOCK>(s.sc, s.perm, n, n);
+        return;
+    }
 #pragma unroll
     for (int g = 0; g < G; ++g)
 #pragma unroll

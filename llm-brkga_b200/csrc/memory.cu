@@ -54,6 +54,16 @@ void dev_free(void* p, cudaStream_t st) {
     if (p) cudaFreeAsync(p, st);
 }
 
+// bytes the pool holds but has not handed out (reusable without a new device allocation)
+size_t pool_spare(int dev) {
+    cudaMemPool_t pool;
+    if (pool_of(dev, &pool) != cudaSuccess) return 0;
+    uint64_t reserved = 0, used = 0;
+    cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved);
+    cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used);
+    return reserved > used ? (size_t)(reserved - used) : 0;
+}
+
 size_t pool_reserved(int dev) {
     cudaMemPool_t pool;
     if (pool_of(dev, &pool) != cudaSuccess) return 0;

@@ -1435,7 +1435,8 @@ static std::map<int, std::pair<void*, size_t>> g_op_buf;
 
 static int32_t op_scratch(size_t need, void** out) {
     int dev = 0;
-    cudaGetDevice(&dev);
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
     auto& b = g_op_buf[dev];
     if (b.second < need) {
         if (b.first) {
@@ -1443,7 +1444,11 @@ static int32_t op_scratch(size_t need, void** out) {
             cudaFree(b.first);
         }
         b = {nullptr, 0};
-        if (cudaMalloc(&b.first, need) != cudaSuccess) return fail(BRKGA_ERR_OOM, "operator scratch");
+        if ((e = cudaMalloc(&b.first, need)) != cudaSuccess) {
+            b.first = nullptr;
+            cudaGetLastError();  // a failed allocation must not surface as a later launch's error
+            return fail(BRKGA_ERR_OOM, std::string("operator scratch: ") + cudaGetErrorString(e));
+        }
         b.second = need;
     }
     *out = b.first;

@@ -64,3 +64,20 @@ def tspj_instance(c, seed):
     jobs = (1.0 + rng.random((c + 1, c + 1)) * 99.0).astype(np.float32)
     jobs[0, :] = 0.0
     return travel, jobs
+
+
+def degenerate_keys(n, seed):
+    """rows whose keys crowd into a few buckets of a value-range bucket sort: every key equal
+    (0, 0.5, 1, -3), keys in [1, 10), negative keys, NaN-heavy rows, infinities and signed
+    zeros, four tie levels; the last row is ordinary keys in [0, 1)"""
+    rng = np.random.default_rng(seed)
+    rows = [np.zeros(n), np.full(n, 0.5), np.full(n, 1.0), np.full(n, -3.0),
+            1.0 + 9.0 * rng.random(n), -5.0 * rng.random(n)]
+    nan = rng.random(n)
+    nan[rng.random(n) < 0.6] = np.nan
+    rows.append(nan)
+    ext = rng.choice(np.array([np.inf, -np.inf, 0.0, -0.0, 0.3], np.float64), n)
+    rows.append(ext)
+    rows.append(rng.integers(0, 4, n) / 4.0)
+    rows.append(rng.random(n))
+    return np.ascontiguousarray(np.array(rows, np.float64).astype(np.float32))

@@ -23,6 +23,28 @@ def test_tsp_decode_fitness_large(cuda, n):
     check_tsp(B().tsp(xy), O.OracleProblem(O.TSP_COORDS, n, xy=xy), keys, cuda)
 
 
+@pytest.mark.parametrize("n", [20000, 65537])
+def test_decode_degenerate_keys_large(cuda, n):
+    """the global-memory kernel's fallback sort on keys that crowd its buckets"""
+    xy = I.tsp_coords(n, seed=5)
+    keys = I.degenerate_keys(n, seed=n)
+    check_tsp(B().tsp(xy), O.OracleProblem(O.TSP_COORDS, n, xy=xy), keys, cuda)
+
+
+def test_tspj_degenerate_keys_large(cuda):
+    """two key segments of 8200 cities and jobs (beyond shared memory) with crowded buckets;
+    travel and job times are plain uniform tables, 8201 x 8201 each"""
+    c = 8200
+    rng = np.random.default_rng(7)
+    travel = rng.random((c + 1, c + 1), dtype=np.float32) * np.float32(100.0)
+    jobs = rng.random((c + 1, c + 1), dtype=np.float32) * np.float32(100.0)
+    keys = I.degenerate_keys(2 * c, seed=8)[[0, 3, 6, 8, 9]]
+    po = O.OracleProblem(O.TSPJ, 2 * c, mat=travel, mat2=jobs)
+    fit, perm = eval_gpu(B().tspj(travel, jobs), keys, cuda)
+    np.testing.assert_array_equal(perm, O.decode_problem(po, keys))
+    np.testing.assert_array_equal(fit.view(np.uint32), O.evaluate(po, keys).view(np.uint32))
+
+
 def test_tsp_unaligned_rows_large(cuda):
     n, ld = 20001, 20003  # odd stride: scalar loads of the given keys
     xy = I.tsp_coords(n, seed=3)

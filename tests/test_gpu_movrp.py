@@ -38,6 +38,18 @@ def test_movrp_decode_objectives(cuda, n, V, overload):
     assert [c for r in routes for c in r] == (perm[0] + 1).tolist()
 
 
+@pytest.mark.parametrize("n", [300, 5000])
+def test_movrp_degenerate_keys(cuda, n):
+    """rows whose sort values crowd a few buckets (a NaN key makes the row hash, and so
+    every value, NaN; huge keys swamp the index offsets) take the bounded fallback sort"""
+    pb, po, _, _ = problems(n, seed=n + 9)
+    keys = I.degenerate_keys(n, seed=n + 10)
+    keys[4] = np.float32(3.0e30)  # every value the same float: ties by index
+    obj, perm = eval_gpu(pb, keys, cuda)
+    np.testing.assert_array_equal(perm, O.decode_problem(po, keys))
+    np.testing.assert_array_equal(obj.view(np.uint32), O.evaluate(po, keys).view(np.uint32))
+
+
 def test_movrp_engine_nsga2_bit_exact(cuda):
     n, P, G = 40, 64, 20
     pb, po, _, _ = problems(n, seed=8, vehicles=4)

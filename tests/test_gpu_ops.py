@@ -72,6 +72,30 @@ def test_tsp_ties_and_wild_keys(cuda, n):
     check_tsp(pb, po, I.wild_keys(32, n, seed=3), cuda)
 
 
+@pytest.mark.parametrize("n", [7, 1000, 5000, 12000])
+def test_decode_degenerate_keys(cuda, n):
+    """keys that crowd the value-range buckets (all equal, outside [0,1), NaN-heavy, few tie
+    levels) take the bounded fallback sort; the order is still (key, index)"""
+    xy = I.tsp_coords(n, seed=3)
+    keys = I.degenerate_keys(n, seed=n)
+    check_tsp(B().tsp(xy), O.OracleProblem(O.TSP_COORDS, n, xy=xy), keys, cuda)
+    w, v, cap = I.knap_items(n, seed=4)
+    fit, perm = eval_gpu(B().knapsack(w, v, cap, greedy=True), keys, cuda)
+    np.testing.assert_array_equal(perm, O.decode(keys))
+    np.testing.assert_array_equal(fit, O.evaluate(O.OracleProblem(O.KNAP_GREEDY, n, w=w, v=v, cap=cap), keys))
+
+
+@pytest.mark.parametrize("c", [3, 500, 2000])
+def test_tspj_degenerate_keys(cuda, c):
+    """two key segments (cities, jobs) with crowded buckets: each segment sorted on its own"""
+    travel, jobs = I.tspj_instance(c, seed=c)
+    keys = I.degenerate_keys(2 * c, seed=c + 1)
+    po = O.OracleProblem(O.TSPJ, 2 * c, mat=travel, mat2=jobs)
+    fit, perm = eval_gpu(B().tspj(travel, jobs), keys, cuda)
+    np.testing.assert_array_equal(perm, O.decode_problem(po, keys))
+    np.testing.assert_array_equal(fit.view(np.uint32), O.evaluate(po, keys).view(np.uint32))
+
+
 @pytest.mark.parametrize("n", [3, 53, 999])
 def test_tsp_unaligned_dense_rows(cuda, n):
     # the reference's dense [pop][chrom_len] layout: rows not 16-byte aligned
