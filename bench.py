@@ -926,6 +926,48 @@ def profile_op(args):
     print(json.dumps({"profile_op": True, "steps": args.steps, "best": float(d_fit.min())}))
 
 
+def profile_kernels(args):
+    """small, fixed launches of one kernel family for profiler captures (no timing):
+    rows   - the generation step and elite partition at TSP n=1000, P=2048 (as --profile-op)
+    big    - rows beyond shared memory: TSP n=65536, 512 rows (134 MB of keys) evaluated
+    knap   - greedy knapsack n=10000, 1024 rows evaluated (BASELINE's largest served knapsack)
+    nsga   - NSGA-II bi-objective TSP n=500, P=2048 engine: initialisation + generations"""
+    import torch
+
+    import brkga_b200 as B
+    what = args.profile_kernels
+    rng = np.random.default_rng(3)
+    if what == "rows":
+        return profile_op(args)
+    if what in ("big", "knap"):
+        if what == "big":
+            n, rows = 65536, 512
+            pb = B.tsp(rng.random((n, 2), dtype=np.float32))
+        else:
+            n, rows = 10000, 1024
+            w = rng.integers(1, 101, n).astype(np.int32)
+            v = rng.integers(1, 101, n).astype(np.int32)
+            pb = B.knapsack(w, v, 0.5 * float(w.sum()))
+        keys = torch.from_numpy((rng.integers(0, 1 << 24, (rows, n)) / float(1 << 24)).astype(np.float32)).cuda()
+        fit = torch.zeros(rows, dtype=torch.float32, device="cuda")
+        for _ in range(args.warmup + args.steps):
+            pb.evaluate_population(keys, fit, rows, n)
+        torch.cuda.synchronize()
+        print(json.dumps({"profile_kernels": what, "steps": args.steps, "best": float(fit.min())}))
+        return
+    if what == "nsga":
+        a = np.random.default_rng(3).random((501, 2), dtype=np.float32)
+        b = np.random.default_rng(4).random((501, 2), dtype=np.float32)
+        s = B.Solver(B.bitsp(a, b), B.params(2048, 0, 204, 0.7, 10000, seed=3))
+        s.initialize()
+        s.evolve(args.warmup + args.steps)
+        s.synchronize()
+        print(json.dumps({"profile_kernels": what, "generations": args.warmup + args.steps}))
+        s.close()
+        return
+    raise SystemExit(f"unknown kernel family {what}")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -935,6 +977,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--profile-op", action="store_true", help="operator kernels only (profiler captures)")
+    ap.add_argument("--profile-kernels", choices=["rows", "big", "knap", "nsga"],
+                    help="small fixed launches of one kernel family (profiler captures)")
     ap.add_argument("--workload", default="tsp1000",
                     choices=["tsp1000", "tsp52", "nsga", "tspj", "movrp", "operators", "batch", "serve", "quality",
                              "external"])
@@ -952,6 +996,9 @@ def main():
     args = ap.parse_args()
     if args.profile_op:
         profile_op(args)
+        return
+    if args.profile_kernels:
+        profile_kernels(args)
         return
     if args.workload != "tsp1000":
         run_workload(args)

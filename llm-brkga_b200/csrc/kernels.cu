@@ -349,21 +349,29 @@ __device__ float knap_greedy(const int32_t* perm, int n, const int32_t* __restri
     if (f == 0 && t == 0) shared_misc[0] = 0;
     __syncthreads();
     long long vt = 0;
-    if (t < 32) {
-        long long r = C - shared_misc[0];
-        for (int b = (int)f + 1; b < n; b += 32) {
-            const int pos = b + t;
-            const int2 x = (pos < n) ? wv[pos] : make_int2(0, 0);
-            const long long wl = (pos < n) ? (long long)x.x : LLONG_MAX;
-            const long long vl = (long long)x.y;
-            int cur = 0;
-            for (;;) {
-                const unsigned mask = __ballot_sync(0xffffffffu, pos < n && t >= cur && wl <= r);
-                if (!mask) break;
-                const int j = __ffs(mask) - 1;
-                r -= __shfl_sync(0xffffffffu, wl, j);
-                vt += __shfl_sync(0xffffffffu, vl, j);
-                cur = j + 1;
+    if (t < 32 && f < n) {
+        // the spare capacity left by the prefix is below the weight of the item that broke
+        // it, so it fits in 32 bits from here on; four chunks of 32 items are loaded before
+        // they are walked, so the walk waits for one load round per 128 items
+        int r = (int)(C - shared_misc[0]);
+        for (int b0 = (int)f + 1; b0 < n; b0 += 128) {
+            int2 x[4];
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const int pos = b0 + 32 * c + t;
+                x[c] = (pos < n) ? wv[pos] : make_int2(INT_MAX, 0);
+            }
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                int cur = 0;
+                for (;;) {
+                    const unsigned mask = __ballot_sync(0xffffffffu, t >= cur && x[c].x <= r);
+                    if (!mask) break;
+                    const int j = __ffs(mask) - 1;
+                    r -= __shfl_sync(0xffffffffu, x[c].x, j);
+                    vt += __shfl_sync(0xffffffffu, x[c].y, j);
+                    cur = j + 1;
+                }
             }
         }
     }
@@ -1265,8 +1273,11 @@ __global__ void __launch_bounds__(RK_THREADS) rank_kernel(RankArgs a) {
         P = d->P;
         mx = d->maximize;
         m = d->m;
+        // both buffer pointers are read with the buffer index (one round trip, not two)
+        const float* f0 = d->fit[0];
+        const float* f1 = d->fit[1];
         buf = a.flip ? (d->cur ^ 1) : d->cur;
-        f = d->fit[buf];
+        f = buf ? f1 : f0;
         sorted = d->sorted;
         gen_new = a.flip ? d->gen + 1 : d->gen;
     } else {
