@@ -124,14 +124,19 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def profile_traffic():
-    """DRAM bytes per launch of the row kernel from the committed ncu summary, or None"""
+def profile_figure(key):
+    """a figure of the row kernel's committed ncu summary (`key: value` line), or None"""
     try:
         txt = open(PROFILE).read()
     except OSError:
         return None
-    m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", txt)
+    m = re.search(key + r":\s*([0-9.eE+]+)", txt)
     return float(m.group(1)) if m else None
+
+
+def profile_traffic():
+    """DRAM bytes per launch of the row kernel from the committed ncu summary, or None"""
+    return profile_figure("traffic_bytes_per_launch")
 
 
 # ---------------------------------------------------------------------------------------
@@ -347,7 +352,12 @@ def run_ours(args, rank, world):
                          "engine_tile": {"threads": s_info[0], "groups": s_info[1], "grid": s_info[2],
                                          "coords_in_smem": bool(s_info[3])},
                          "algorithmic_bytes_per_launch": alg, "kernel_ms": row_ms, "peak_kind": peak_kind,
-                         "sort_kernel_ms": sort_ms},
+                         "sort_kernel_ms": sort_ms,
+                         # the in-block argsort's bound: shared-memory pipe utilisation of the
+                         # same kernel (ncu, wavefronts as % of the per-SM peak over the
+                         # kernel's elapsed time)
+                         "smem": {"wavefront_pct_of_peak": profile_figure("smem_wavefront_pct_of_peak"),
+                                  "source": "profiles/row_kernel_tsp_n1000_p2048.md"}},
             "gpu_launches": 2 * args.steps * gps,
             # rows decoded and evaluated per generation: children and mutants (elites keep
             # their fitness, as the reference's host path does)
