@@ -726,6 +726,10 @@ __global__ void __cluster_dims__(kPeelCluster, 1, 1) __launch_bounds__(kPeelThre
     cluster.sync();
     constexpr int NW = kPeelCluster * kPeelWords;
     int survivors = 0, rest = 0;
+    // thread 0 of the cluster's first CTA records the front table (start of each front in
+    // rank order, the cut front) for the grid-wide crowding and placement of mode 0
+    int32_t* const ft = (crank == 0 && t == 0) ? d.nft : nullptr;
+    int start = 0;
     for (int k = 0; k < N; ++k) {
         // the whole front k, gathered from every CTA of the cluster
         if (t < NW) {
@@ -739,11 +743,26 @@ __global__ void __cluster_dims__(kPeelCluster, 1, 1) __launch_bounds__(kPeelThre
         if (t < NW)
             for (uint32_t x = Ffull[t]; x; x &= x - 1) list[base++] = (uint16_t)(32 * t + __ffs(x) - 1);
         __syncthreads();
-        if (nf == 0) break;  // every CTA sees the same front
+        if (nf == 0) {  // every CTA sees the same front
+            if (ft) {
+                ft[0] = k;
+                ft[1] = -1;
+                ft[2 + k] = start;
+            }
+            break;
+        }
+        if (ft) ft[2 + k] = start;
+        start += (int)nf;
         if (mode == 0) {
             survivors += (k == 0) ? 2 * (int)nf : (int)nf;
             if (survivors > d.P) {
                 rest = k + 1;
+                if (ft) {  // the cut front k, then the points left as one last front
+                    ft[1] = k;
+                    ft[3 + k] = start;
+                    ft[4 + k] = N;
+                    ft[0] = (start < N) ? k + 2 : k + 1;
+                }
                 break;
             }
         }
@@ -881,11 +900,123 @@ __global__ void __launch_bounds__(kOrdThreads) nsga_order_kernel(PopDesc* dd, in
     for (int j = lane; j < N; j += 32) cnt += (okeys[j] < me) ? 1 : 0;
 #pragma unroll
     for (int off = 16; off >= 1; off >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, off);
-    if (lane == 0 && i < N) d.nord[(size_t)o * 2 * d.P + cnt] = i;
+    if (lane == 0 && i < N) {
+        d.nord[(size_t)o * 2 * d.P + cnt] = i;
+        if (d.npos) d.npos[(size_t)o * 2 * d.P + i] = cnt;
+    }
+}
+
+// Mode 0 (the pool of a generation), grid-wide, one thread per pool point:
+//  - its crowding distance from the two orders and the peel's front table, with the float
+//    operations of crowding_pass in the same order (objective 0, then 1; a first-front
+//    point adds the terms of its two list copies, (v - prev) / range then (next - v) /
+//    range; a front extreme is +inf);
+//  - survivors of the whole fronts before the cut (core/population.hpp:491-517): front r
+//    starts at survivor entry first(r) + size(0) (rank-0 points count twice), members in
+//    objective-1 order, a rank-0 point as two adjacent entries;
+//  - the smallest first objective among them (atomic minimum of order keys).
+constexpr int kCrowdThreads = 256;
+
+__global__ void __launch_bounds__(kCrowdThreads) nsga_crowd_place_kernel(PopDesc* dd) {
+    const PopDesc& d = dd[blockIdx.y];
+    if (!select_active(d, 0)) return;
+    const int N = 2 * d.P;
+    const int i = blockIdx.x * kCrowdThreads + threadIdx.x;
+    if (i >= N) return;
+    const float* __restrict__ f = d.fit[d.cur];
+    const int32_t* __restrict__ ft = d.nft;
+    const int r = __ldg(d.domcnt + i);
+    const int fs = __ldg(ft + 2 + r), fe = __ldg(ft + 3 + r) - 1, size = fe - fs + 1;
+    const int p0 = __ldg(d.npos + i), p1 = __ldg(d.npos + N + i);
+    float cd = 0.0f;
+#pragma unroll
+    for (int o = 0; o < 2; ++o) {
+        const int32_t* __restrict__ ord = d.nord + (size_t)o * N;
+        const int p = o ? p1 : p0;
+        const bool edge = (r == 0) ? (size == 1 || p == fs || p == fe) : (size <= 2 || p == fs || p == fe);
+        if (edge) {
+            cd = INFINITY;
+            continue;
+        }
+        const float range = __fsub_rn(__ldg(f + 2 * __ldg(ord + fe) + o), __ldg(f + 2 * __ldg(ord + fs) + o));
+        if (range > 0.0f) {
+            const float vp = __ldg(f + 2 * __ldg(ord + p - 1) + o), vn = __ldg(f + 2 * __ldg(ord + p + 1) + o);
+            if (r == 0) {
+                const float v = __ldg(f + 2 * i + o);
+                cd = __fadd_rn(__fadd_rn(cd, __fdiv_rn(__fsub_rn(v, vp), range)), __fdiv_rn(__fsub_rn(vn, v), range));
+            } else {
+                cd = __fadd_rn(cd, __fdiv_rn(__fsub_rn(vn, vp), range));
+            }
+        }
+    }
+    d.ncdp[i] = cd;
+    const int cut = __ldg(ft + 1);
+    if (r < cut) {
+        const int q = (r == 0) ? 2 * (p1 - fs) : fs + __ldg(ft + 3) + (p1 - fs);
+        d.nsel[q] = i;
+        d.nrank[q] = r;
+        d.ncd[q] = cd;
+        if (r == 0) {
+            d.nsel[q + 1] = i;
+            d.nrank[q + 1] = r;
+            d.ncd[q + 1] = cd;
+        }
+        atomicMin(d.nfmin, okey(__ldg(f + 2 * i)));
+    }
+}
+
+// Mode 0, one CTA per population: the cut front's entries sorted by (crowding descending,
+// index, copy), the first P - (entries before it) taken; then the generation's history
+// entry (the survivors' smallest first objective) and the minimum's reset.
+__global__ void __launch_bounds__(kNsgaBlock, 1) nsga_cut_kernel(PopDesc* dd) {
+    extern __shared__ unsigned long long ckeys[];
+    __shared__ float redf[32];
+    PopDesc& d = dd[blockIdx.x];
+    if (!select_active(d, 0)) return;
+    const int t = threadIdx.x;
+    const int P = d.P, N = 2 * P;
+    const int32_t* __restrict__ ft = d.nft;
+    const float* __restrict__ f = d.fit[d.cur];
+    const int cut = ft[1];
+    const int fs = ft[2 + cut], nc = ft[3 + cut] - fs;
+    const int mult = (cut == 0) ? 2 : 1;
+    const int rb = (cut == 0) ? 0 : fs + ft[3];
+    const int take = P - rb, E = nc * mult, K2 = npow2(E);
+    const int32_t* __restrict__ ord1 = d.nord + N;
+    for (int e = t; e < K2; e += kNsgaBlock) {
+        unsigned long long kk = ~0ull;
+        if (e < E) {
+            const int i = __ldg(ord1 + fs + e / mult);
+            kk = ((unsigned long long)cd_key(__ldg(d.ncdp + i)) << 32) | ((unsigned long long)i << 1) |
+                 (unsigned long long)(e % mult);
+        }
+        ckeys[e] = kk;
+    }
+    __syncthreads();
+    bitonic_u64<kNsgaBlock>(ckeys, K2);
+    float fmin = INFINITY;
+    for (int k = t; k < take; k += kNsgaBlock) {
+        const int i = (int)((ckeys[k] >> 1) & 0x7FFFu);
+        const int q = rb + k;
+        d.nsel[q] = i;
+        d.nrank[q] = cut;
+        d.ncd[q] = __ldg(d.ncdp + i);
+        fmin = fminf(fmin, __ldg(f + 2 * i));
+    }
+    fmin = block_min_f(fmin, redf);
+    if (t == 0) {
+        const uint32_t k = *d.nfmin;
+        if (k != 0xFFFFFFFFu) fmin = fminf(fmin, __uint_as_float((k & 0x80000000u) ? (k & 0x7FFFFFFFu) : ~k));
+        *d.nfmin = 0xFFFFFFFFu;
+        if (d.history) {
+            const uint32_t g = d.gen + 1;
+            if ((int)g < d.hist_cap) d.history[g] = fmin;
+        }
+    }
 }
 
 // crowding and (mode 0) survivors from the ranks and orders above; one CTA per population
-__global__ void __launch_bounds__(kNsgaBlock) nsga_select_kernel(PopDesc* dd, int mode) {
+__global__ void __launch_bounds__(kNsgaBlock, 1) nsga_select_kernel(PopDesc* dd, int mode) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ uint32_t wt32[32];
     __shared__ float redf[32];
@@ -1109,6 +1240,8 @@ cudaError_t nsga_prepare(int maxP) {
         e = raise_smem_limit(reinterpret_cast<const void*>(nsga_order_kernel), (size_t)2 * maxP * 8);
     if (e == cudaSuccess)
         e = raise_smem_limit(reinterpret_cast<const void*>(near_build_kernel), (size_t)((maxP + 31) / 32) * 32 * 8);
+    if (e == cudaSuccess)
+        e = raise_smem_limit(reinterpret_cast<const void*>(nsga_cut_kernel), (size_t)npow2(4 * maxP) * 8);
     return e;
 }
 
@@ -1141,6 +1274,14 @@ cudaError_t nsga_enqueue_select(PopDesc* dd, int npops, int maxP, int mode, cuda
     nsga_order_kernel<<<dim3((maxN + kOrdPerCta - 1) / kOrdPerCta, 2, npops), kOrdThreads, (size_t)maxN * 8, st>>>(
         dd, mode);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (mode == 0) {
+        // a generation's pool: crowding and whole fronts over the grid, then the cut front
+        nsga_crowd_place_kernel<<<dim3((maxN + kCrowdThreads - 1) / kCrowdThreads, npops), kCrowdThreads, 0, st>>>(
+            dd);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        nsga_cut_kernel<<<npops, kNsgaBlock, (size_t)npow2(2 * maxN) * 8, st>>>(dd);
+        return cudaGetLastError();
+    }
     nsga_select_kernel<<<npops, kNsgaBlock, sel_smem_bytes(maxN), st>>>(dd, mode);
     return cudaGetLastError();
 }
@@ -1188,6 +1329,18 @@ int32_t nsga_alloc(PopDesc& d, int P, double mut_rate, int div_interval, int Mn,
     d.nu = (int32_t*)p;
     if ((st = get((size_t)2 * N * 4, &p)) != BRKGA_OK) return st;
     d.nord = (int32_t*)p;
+    if ((st = get((size_t)2 * N * 4, &p)) != BRKGA_OK) return st;
+    d.npos = (int32_t*)p;
+    if ((st = get((size_t)(N + 4) * 4, &p)) != BRKGA_OK) return st;
+    d.nft = (int32_t*)p;
+    if ((st = get((size_t)N * 4, &p)) != BRKGA_OK) return st;
+    d.ncdp = (float*)p;
+    if ((st = get(16, &p)) != BRKGA_OK) return st;
+    d.nfmin = (uint32_t*)p;
+    if (cudaMemsetAsync(d.nfmin, 0xFF, 4, stream) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(BRKGA_ERR_CUDA, "NSGA-II state initialisation");
+    }
     d.domW = W;
     d.Mn = Mn;
     d.mutT = prob_threshold(mut_rate);
