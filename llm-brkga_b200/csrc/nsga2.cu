@@ -752,6 +752,8 @@ __global__ void __cluster_dims__(kPeelCluster, 1, 1) __launch_bounds__(kPeelThre
             break;
         }
         if (ft) ft[2 + k] = start;
+        if (crank == 0 && d.nlist)
+            for (int j = t; j < (int)nf; j += kPeelThreads) d.nlist[start + j] = list[j];
         start += (int)nf;
         if (mode == 0) {
             survivors += (k == 0) ? 2 * (int)nf : (int)nf;
@@ -900,49 +902,141 @@ __global__ void __launch_bounds__(kOrdThreads) nsga_order_kernel(PopDesc* dd, in
     for (int j = lane; j < N; j += 32) cnt += (okeys[j] < me) ? 1 : 0;
 #pragma unroll
     for (int off = 16; off >= 1; off >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, off);
-    if (lane == 0 && i < N) {
-        d.nord[(size_t)o * 2 * d.P + cnt] = i;
-        if (d.npos) d.npos[(size_t)o * 2 * d.P + i] = cnt;
-    }
+    if (lane == 0 && i < N) d.nord[(size_t)o * 2 * d.P + cnt] = i;
 }
 
-// Mode 0 (the pool of a generation), grid-wide, one thread per pool point:
-//  - its crowding distance from the two orders and the peel's front table, with the float
-//    operations of crowding_pass in the same order (objective 0, then 1; a first-front
-//    point adds the terms of its two list copies, (v - prev) / range then (next - v) /
-//    range; a front extreme is +inf);
-//  - survivors of the whole fronts before the cut (core/population.hpp:491-517): front r
-//    starts at survivor entry first(r) + size(0) (rank-0 points count twice), members in
-//    objective-1 order, a rank-0 point as two adjacent entries;
-//  - the smallest first objective among them (atomic minimum of order keys).
-constexpr int kCrowdThreads = 256;
+// Mode 0 (the pool of a generation), one warp per pool point, over the members of its own
+// front only (the peel's lists): its position in the front in each objective order, its
+// neighbours and the front's extremes in both orders, so its crowding distance (the float
+// operations of crowding_pass in the same order) and, for whole fronts before the cut, its
+// survivor entries: front r starts at survivor entry first(r) + size(0) (rank-0 points
+// count twice), members in objective-1 order, a rank-0 point as two adjacent entries; and
+// the smallest first objective among them (atomic minimum of order keys).  Keys are
+// (okey(value) << 32 | index); a value is recovered from its key.  CTAs take the points in
+// rank order, kFrontWarps at a time, so a CTA's warps share a front, whose members' keys
+// the CTA stages in shared memory once (a warp whose point lies in a later front reads
+// that front from global memory).  Points of the last front of a peel stopped at the cut
+// are never selected and are skipped.  Work: the sum of the squared front sizes instead
+// of N^2 per objective.
+constexpr int kFrontWarps = 8;
 
-__global__ void __launch_bounds__(kCrowdThreads) nsga_crowd_place_kernel(PopDesc* dd) {
+__device__ __forceinline__ float key_value(unsigned long long k) {
+    const uint32_t o = (uint32_t)(k >> 32);
+    return __uint_as_float((o & 0x80000000u) ? (o & 0x7FFFFFFFu) : ~o);
+}
+
+// one member's two keys -> the running position, neighbours and extremes of the point
+struct FrontScan {
+    unsigned long long me0, me1;
+    int below0 = 0, below1 = 0;
+    unsigned long long lo0 = 0ull, hi0 = ~0ull, lo1 = 0ull, hi1 = ~0ull;  // neighbours (0 / ~0: none)
+    unsigned long long mn0 = ~0ull, mx0 = 0ull, mn1 = ~0ull, mx1 = 0ull;  // front extremes
+    __device__ __forceinline__ void add(unsigned long long k0, unsigned long long k1) {
+        below0 += (k0 < me0) ? 1 : 0;
+        below1 += (k1 < me1) ? 1 : 0;
+        if (k0 < me0 && k0 > lo0) lo0 = k0;
+        if (k0 > me0 && k0 < hi0) hi0 = k0;
+        if (k1 < me1 && k1 > lo1) lo1 = k1;
+        if (k1 > me1 && k1 < hi1) hi1 = k1;
+        mn0 = k0 < mn0 ? k0 : mn0;
+        mx0 = k0 > mx0 ? k0 : mx0;
+        mn1 = k1 < mn1 ? k1 : mn1;
+        mx1 = k1 > mx1 ? k1 : mx1;
+    }
+    __device__ __forceinline__ void reduce() {
+#pragma unroll
+        for (int off = 16; off >= 1; off >>= 1) {
+            below0 += __shfl_xor_sync(0xffffffffu, below0, off);
+            below1 += __shfl_xor_sync(0xffffffffu, below1, off);
+            unsigned long long x;
+            x = __shfl_xor_sync(0xffffffffu, lo0, off);
+            lo0 = x > lo0 ? x : lo0;
+            x = __shfl_xor_sync(0xffffffffu, hi0, off);
+            hi0 = x < hi0 ? x : hi0;
+            x = __shfl_xor_sync(0xffffffffu, lo1, off);
+            lo1 = x > lo1 ? x : lo1;
+            x = __shfl_xor_sync(0xffffffffu, hi1, off);
+            hi1 = x < hi1 ? x : hi1;
+            x = __shfl_xor_sync(0xffffffffu, mn0, off);
+            mn0 = x < mn0 ? x : mn0;
+            x = __shfl_xor_sync(0xffffffffu, mx0, off);
+            mx0 = x > mx0 ? x : mx0;
+            x = __shfl_xor_sync(0xffffffffu, mn1, off);
+            mn1 = x < mn1 ? x : mn1;
+            x = __shfl_xor_sync(0xffffffffu, mx1, off);
+            mx1 = x > mx1 ? x : mx1;
+        }
+    }
+};
+
+__device__ __forceinline__ unsigned long long obj_key(float v, int j) {
+    return ((unsigned long long)okey(v) << 32) | (uint32_t)j;
+}
+
+__global__ void __launch_bounds__(kFrontWarps * 32) nsga_front_crowd_kernel(PopDesc* dd) {
+    extern __shared__ uint2 fkeys[];  // [front size]: the staged front's (okey0, okey1)
+    __shared__ int s_front[3];        // staged front: rank, first position, size
     const PopDesc& d = dd[blockIdx.y];
     if (!select_active(d, 0)) return;
     const int N = 2 * d.P;
-    const int i = blockIdx.x * kCrowdThreads + threadIdx.x;
-    if (i >= N) return;
-    const float* __restrict__ f = d.fit[d.cur];
     const int32_t* __restrict__ ft = d.nft;
+    const int cut = __ldg(ft + 1);
+    const int end = (cut >= 0) ? __ldg(ft + 3 + cut) : N;  // positions of the fronts up to the cut
+    const int pos0 = blockIdx.x * kFrontWarps;
+    if (pos0 >= end) return;
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    const float2* __restrict__ f2 = reinterpret_cast<const float2*>(d.fit[d.cur]);
+    const int32_t* __restrict__ list = d.nlist;
+    if (t == 0) {
+        const int r0 = __ldg(d.domcnt + __ldg(list + pos0));
+        s_front[0] = r0;
+        s_front[1] = __ldg(ft + 2 + r0);
+        s_front[2] = __ldg(ft + 3 + r0) - s_front[1];
+    }
+    __syncthreads();
+    const int r0 = s_front[0], fs0 = s_front[1], size0 = s_front[2];
+    staged<kFrontWarps * 32, 4>(
+        size0, [&](int j) { return __ldg(f2 + __ldg(list + fs0 + j)); },
+        [&](int j, float2 v) { fkeys[j] = make_uint2(okey(v.x), okey(v.y)); });
+    __syncthreads();
+    const int pos = pos0 + w;
+    if (pos >= end) return;
+    const int i = __ldg(list + pos);
     const int r = __ldg(d.domcnt + i);
-    const int fs = __ldg(ft + 2 + r), fe = __ldg(ft + 3 + r) - 1, size = fe - fs + 1;
-    const int p0 = __ldg(d.npos + i), p1 = __ldg(d.npos + N + i);
+    const int fs = __ldg(ft + 2 + r), size = __ldg(ft + 3 + r) - fs;
+    const float2 vi = __ldg(f2 + i);
+    FrontScan sc;
+    sc.me0 = obj_key(vi.x, i);
+    sc.me1 = obj_key(vi.y, i);
+    if (r == r0) {
+        for (int j = lane; j < size; j += 32) {
+            const uint2 k = fkeys[j];
+            const int m = __ldg(list + fs + j);
+            sc.add(((unsigned long long)k.x << 32) | (uint32_t)m, ((unsigned long long)k.y << 32) | (uint32_t)m);
+        }
+    } else {
+        for (int j = lane; j < size; j += 32) {
+            const int m = __ldg(list + fs + j);
+            const float2 v = __ldg(f2 + m);
+            sc.add(obj_key(v.x, m), obj_key(v.y, m));
+        }
+    }
+    sc.reduce();
+    if (lane != 0) return;
     float cd = 0.0f;
 #pragma unroll
     for (int o = 0; o < 2; ++o) {
-        const int32_t* __restrict__ ord = d.nord + (size_t)o * N;
-        const int p = o ? p1 : p0;
-        const bool edge = (r == 0) ? (size == 1 || p == fs || p == fe) : (size <= 2 || p == fs || p == fe);
+        const int p = o ? sc.below1 : sc.below0;  // position inside the front
+        const bool edge = (r == 0) ? (size == 1 || p == 0 || p == size - 1) : (size <= 2 || p == 0 || p == size - 1);
         if (edge) {
             cd = INFINITY;
             continue;
         }
-        const float range = __fsub_rn(__ldg(f + 2 * __ldg(ord + fe) + o), __ldg(f + 2 * __ldg(ord + fs) + o));
+        const float range = __fsub_rn(key_value(o ? sc.mx1 : sc.mx0), key_value(o ? sc.mn1 : sc.mn0));
         if (range > 0.0f) {
-            const float vp = __ldg(f + 2 * __ldg(ord + p - 1) + o), vn = __ldg(f + 2 * __ldg(ord + p + 1) + o);
+            const float vp = key_value(o ? sc.lo1 : sc.lo0), vn = key_value(o ? sc.hi1 : sc.hi0);
             if (r == 0) {
-                const float v = __ldg(f + 2 * i + o);
+                const float v = key_value(o ? sc.me1 : sc.me0);
                 cd = __fadd_rn(__fadd_rn(cd, __fdiv_rn(__fsub_rn(v, vp), range)), __fdiv_rn(__fsub_rn(vn, v), range));
             } else {
                 cd = __fadd_rn(cd, __fdiv_rn(__fsub_rn(vn, vp), range));
@@ -950,9 +1044,8 @@ __global__ void __launch_bounds__(kCrowdThreads) nsga_crowd_place_kernel(PopDesc
         }
     }
     d.ncdp[i] = cd;
-    const int cut = __ldg(ft + 1);
     if (r < cut) {
-        const int q = (r == 0) ? 2 * (p1 - fs) : fs + __ldg(ft + 3) + (p1 - fs);
+        const int q = (r == 0) ? 2 * sc.below1 : fs + __ldg(ft + 3) + sc.below1;
         d.nsel[q] = i;
         d.nrank[q] = r;
         d.ncd[q] = cd;
@@ -961,7 +1054,7 @@ __global__ void __launch_bounds__(kCrowdThreads) nsga_crowd_place_kernel(PopDesc
             d.nrank[q + 1] = r;
             d.ncd[q + 1] = cd;
         }
-        atomicMin(d.nfmin, okey(__ldg(f + 2 * i)));
+        atomicMin(d.nfmin, (uint32_t)(sc.me0 >> 32));
     }
 }
 
@@ -974,7 +1067,7 @@ __global__ void __launch_bounds__(kNsgaBlock, 1) nsga_cut_kernel(PopDesc* dd) {
     PopDesc& d = dd[blockIdx.x];
     if (!select_active(d, 0)) return;
     const int t = threadIdx.x;
-    const int P = d.P, N = 2 * P;
+    const int P = d.P;
     const int32_t* __restrict__ ft = d.nft;
     const float* __restrict__ f = d.fit[d.cur];
     const int cut = ft[1];
@@ -982,11 +1075,11 @@ __global__ void __launch_bounds__(kNsgaBlock, 1) nsga_cut_kernel(PopDesc* dd) {
     const int mult = (cut == 0) ? 2 : 1;
     const int rb = (cut == 0) ? 0 : fs + ft[3];
     const int take = P - rb, E = nc * mult, K2 = npow2(E);
-    const int32_t* __restrict__ ord1 = d.nord + N;
+    const int32_t* __restrict__ mem = d.nlist + fs;
     for (int e = t; e < K2; e += kNsgaBlock) {
         unsigned long long kk = ~0ull;
         if (e < E) {
-            const int i = __ldg(ord1 + fs + e / mult);
+            const int i = __ldg(mem + e / mult);
             kk = ((unsigned long long)cd_key(__ldg(d.ncdp + i)) << 32) | ((unsigned long long)i << 1) |
                  (unsigned long long)(e % mult);
         }
@@ -1242,6 +1335,8 @@ cudaError_t nsga_prepare(int maxP) {
         e = raise_smem_limit(reinterpret_cast<const void*>(near_build_kernel), (size_t)((maxP + 31) / 32) * 32 * 8);
     if (e == cudaSuccess)
         e = raise_smem_limit(reinterpret_cast<const void*>(nsga_cut_kernel), (size_t)npow2(4 * maxP) * 8);
+    if (e == cudaSuccess)
+        e = raise_smem_limit(reinterpret_cast<const void*>(nsga_front_crowd_kernel), (size_t)2 * maxP * sizeof(uint2));
     return e;
 }
 
@@ -1271,17 +1366,18 @@ cudaError_t nsga_enqueue_select(PopDesc* dd, int npops, int maxP, int mode, cuda
     if (e != cudaSuccess) return e;
     nsga_peel_cluster_kernel<<<npops * kPeelCluster, kPeelThreads, 0, st>>>(dd, mode);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    nsga_order_kernel<<<dim3((maxN + kOrdPerCta - 1) / kOrdPerCta, 2, npops), kOrdThreads, (size_t)maxN * 8, st>>>(
-        dd, mode);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (mode == 0) {
-        // a generation's pool: crowding and whole fronts over the grid, then the cut front
-        nsga_crowd_place_kernel<<<dim3((maxN + kCrowdThreads - 1) / kCrowdThreads, npops), kCrowdThreads, 0, st>>>(
-            dd);
+        // a generation's pool: crowding and whole fronts from each point's own front, then
+        // the cut front
+        nsga_front_crowd_kernel<<<dim3((maxN + kFrontWarps - 1) / kFrontWarps, npops), kFrontWarps * 32,
+                                  (size_t)maxN * sizeof(uint2), st>>>(dd);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         nsga_cut_kernel<<<npops, kNsgaBlock, (size_t)npow2(2 * maxN) * 8, st>>>(dd);
         return cudaGetLastError();
     }
+    nsga_order_kernel<<<dim3((maxN + kOrdPerCta - 1) / kOrdPerCta, 2, npops), kOrdThreads, (size_t)maxN * 8, st>>>(
+        dd, mode);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
     nsga_select_kernel<<<npops, kNsgaBlock, sel_smem_bytes(maxN), st>>>(dd, mode);
     return cudaGetLastError();
 }
@@ -1329,12 +1425,12 @@ int32_t nsga_alloc(PopDesc& d, int P, double mut_rate, int div_interval, int Mn,
     d.nu = (int32_t*)p;
     if ((st = get((size_t)2 * N * 4, &p)) != BRKGA_OK) return st;
     d.nord = (int32_t*)p;
-    if ((st = get((size_t)2 * N * 4, &p)) != BRKGA_OK) return st;
-    d.npos = (int32_t*)p;
     if ((st = get((size_t)(N + 4) * 4, &p)) != BRKGA_OK) return st;
     d.nft = (int32_t*)p;
     if ((st = get((size_t)N * 4, &p)) != BRKGA_OK) return st;
     d.ncdp = (float*)p;
+    if ((st = get((size_t)N * 4, &p)) != BRKGA_OK) return st;
+    d.nlist = (int32_t*)p;
     if ((st = get(16, &p)) != BRKGA_OK) return st;
     d.nfmin = (uint32_t*)p;
     if (cudaMemsetAsync(d.nfmin, 0xFF, 4, stream) != cudaSuccess) {
