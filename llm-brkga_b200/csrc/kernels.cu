@@ -283,32 +283,49 @@ __device__ __forceinline__ void canon_sum(int nedges, EdgeF edge, float* red, fl
     }
 }
 
+// exclusive block scan of two 64-bit values at once (red: 64 entries)
 template <int BLOCK>
-__device__ __forceinline__ long long block_excl_scan_ll(long long v, long long* red, long long* total) {
+__device__ __forceinline__ void block_excl_scan_ll2(long long a, long long b, long long* red, long long* ea,
+                                                    long long* eb, long long* ta, long long* tb) {
     constexpr int NW = BLOCK / 32;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    long long x = v;
+    long long x = a, y = b;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-        const long long y = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= o) x += y;
+        const long long xu = __shfl_up_sync(0xffffffffu, x, o);
+        const long long yu = __shfl_up_sync(0xffffffffu, y, o);
+        if (lane >= o) {
+            x += xu;
+            y += yu;
+        }
     }
-    if (lane == 31) red[w] = x;
+    if (lane == 31) {
+        red[w] = x;
+        red[32 + w] = y;
+    }
     __syncthreads();
     if (w == 0) {
-        long long s = (lane < NW) ? red[lane] : 0ll;
+        long long sx = (lane < NW) ? red[lane] : 0ll, sy = (lane < NW) ? red[32 + lane] : 0ll;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            const long long y = __shfl_up_sync(0xffffffffu, s, o);
-            if (lane >= o) s += y;
+            const long long xu = __shfl_up_sync(0xffffffffu, sx, o);
+            const long long yu = __shfl_up_sync(0xffffffffu, sy, o);
+            if (lane >= o) {
+                sx += xu;
+                sy += yu;
+            }
         }
-        if (lane < NW) red[lane] = s;
+        if (lane < NW) {
+            red[lane] = sx;
+            red[32 + lane] = sy;
+        }
     }
     __syncthreads();
-    const long long base = (w > 0) ? red[w - 1] : 0ll;
-    *total = red[NW - 1];
+    *ea = ((w > 0) ? red[w - 1] : 0ll) + x - a;
+    *eb = ((w > 0) ? red[32 + w - 1] : 0ll) + y - b;
+    *ta = red[NW - 1];
+    *tb = red[32 + NW - 1];
     __syncthreads();
-    return base + x - v;
 }
 
 // knapsack greedy in key order: prefix of the sorted items that fits, then a
@@ -328,26 +345,34 @@ __device__ float knap_greedy(const int32_t* perm, int n, const int32_t* __restri
     __syncthreads();
     const int ch = (n + BLOCK - 1) / BLOCK;
     const int p0 = t * ch, p1 = min(n, p0 + ch);
-    long long ws = 0;
-    for (int p = p0; p < p1; ++p) ws += wv[p].x;
-    long long tot;
-    const long long base = block_excl_scan_ll<BLOCK>(ws, red, &tot);
-    // positions whose inclusive prefix weight stays <= C
-    long long S = base, cnt = 0, val = 0, lastS = -1;
+    long long ws = 0, vs = 0;
     for (int p = p0; p < p1; ++p) {
         const int2 x = wv[p];
-        S += x.x;
-        if (S <= C) {
-            ++cnt;
-            val += x.y;
-            lastS = S;
-        }
+        ws += x.x;
+        vs += x.y;
     }
-    const long long f = block_sum_ll<BLOCK>(cnt, red);
-    const long long v0 = block_sum_ll<BLOCK>(val, red);
-    if (f > 0 && p0 < p1 && f - 1 >= p0 && f - 1 < p1) shared_misc[0] = lastS;
-    if (f == 0 && t == 0) shared_misc[0] = 0;
+    long long S, V, totw, totv;
+    block_excl_scan_ll2<BLOCK>(ws, vs, red, &S, &V, &totw, &totv);
+    // the prefix: positions whose inclusive prefix weight stays <= C.  Weights are >= 0, so
+    // the prefix weight only grows and exactly one position breaks it (none when every item
+    // fits); the thread holding it records the prefix's weight, length and value
+    if (t == 0 && totw <= C) {
+        shared_misc[0] = totw;
+        shared_misc[1] = n;
+        shared_misc[2] = totv;
+    }
+    for (int p = p0; p < p1; ++p) {
+        const int2 x = wv[p];
+        if (S <= C && S + x.x > C) {
+            shared_misc[0] = S;
+            shared_misc[1] = p;
+            shared_misc[2] = V;
+        }
+        S += x.x;
+        V += x.y;
+    }
     __syncthreads();
+    const long long f = shared_misc[1], v0 = shared_misc[2];
     long long vt = 0;
     if (t < 32 && f < n) {
         // the spare capacity left by the prefix is below the weight of the item that broke
@@ -579,7 +604,7 @@ __global__ void __launch_bounds__(BLOCK, RowResidency<BLOCK, G>::value) row_kern
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ PopDesc sd;
     __shared__ uint32_t warp_tot[32];
-    __shared__ long long red_ll[32];
+    __shared__ long long red_ll[64];
     __shared__ float red_f[32];
     __shared__ long long misc[4];
 
@@ -965,7 +990,7 @@ __global__ void __launch_bounds__(kBigBlock) row_kernel_big(RowLaunch L) {
     constexpr int BLOCK = kBigBlock;
     __shared__ PopDesc sd;
     __shared__ uint32_t warp_tot[32];
-    __shared__ long long red_ll[32];
+    __shared__ long long red_ll[64];
     __shared__ float red_f[32];
     __shared__ long long misc[4];
     const int t = threadIdx.x;
