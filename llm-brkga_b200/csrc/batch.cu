@@ -65,7 +65,27 @@ struct Group {
     // batch of same-kind instances, +12%; 1 keeps the served mix of kinds and sizes
     // balanced, 8 there cost 8%)
     int task_group = 1;
+    int32_t* work = nullptr;  // the row kernel's dynamic dealing counter (launches on `stream`)
 };
+
+// the group's stream and its zeroed row-dealing counter
+static int32_t group_start(Group& g) {
+    cudaError_t e = cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return cuda_fail(e, "stream");
+    int32_t st = dev_alloc((void**)&g.work, 8, g.stream);
+    if (st != BRKGA_OK) return st;
+    if ((e = cudaMemsetAsync(g.work, 0, 8, g.stream)) != cudaSuccess) return cuda_fail(e, "work counter");
+    return BRKGA_OK;
+}
+
+static void group_stop(Group& g) {
+    if (!g.stream) return;
+    if (g.work) dev_free(g.work, g.stream);
+    g.work = nullptr;
+    cudaStreamSynchronize(g.stream);
+    cudaStreamDestroy(g.stream);
+    g.stream = nullptr;
+}
 
 static void free_plan(Group& g) {
     for (void* p : g.plan_allocs) dev_free(p, g.stream);
@@ -149,6 +169,10 @@ static RowLaunch bucket_launch(const Group& g, const Bucket& b, int mode, bool a
     L.max_n = b.max_n;
     L.max_points = b.max_pts;
     L.stage_xy = b.stage ? 1 : 0;
+    // rows dealt from the work counter when a CTA takes several at a time (a batch: +8 %
+    // on 256 island instances); one row per grab (the server's mix) costs more than it
+    // balances (-4 %), so those launches deal statically
+    L.work = (L.task_group > 1) ? g.work : nullptr;
     return L;
 }
 
@@ -512,12 +536,12 @@ int32_t brkga_batch_create(brkga_problem* const* problems, const brkga_params* p
     auto* b = new brkga_batch;
     b->g.device = dev;
     b->g.task_group = 8;
-    cudaError_t e = cudaStreamCreateWithFlags(&b->g.stream, cudaStreamNonBlocking);
-    if (e != cudaSuccess) {
-        delete b;
-        return cuda_fail(e, "stream");
+    int32_t st = group_start(b->g);
+    if (st != BRKGA_OK) {
+        brkga_batch_destroy(b);
+        return st;
     }
-    int32_t st = BRKGA_OK;
+    cudaError_t e = cudaSuccess;
     for (int i = 0; i < count && st == BRKGA_OK; ++i) {
         Member* m = nullptr;
         st = make_member(problem_data(problems[i]), params[i], b->g.stream, &m);
@@ -548,8 +572,7 @@ int32_t brkga_batch_destroy(brkga_batch* b) {
     free_plan(b->g);
     for (Member* m : b->g.members) release_member(m, b->g.stream);
     if (b->g.dd) dev_free(b->g.dd, b->g.stream);
-    cudaStreamSynchronize(b->g.stream);
-    cudaStreamDestroy(b->g.stream);
+    group_stop(b->g);
     delete b;
     return BRKGA_OK;
 }
@@ -773,10 +796,10 @@ int32_t brkga_server_create(const brkga_server_config* cfg, brkga_server** out) 
     auto* s = new brkga_server;
     s->cfg = *cfg;
     s->g.device = cfg->device;
-    cudaError_t e = cudaStreamCreateWithFlags(&s->g.stream, cudaStreamNonBlocking);
-    if (e != cudaSuccess) {
-        delete s;
-        return cuda_fail(e, "stream");
+    int32_t st = group_start(s->g);
+    if (st != BRKGA_OK) {
+        brkga_server_destroy(s);
+        return st;
     }
     size_t fr = 0, tot = 0;
     cudaMemGetInfo(&fr, &tot);
@@ -796,8 +819,7 @@ int32_t brkga_server_destroy(brkga_server* s) {
     if (s->g.dd) dev_free(s->g.dd, s->g.stream);
     if (s->d_best) dev_free(s->d_best, s->g.stream);
     if (s->d_gens) dev_free(s->d_gens, s->g.stream);
-    cudaStreamSynchronize(s->g.stream);
-    cudaStreamDestroy(s->g.stream);
+    group_stop(s->g);
     delete s;
     return BRKGA_OK;
 }

@@ -599,7 +599,7 @@ struct RowResidency {
     static constexpr int value = want < 1 ? 1 : (want > 32 ? 32 : want);
 };
 
-template <int BLOCK, int G>
+template <int BLOCK, int G, bool DYN>
 __global__ void __launch_bounds__(BLOCK, RowResidency<BLOCK, G>::value) row_kernel(RowLaunch L) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ PopDesc sd;
@@ -608,16 +608,28 @@ __global__ void __launch_bounds__(BLOCK, RowResidency<BLOCK, G>::value) row_kern
     __shared__ float red_f[32];
     __shared__ long long misc[4];
 
+    __shared__ int grab[2];
+
     const int t = threadIdx.x;
     const RowSmem s = carve(smem_raw, BLOCK, G, L.max_n, L.max_points);
     int cur_pid = -1;
     zero_counters<BLOCK, G>(s);
 
-    // tasks are dealt to CTAs in groups of K consecutive tasks, round robin: neighbouring
-    // rows of one population stay in one CTA (its descriptor and coordinates are staged
-    // once per group) while every CTA still gets a mix of the whole list
+    // tasks are dealt to CTAs in groups of K consecutive tasks: neighbouring rows of one
+    // population stay in one CTA (its descriptor and coordinates are staged once per
+    // group).  Statically, group g goes to CTA g % grid.  With dynamic dealing (DYN, the
+    // shared launches of batches and the server, whose rows differ in length and kind), a
+    // CTA takes the next group from the work counter whenever it finishes one, so no SM
+    // idles while another still holds several long rows.
     const int K = L.task_group > 1 ? L.task_group : 1;
-    for (int g0 = blockIdx.x * K; g0 < L.ntasks; g0 += gridDim.x * K)
+    if (DYN) {
+        if (t == 0) grab[0] = atomicAdd(L.work, K);
+        __syncthreads();
+    }
+    int round = 0;
+    for (int g0 = DYN ? grab[0] : blockIdx.x * K; g0 < L.ntasks;) {
+        int next = 0;
+        if (DYN && t == 0) next = atomicAdd(L.work, K);  // the following group, used after this one
     for (int task = g0; task < min(L.ntasks, g0 + K); ++task) {
         int pid = 0, r = task;
         if (L.tasks) {
@@ -967,6 +979,20 @@ __global__ void __launch_bounds__(BLOCK, RowResidency<BLOCK, G>::value) row_kern
             }
         }
         __syncthreads();
+    }
+        if (DYN) {
+            ++round;
+            if (t == 0) grab[round & 1] = next;
+            __syncthreads();
+            g0 = grab[round & 1];
+        } else {
+            g0 += gridDim.x * K;
+        }
+    }
+    if (DYN && t == 0 && atomicAdd(L.work + 1, 1) == (int)gridDim.x - 1) {
+        // every CTA has taken its last group: leave the counter zero for the next launch
+        L.work[0] = 0;
+        L.work[1] = 0;
     }
 }
 
@@ -1761,9 +1787,9 @@ int row_global_grid(int rows, int max_n) {
 
 using RowFn = void (*)(RowLaunch);
 
-static RowFn row_fn(const RowTile& t) {
+static RowFn row_fn(const RowTile& t, bool dyn = false) {
 #define BK_TILE(B, G) \
-    if (t.block == B && t.groups == G) return row_kernel<B, G>;
+    if (t.block == B && t.groups == G) return dyn ? row_kernel<B, G, true> : row_kernel<B, G, false>;
     BK_TILE(32, 1)
     BK_TILE(64, 1)
     BK_TILE(64, 2)
@@ -1827,6 +1853,7 @@ cudaError_t prepare_rows(const RowTile& tile, size_t smem, int* per_sm) {
     RowFn fn = row_fn(tile);
     if (!fn) return cudaErrorInvalidValue;
     cudaError_t e = raise_smem_limit(reinterpret_cast<const void*>(fn), smem);
+    if (e == cudaSuccess) e = raise_smem_limit(reinterpret_cast<const void*>(row_fn(tile, true)), smem);
     // the MO-VRP kernel has the same launch bounds and shared memory
     if (e == cudaSuccess) e = raise_smem_limit(reinterpret_cast<const void*>(movrp_fn(tile)), smem);
     if (e != cudaSuccess) return e;
@@ -1842,7 +1869,7 @@ cudaError_t launch_rows(const RowLaunch& L, int kind, const RowTile& tile, int g
         row_kernel_big<<<grid, kBigBlock, 0, s>>>(L);
         return cudaGetLastError();
     }
-    RowFn fn = (kind == MOVRP) ? movrp_fn(tile) : row_fn(tile);
+    RowFn fn = (kind == MOVRP) ? movrp_fn(tile) : row_fn(tile, L.work != nullptr);
     if (!fn) return cudaErrorInvalidValue;
     if (L.ntasks <= 0 || grid <= 0) return cudaSuccess;
     if (grid > L.ntasks) grid = L.ntasks;

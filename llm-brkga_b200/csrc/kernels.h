@@ -42,6 +42,9 @@ struct RowLaunch {
     void* gscratch;          // global-scratch kernel (RowTile{0,0}): grid slices of gstride bytes
     size_t gstride;
     int32_t task_group;      // tasks dealt to CTAs in groups of this many consecutive tasks (0, 1: one)
+    int32_t* work;           // dynamic dealing (batches and the server): [next group, CTAs done],
+                             // zero before the launch and left zero by its last CTA; nullptr:
+                             // group g goes to CTA g % grid
     int32_t ls_moves;        // MODE_LSEARCH: segment reversals per individual
     int32_t ls_force;        // MODE_LSEARCH: run whatever the generation (operator); rank q = row q
 };

@@ -686,11 +686,10 @@ __global__ void __cluster_dims__(kPeelCluster, 1, 1) __launch_bounds__(kPeelThre
     __shared__ uint32_t C[kCB][kPeelWords];  // count planes of the own words (two's complement)
     __shared__ uint32_t A[kPeelWords], V[kPeelWords];
     __shared__ uint32_t Floc[2][kPeelWords];  // own words of the next front, by front parity
-    __shared__ uint32_t Ffull[kPeelCluster * kPeelWords];
     __shared__ uint16_t list[kMaxPool];
+    __shared__ uint32_t s_nf[2];              // member count of front k, by front parity
     __shared__ uint32_t part[kPeelWarps][kDB][kPeelWords];
     __shared__ uint16_t r16[kPeelWords * 32];
-    __shared__ uint32_t wt32[32];
     cg::cluster_group cluster = cg::this_cluster();
     const int crank = (int)cluster.block_rank();
     PopDesc& d = dd[blockIdx.x / kPeelCluster];
@@ -723,6 +722,10 @@ __global__ void __cluster_dims__(kPeelCluster, 1, 1) __launch_bounds__(kPeelThre
         Floc[0][t] = z;
         for (uint32_t x = z; x; x &= x - 1) r16[32 * t + __ffs(x) - 1] = 0;
     }
+    if (t == 0) {
+        s_nf[0] = 0;
+        s_nf[1] = 0;
+    }
     cluster.sync();
     constexpr int NW = kPeelCluster * kPeelWords;
     int survivors = 0, rest = 0;
@@ -731,18 +734,28 @@ __global__ void __cluster_dims__(kPeelCluster, 1, 1) __launch_bounds__(kPeelThre
     int32_t* const ft = (crank == 0 && t == 0) ? d.nft : nullptr;
     int start = 0;
     for (int k = 0; k < N; ++k) {
-        // the whole front k, gathered from every CTA of the cluster
-        if (t < NW) {
-            const uint32_t* rem = cluster.map_shared_rank(&Floc[k & 1][0], t / kPeelWords);
-            Ffull[t] = rem[t % kPeelWords];
+        // the whole front k, gathered from every CTA of the cluster; its member list is
+        // filled through one shared-memory atomic per warp (the order of the list does
+        // not matter: the column sums, the crowding scan and the cut-front sort do not
+        // depend on it)
+        uint32_t fw = 0u;
+        if (t < NW) fw = cluster.map_shared_rank(&Floc[k & 1][0], t / kPeelWords)[t % kPeelWords];
+        {
+            const uint32_t pc = __popc(fw);
+            uint32_t inc = pc;  // inclusive prefix of the warp's counts
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+                if (lane >= o) inc += y;
+            }
+            uint32_t wbase = 0u;
+            if (lane == 31 && inc) wbase = atomicAdd(&s_nf[k & 1], inc);
+            uint32_t base = __shfl_sync(0xffffffffu, wbase, 31) + inc - pc;
+            for (uint32_t x = fw; x; x &= x - 1) list[base++] = (uint16_t)(32 * t + __ffs(x) - 1);
+            if (t == 0) s_nf[(k + 1) & 1] = 0u;  // read by every thread before the last barrier
         }
         __syncthreads();
-        const uint32_t pc = (t < NW) ? __popc(Ffull[t]) : 0u;
-        uint32_t nf = 0;
-        uint32_t base = block_exclusive_scan<kPeelThreads>(pc, wt32, &nf);
-        if (t < NW)
-            for (uint32_t x = Ffull[t]; x; x &= x - 1) list[base++] = (uint16_t)(32 * t + __ffs(x) - 1);
-        __syncthreads();
+        const uint32_t nf = s_nf[k & 1];
         if (nf == 0) {  // every CTA sees the same front
             if (ft) {
                 ft[0] = k;
