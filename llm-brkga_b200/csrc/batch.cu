@@ -700,6 +700,8 @@ size_t estimate_bytes(const brkga_problem_desc& d, const brkga_params& p) {
     case BRKGA_BITSP_COORDS: b += 2 * (n + 1) * 8; break;
     case BRKGA_BITSP_MATRIX: b += 2 * (n + 1) * (n + 1) * 4; break;
     case BRKGA_TSPJ: b += 2 * (n + 1) * (n + 1) * 4; break;
+    case BRKGA_KNAP_THRESHOLD:
+    case BRKGA_KNAP_GREEDY: b += n * 16; break;  // weights, values and the (weight, value) pairs
     default: b += n * 8;
     }
     return b + 4096;

@@ -113,6 +113,12 @@ int32_t make_problem(const brkga_problem_desc* d, int device, std::shared_ptr<Pr
         pd->w = (int32_t*)p;
         if (st == BRKGA_OK) st = upload(*pd, d->values, (size_t)n * 4, &p);
         pd->v = (int32_t*)p;
+        if (st == BRKGA_OK) {
+            std::vector<int2> wv(n);
+            for (int i = 0; i < n; ++i) wv[i] = make_int2(d->weights[i], d->values[i]);
+            st = upload(*pd, wv.data(), (size_t)n * sizeof(int2), &p);
+            pd->wv = (int2*)p;
+        }
         break;
     }
     case BRKGA_TSPJ: {
@@ -197,7 +203,7 @@ void fill_instance(PopDesc& d, const ProblemData& pd) {
     d.mat = pd.mat;
     d.mat2 = pd.mat2;
     d.w = pd.w;
-    d.v = pd.v;
+    d.wv = pd.wv;
     d.cap = pd.cap;
     d.capi = pd.capi;
     d.jt = pd.jt;

@@ -95,7 +95,7 @@ struct PopDesc {
     const float* mat;         // TSP [n][n]; bi-TSP [n+1][n+1]; TSPJ travel times [c+1][c+1] (n = 2c)
     const float* mat2;        // bi-TSP second matrix; TSPJ job durations [c+1][c+1]
     const int32_t* w;
-    const int32_t* v;
+    const int2* wv;           // knapsack: (weight, value) pairs (one load per item in key order)
     const float* jt;          // job scheduling: job times [n]
     int32_t machines;
     int32_t function;         // continuous: Function and bounds

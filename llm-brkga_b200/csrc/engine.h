@@ -67,6 +67,7 @@ struct ProblemData {
     float* mat2 = nullptr;
     int32_t* w = nullptr;
     int32_t* v = nullptr;
+    int2* wv = nullptr;      // knapsack: (weight, value) interleaved, one load per item
     float* jt = nullptr;     // job scheduling: job times
     int machines = 0;
     int function = 0;        // continuous: brkga_function, bounds

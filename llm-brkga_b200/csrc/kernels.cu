@@ -334,14 +334,12 @@ __device__ __forceinline__ void block_excl_scan_ll2(long long a, long long b, lo
 // the whole block, so the scans read on-chip data instead of one dependent round of loads
 // per 32 items.
 template <int BLOCK>
-__device__ float knap_greedy(const int32_t* perm, int n, const int32_t* __restrict__ w,
-                             const int32_t* __restrict__ v, long long C, long long* red,
-                             long long* shared_misc, int2* wv) {
+__device__ float knap_greedy(const int32_t* perm, int n, const int2* __restrict__ items, long long C,
+                             long long* red, long long* shared_misc, int2* wv) {
     const int t = threadIdx.x;
-    for (int p = t; p < n; p += BLOCK) {
-        const int it = perm[p];
-        wv[p] = make_int2(__ldg(w + it), __ldg(v + it));
-    }
+    // one 8-byte load per item from the interleaved (weight, value) table: an item's pair
+    // sits in one cache line, so the random gather touches half the lines of two tables
+    for (int p = t; p < n; p += BLOCK) wv[p] = __ldg(items + perm[p]);
     __syncthreads();
     const int ch = (n + BLOCK - 1) / BLOCK;
     const int p0 = t * ch, p1 = min(n, p0 + ch);
@@ -386,6 +384,9 @@ __device__ float knap_greedy(const int32_t* perm, int n, const int32_t* __restri
                 const int pos = b0 + 32 * c + t;
                 x[c] = (pos < n) ? wv[pos] : make_int2(INT_MAX, 0);
             }
+            // one vote for the 128 items: once the spare capacity is small most groups hold
+            // no item that fits, and the walk passes them without stepping chunk by chunk
+            if (!__any_sync(0xffffffffu, x[0].x <= r || x[1].x <= r || x[2].x <= r || x[3].x <= r)) continue;
 #pragma unroll
             for (int c = 0; c < 4; ++c) {
                 int cur = 0;
@@ -407,10 +408,9 @@ __device__ float knap_greedy(const int32_t* perm, int n, const int32_t* __restri
 // the same, called rather than inlined: in the one-group row kernels (48 registers) an
 // inlined copy spills registers on every kind's path
 template <int BLOCK>
-__device__ __noinline__ float knap_greedy_call(const int32_t* perm, int n, const int32_t* __restrict__ w,
-                                               const int32_t* __restrict__ v, long long C, long long* red,
-                                               long long* shared_misc, int2* wv) {
-    return knap_greedy<BLOCK>(perm, n, w, v, C, red, shared_misc, wv);
+__device__ __noinline__ float knap_greedy_call(const int32_t* perm, int n, const int2* __restrict__ items,
+                                               long long C, long long* red, long long* shared_misc, int2* wv) {
+    return knap_greedy<BLOCK>(perm, n, items, C, red, shared_misc, wv);
 }
 
 // TSPJ makespan (configs/tspj_config.hpp:555-585): the city tour from the depot (node 0)
@@ -879,7 +879,7 @@ __global__ void __launch_bounds__(BLOCK, RowResidency<BLOCK, G>::value) row_kern
                         const int i = 4 * (t + gg * BLOCK) + l;
                         if (i < n && k[gg][l] > 0.5f) {
                             tw += __ldg(sd.w + i);
-                            tv += __ldg(sd.v + i);
+                            tv += __ldg(&sd.wv[i].y);
                         }
                     }
                 tw = block_sum_ll<BLOCK>(tw, red_ll);
@@ -937,10 +937,10 @@ __global__ void __launch_bounds__(BLOCK, RowResidency<BLOCK, G>::value) row_kern
                     }, red_f, res);
                 } else if (kind == KNAP_GREEDY) {
                     if constexpr (G == 1)
-                        res[0] = knap_greedy_call<BLOCK>(s.perm, n, sd.w, sd.v, sd.capi, red_ll, misc,
+                        res[0] = knap_greedy_call<BLOCK>(s.perm, n, sd.wv, sd.capi, red_ll, misc,
                                                          reinterpret_cast<int2*>(s.sc));
                     else
-                        res[0] = knap_greedy<BLOCK>(s.perm, n, sd.w, sd.v, sd.capi, red_ll, misc,
+                        res[0] = knap_greedy<BLOCK>(s.perm, n, sd.wv, sd.capi, red_ll, misc,
                                                     reinterpret_cast<int2*>(s.sc));
                 } else if (kind == TSPJ) {
                     if constexpr (G == 1)
@@ -1180,7 +1180,7 @@ __global__ void __launch_bounds__(kBigBlock) row_kernel_big(RowLaunch L) {
             for (int i = t; i < n; i += BLOCK)
                 if (row[i] > 0.5f) {
                     tw += __ldg(sd.w + i);
-                    tv += __ldg(sd.v + i);
+                    tv += __ldg(&sd.wv[i].y);
                 }
             tw = block_sum_ll<BLOCK>(tw, red_ll);
             tv = block_sum_ll<BLOCK>(tv, red_ll);
@@ -1270,7 +1270,7 @@ __global__ void __launch_bounds__(kBigBlock) row_kernel_big(RowLaunch L) {
                     d[1] = __ldg(m1 + (size_t)a * np1 + b);
                 }, red_f, res);
             } else if (kind == KNAP_GREEDY) {
-                res[0] = knap_greedy<BLOCK>(perm, n, sd.w, sd.v, sd.capi, red_ll, misc, reinterpret_cast<int2*>(sc));
+                res[0] = knap_greedy<BLOCK>(perm, n, sd.wv, sd.capi, red_ll, misc, reinterpret_cast<int2*>(sc));
             } else if (kind == TSPJ) {
                 res[0] = tspj_makespan<BLOCK>(perm, n / 2, sd.mat, sd.mat2, red_f);
             }
