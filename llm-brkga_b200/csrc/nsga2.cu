@@ -986,35 +986,12 @@ __device__ __forceinline__ unsigned long long obj_key(float v, int j) {
     return ((unsigned long long)okey(v) << 32) | (uint32_t)j;
 }
 
-__global__ void __launch_bounds__(kFrontWarps * 32) nsga_front_crowd_kernel(PopDesc* dd) {
-    extern __shared__ uint2 fkeys[];  // [front size]: the staged front's (okey0, okey1)
-    __shared__ int s_front[3];        // staged front: rank, first position, size
-    const PopDesc& d = dd[blockIdx.y];
-    if (!select_active(d, 0)) return;
-    const int N = 2 * d.P;
-    const int32_t* __restrict__ ft = d.nft;
-    const int cut = __ldg(ft + 1);
-    const int end = (cut >= 0) ? __ldg(ft + 3 + cut) : N;  // positions of the fronts up to the cut
-    const int pos0 = blockIdx.x * kFrontWarps;
-    if (pos0 >= end) return;
-    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
-    const float2* __restrict__ f2 = reinterpret_cast<const float2*>(d.fit[d.cur]);
-    const int32_t* __restrict__ list = d.nlist;
-    if (t == 0) {
-        const int r0 = __ldg(d.domcnt + __ldg(list + pos0));
-        s_front[0] = r0;
-        s_front[1] = __ldg(ft + 2 + r0);
-        s_front[2] = __ldg(ft + 3 + r0) - s_front[1];
-    }
-    __syncthreads();
-    const int r0 = s_front[0], fs0 = s_front[1], size0 = s_front[2];
-    staged<kFrontWarps * 32, 4>(
-        size0, [&](int j) { return __ldg(f2 + __ldg(list + fs0 + j)); },
-        [&](int j, float2 v) { fkeys[j] = make_uint2(okey(v.x), okey(v.y)); });
-    __syncthreads();
-    const int pos = pos0 + w;
-    if (pos >= end) return;
-    const int i = __ldg(list + pos);
+// one pool point of nsga_front_crowd_kernel (one warp): the scan of its front, then lane
+// 0's crowding distance and survivor entries
+__device__ __forceinline__ void front_crowd_point(const PopDesc& d, const int32_t* __restrict__ ft,
+                                                  const float2* __restrict__ f2, const int32_t* __restrict__ list,
+                                                  const uint2* fkeys, int r0, int lane, int i, int cut,
+                                                  uint32_t* s_min) {
     const int r = __ldg(d.domcnt + i);
     const int fs = __ldg(ft + 2 + r), size = __ldg(ft + 3 + r) - fs;
     const float2 vi = __ldg(f2 + i);
@@ -1067,58 +1044,87 @@ __global__ void __launch_bounds__(kFrontWarps * 32) nsga_front_crowd_kernel(PopD
             d.nrank[q + 1] = r;
             d.ncd[q + 1] = cd;
         }
-        atomicMin(d.nfmin, (uint32_t)(sc.me0 >> 32));
+        atomicMin(s_min, (uint32_t)(sc.me0 >> 32));
     }
 }
 
-// Mode 0, one CTA per population: the cut front's entries sorted by (crowding descending,
-// index, copy), the first P - (entries before it) taken; then the generation's history
-// entry (the survivors' smallest first objective) and the minimum's reset.
-__global__ void __launch_bounds__(kNsgaBlock, 1) nsga_cut_kernel(PopDesc* dd) {
-    extern __shared__ unsigned long long ckeys[];
-    __shared__ float redf[32];
-    PopDesc& d = dd[blockIdx.x];
+__global__ void __launch_bounds__(kFrontWarps * 32) nsga_front_crowd_kernel(PopDesc* dd) {
+    extern __shared__ uint2 fkeys[];  // [front size]: the staged front's (okey0, okey1)
+    __shared__ int s_front[3];        // staged front: rank, first position, size
+    __shared__ uint32_t s_min;        // the CTA's smallest first-objective key among survivors
+    const PopDesc& d = dd[blockIdx.y];
     if (!select_active(d, 0)) return;
-    const int t = threadIdx.x;
-    const int P = d.P;
+    const int N = 2 * d.P;
     const int32_t* __restrict__ ft = d.nft;
-    const float* __restrict__ f = d.fit[d.cur];
-    const int cut = ft[1];
-    const int fs = ft[2 + cut], nc = ft[3 + cut] - fs;
-    const int mult = (cut == 0) ? 2 : 1;
-    const int rb = (cut == 0) ? 0 : fs + ft[3];
-    const int take = P - rb, E = nc * mult, K2 = npow2(E);
-    const int32_t* __restrict__ mem = d.nlist + fs;
-    for (int e = t; e < K2; e += kNsgaBlock) {
-        unsigned long long kk = ~0ull;
-        if (e < E) {
-            const int i = __ldg(mem + e / mult);
-            kk = ((unsigned long long)cd_key(__ldg(d.ncdp + i)) << 32) | ((unsigned long long)i << 1) |
-                 (unsigned long long)(e % mult);
-        }
-        ckeys[e] = kk;
+    const int cut = __ldg(ft + 1);
+    const int end = (cut >= 0) ? __ldg(ft + 3 + cut) : N;  // positions of the fronts up to the cut
+    const int pos0 = blockIdx.x * kFrontWarps;
+    if (pos0 >= end) return;
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    const float2* __restrict__ f2 = reinterpret_cast<const float2*>(d.fit[d.cur]);
+    const int32_t* __restrict__ list = d.nlist;
+    if (t == 0) {
+        const int r0 = __ldg(d.domcnt + __ldg(list + pos0));
+        s_front[0] = r0;
+        s_front[1] = __ldg(ft + 2 + r0);
+        s_front[2] = __ldg(ft + 3 + r0) - s_front[1];
+        s_min = 0xFFFFFFFFu;
     }
     __syncthreads();
-    bitonic_u64<kNsgaBlock>(ckeys, K2);
-    float fmin = INFINITY;
-    for (int k = t; k < take; k += kNsgaBlock) {
-        const int i = (int)((ckeys[k] >> 1) & 0x7FFFu);
-        const int q = rb + k;
-        d.nsel[q] = i;
-        d.nrank[q] = cut;
-        d.ncd[q] = __ldg(d.ncdp + i);
-        fmin = fminf(fmin, __ldg(f + 2 * i));
-    }
-    fmin = block_min_f(fmin, redf);
-    if (t == 0) {
-        const uint32_t k = *d.nfmin;
-        if (k != 0xFFFFFFFFu) fmin = fminf(fmin, __uint_as_float((k & 0x80000000u) ? (k & 0x7FFFFFFFu) : ~k));
-        *d.nfmin = 0xFFFFFFFFu;
-        if (d.history) {
-            const uint32_t g = d.gen + 1;
-            if ((int)g < d.hist_cap) d.history[g] = fmin;
+    const int r0 = s_front[0], fs0 = s_front[1], size0 = s_front[2];
+    staged<kFrontWarps * 32, 4>(
+        size0, [&](int j) { return __ldg(f2 + __ldg(list + fs0 + j)); },
+        [&](int j, float2 v) { fkeys[j] = make_uint2(okey(v.x), okey(v.y)); });
+    __syncthreads();
+    const int pos = pos0 + w;
+    if (pos < end) front_crowd_point(d, ft, f2, list, fkeys, r0, lane, __ldg(list + pos), cut, &s_min);
+    __syncthreads();
+    if (t == 0 && s_min != 0xFFFFFFFFu) atomicMin(d.nfmin, s_min);
+}
+
+// Mode 0, over the grid, one warp per member of the cut front: the member's place among
+// the front's entries in (crowding descending, index, copy) order, by counting the members
+// with a smaller (crowding key, index) (every CTA stages the front's keys), a first-front
+// point as two adjacent entries; entries before P - (entries of the whole fronts) become
+// survivors.  The survivors' smallest first objective goes into the atomic minimum that
+// the gather kernel's last CTA turns into the generation's history entry.
+__global__ void __launch_bounds__(kFrontWarps * 32) nsga_cut_kernel(PopDesc* dd) {
+    extern __shared__ unsigned long long ckeys[];  // [cut front size]
+    __shared__ uint32_t s_min;
+    const PopDesc& d = dd[blockIdx.y];
+    if (!select_active(d, 0)) return;
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    const int32_t* __restrict__ ft = d.nft;
+    const int cut = __ldg(ft + 1);
+    const int fs = __ldg(ft + 2 + cut), nc = __ldg(ft + 3 + cut) - fs;
+    const int j0 = blockIdx.x * kFrontWarps;
+    if (j0 >= nc) return;
+    const int mult = (cut == 0) ? 2 : 1;
+    const int rb = (cut == 0) ? 0 : fs + __ldg(ft + 3);
+    const int take = d.P - rb;
+    const int32_t* __restrict__ mem = d.nlist + fs;
+    staged<kFrontWarps * 32, 4>(
+        nc, [&](int j) { return __ldg(mem + j); },
+        [&](int j, int m) { ckeys[j] = ((unsigned long long)cd_key(__ldg(d.ncdp + m)) << 32) | (uint32_t)m; });
+    if (t == 0) s_min = 0xFFFFFFFFu;
+    __syncthreads();
+    const int j = j0 + w;
+    if (j < nc) {
+        const unsigned long long me = ckeys[j];
+        int c = 0;
+        for (int k = lane; k < nc; k += 32) c += (ckeys[k] < me) ? 1 : 0;
+#pragma unroll
+        for (int off = 16; off >= 1; off >>= 1) c += __shfl_xor_sync(0xffffffffu, c, off);
+        if (lane < mult && mult * c + lane < take) {
+            const int m = (int)(uint32_t)me, q = rb + mult * c + lane;
+            d.nsel[q] = m;
+            d.nrank[q] = cut;
+            d.ncd[q] = __ldg(d.ncdp + m);
+            atomicMin(&s_min, okey(__ldg(d.fit[d.cur] + 2 * m)));
         }
     }
+    __syncthreads();
+    if (t == 0 && s_min != 0xFFFFFFFFu) atomicMin(d.nfmin, s_min);
 }
 
 // crowding and (mode 0) survivors from the ranks and orders above; one CTA per population
@@ -1200,6 +1206,15 @@ __global__ void __launch_bounds__(kGatherWarps * 32) nsga_gather_kernel(PopDesc*
     if (threadIdx.x == 0) {
         __threadfence();
         if (atomicAdd(d.done, 1) == (int)gridDim.x - 1) {
+            // the generation's history entry: the survivors' smallest first objective (the
+            // crowding and cut kernels' atomic minimum of order keys; +inf when none is a
+            // number), then the minimum's reset
+            const uint32_t k = *d.nfmin;
+            const uint32_t g = d.gen + 1;
+            if (d.history && (int)g < d.hist_cap)
+                d.history[g] = (k == 0xFFFFFFFFu) ? INFINITY
+                                                  : __uint_as_float((k & 0x80000000u) ? (k & 0x7FFFFFFFu) : ~k);
+            *d.nfmin = 0xFFFFFFFFu;
             d.cur = cur ^ 1;
             d.gen += 1;
             d.advanced = 1;
@@ -1347,7 +1362,7 @@ cudaError_t nsga_prepare(int maxP) {
     if (e == cudaSuccess)
         e = raise_smem_limit(reinterpret_cast<const void*>(near_build_kernel), (size_t)((maxP + 31) / 32) * 32 * 8);
     if (e == cudaSuccess)
-        e = raise_smem_limit(reinterpret_cast<const void*>(nsga_cut_kernel), (size_t)npow2(4 * maxP) * 8);
+        e = raise_smem_limit(reinterpret_cast<const void*>(nsga_cut_kernel), (size_t)2 * maxP * 8);
     if (e == cudaSuccess)
         e = raise_smem_limit(reinterpret_cast<const void*>(nsga_front_crowd_kernel), (size_t)2 * maxP * sizeof(uint2));
     return e;
@@ -1385,7 +1400,8 @@ cudaError_t nsga_enqueue_select(PopDesc* dd, int npops, int maxP, int mode, cuda
         nsga_front_crowd_kernel<<<dim3((maxN + kFrontWarps - 1) / kFrontWarps, npops), kFrontWarps * 32,
                                   (size_t)maxN * sizeof(uint2), st>>>(dd);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
-        nsga_cut_kernel<<<npops, kNsgaBlock, (size_t)npow2(2 * maxN) * 8, st>>>(dd);
+        nsga_cut_kernel<<<dim3((maxN + kFrontWarps - 1) / kFrontWarps, npops), kFrontWarps * 32,
+                          (size_t)maxN * 8, st>>>(dd);
         return cudaGetLastError();
     }
     nsga_order_kernel<<<dim3((maxN + kOrdPerCta - 1) / kOrdPerCta, 2, npops), kOrdThreads, (size_t)maxN * 8, st>>>(
