@@ -614,6 +614,7 @@ __global__ void __launch_bounds__(BLOCK, RowResidency<BLOCK, G>::value) row_kern
     const RowSmem s = carve(smem_raw, BLOCK, G, L.max_n, L.max_points);
     int cur_pid = -1;
     zero_counters<BLOCK, G>(s);
+    dep_wait();  // shared memory only above this line
 
     // tasks are dealt to CTAs in groups of K consecutive tasks: neighbouring rows of one
     // population stay in one CTA (its descriptor and coordinates are staged once per
@@ -1313,6 +1314,7 @@ __host__ __device__ inline int next_pow2(int x) {
 __global__ void __launch_bounds__(RK_THREADS) rank_kernel(RankArgs a) {
     extern __shared__ unsigned long long rk_keys[];
     const int t = threadIdx.x, pop = blockIdx.y;
+    dep_wait();
     PopDesc* d = a.descs ? a.descs + pop : nullptr;
     int P, mx, m, buf = 0;
     const float* f;
@@ -1587,6 +1589,7 @@ __global__ void __launch_bounds__(BLOCK, RowResidency<BLOCK, G>::value) movrp_ro
     const RowSmem s = carve(smem_raw, BLOCK, G, L.max_n, L.max_points);
     int cur_pid = -1;
     zero_counters<BLOCK, G>(s);
+    dep_wait();  // shared memory only above this line
 
     for (int task = blockIdx.x; task < L.ntasks; task += gridDim.x) {
         int pid = 0, r = task;
@@ -1874,8 +1877,7 @@ cudaError_t launch_rows(const RowLaunch& L, int kind, const RowTile& tile, int g
     if (L.ntasks <= 0 || grid <= 0) return cudaSuccess;
     if (grid > L.ntasks) grid = L.ntasks;
     const size_t smem = row_smem_bytes(tile, L.max_n, L.max_points, kind, L.stage_xy != 0);
-    fn<<<grid, tile.block, smem, s>>>(L);
-    return cudaGetLastError();
+    return launch_dep(fn, dim3(grid), dim3(tile.block), smem, s, L);
 }
 
 cudaError_t launch_rows_auto(const RowLaunch& L, int kind, const RowTile& tile, cudaStream_t s) {
@@ -1896,24 +1898,21 @@ cudaError_t launch_sort_raw(const float* fit, int P, int segments, int maximize,
     if (P <= 0 || segments <= 0) return cudaSuccess;
     RankArgs a{nullptr, fit, sorted, P, maximize, 0, 0};
     dim3 grid((P + RK_CH - 1) / RK_CH, segments);
-    rank_kernel<<<grid, RK_THREADS, (size_t)P * 8, s>>>(a);
-    return cudaGetLastError();
+    return launch_dep(rank_kernel, grid, dim3(RK_THREADS), (size_t)P * 8, s, a);
 }
 
 cudaError_t launch_sort_pops(PopDesc* descs, int npops, int maxP, int flip, cudaStream_t s) {
     if (npops <= 0) return cudaSuccess;
     RankArgs a{descs, nullptr, nullptr, 0, 0, flip, 0};
     dim3 grid((maxP + RK_CH - 1) / RK_CH, npops);
-    rank_kernel<<<grid, RK_THREADS, (size_t)maxP * 8, s>>>(a);
-    return cudaGetLastError();
+    return launch_dep(rank_kernel, grid, dim3(RK_THREADS), (size_t)maxP * 8, s, a);
 }
 
 cudaError_t launch_sort_pops_after_ls(PopDesc* descs, int npops, int maxP, cudaStream_t s) {
     if (npops <= 0) return cudaSuccess;
     RankArgs a{descs, nullptr, nullptr, 0, 0, 0, 1};
     dim3 grid((maxP + RK_CH - 1) / RK_CH, npops);
-    rank_kernel<<<grid, RK_THREADS, (size_t)maxP * 8, s>>>(a);
-    return cudaGetLastError();
+    return launch_dep(rank_kernel, grid, dim3(RK_THREADS), (size_t)maxP * 8, s, a);
 }
 
 cudaError_t launch_migrate(PopDesc* descs, int ninst, int k, int migrants, int max_n, cudaStream_t s) {

@@ -92,4 +92,25 @@ cudaError_t launch_migrate(PopDesc* descs, int ninst, int k, int migrants, int m
 
 int device_sm_count();
 
+// Launch with programmatic stream serialization: the kernel is scheduled as the one before
+// it in the stream drains, and waits for it (dep_wait) before it touches global memory.
+// Only kernels that call dep_wait before any global-memory access are launched this way.
+template <typename... Args>
+inline cudaError_t launch_dep(void (*fn)(Args...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                              Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, fn, args...);
+    if (e != cudaSuccess) cudaGetLastError();  // the status is returned, not left behind
+    return e;
+}
+
 }  // namespace bk

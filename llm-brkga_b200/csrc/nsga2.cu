@@ -216,6 +216,7 @@ constexpr int kDom2ColGroups = 4;  // column groups: warp g of a row group takes
 constexpr int kDom2Warps = kDom2RowWarps * kDom2ColGroups;
 
 __global__ void __launch_bounds__(kDom2Warps * 32) dom2_build_kernel(DomArgs a) {
+    dep_wait();
     extern __shared__ float2 so[];  // [32 * ceil(N / 32)] objectives
     __shared__ int cpart[kDom2ColGroups][kDom2RowWarps * kDom2Rows];
     const float* obj;
@@ -682,6 +683,7 @@ constexpr int kPeelSlices = kPeelThreads / kPeelWords, kPeelWarps = kPeelThreads
 
 __global__ void __cluster_dims__(kPeelCluster, 1, 1) __launch_bounds__(kPeelThreads)
     nsga_peel_cluster_kernel(PopDesc* dd, int mode) {
+    dep_wait();
     namespace cg = cooperative_groups;
     __shared__ uint32_t C[kCB][kPeelWords];  // count planes of the own words (two's complement)
     __shared__ uint32_t A[kPeelWords], V[kPeelWords];
@@ -896,6 +898,7 @@ __global__ void __cluster_dims__(kPeelCluster, 1, 1) __launch_bounds__(kPeelThre
 constexpr int kOrdThreads = 1024, kOrdPerCta = kOrdThreads / 32;
 
 __global__ void __launch_bounds__(kOrdThreads) nsga_order_kernel(PopDesc* dd, int mode) {
+    dep_wait();
     extern __shared__ unsigned long long okeys[];  // [N]
     const PopDesc& d = dd[blockIdx.z];
     if (!select_active(d, mode)) return;
@@ -1049,6 +1052,7 @@ __device__ __forceinline__ void front_crowd_point(const PopDesc& d, const int32_
 }
 
 __global__ void __launch_bounds__(kFrontWarps * 32) nsga_front_crowd_kernel(PopDesc* dd) {
+    dep_wait();
     extern __shared__ uint2 fkeys[];  // [front size]: the staged front's (okey0, okey1)
     __shared__ int s_front[3];        // staged front: rank, first position, size
     __shared__ uint32_t s_min;        // the CTA's smallest first-objective key among survivors
@@ -1089,6 +1093,7 @@ __global__ void __launch_bounds__(kFrontWarps * 32) nsga_front_crowd_kernel(PopD
 // survivors.  The survivors' smallest first objective goes into the atomic minimum that
 // the gather kernel's last CTA turns into the generation's history entry.
 __global__ void __launch_bounds__(kFrontWarps * 32) nsga_cut_kernel(PopDesc* dd) {
+    dep_wait();
     extern __shared__ unsigned long long ckeys[];  // [cut front size]
     __shared__ uint32_t s_min;
     const PopDesc& d = dd[blockIdx.y];
@@ -1129,6 +1134,7 @@ __global__ void __launch_bounds__(kFrontWarps * 32) nsga_cut_kernel(PopDesc* dd)
 
 // crowding and (mode 0) survivors from the ranks and orders above; one CTA per population
 __global__ void __launch_bounds__(kNsgaBlock, 1) nsga_select_kernel(PopDesc* dd, int mode) {
+    dep_wait();
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ uint32_t wt32[32];
     __shared__ float redf[32];
@@ -1179,6 +1185,7 @@ __global__ void __launch_bounds__(kNsgaBlock) peel_op_kernel(int N, const uint32
 constexpr int kGatherWarps = 8;
 
 __global__ void __launch_bounds__(kGatherWarps * 32) nsga_gather_kernel(PopDesc* dd) {
+    dep_wait();
     PopDesc& d = dd[blockIdx.y];
     if (at_limit(d)) {
         if (blockIdx.x == 0 && threadIdx.x == 0) d.advanced = 0;
@@ -1239,6 +1246,7 @@ __device__ __forceinline__ bool div_due(const PopDesc& d) {
 constexpr int kNearWarps = 4, kNearRows = 4;
 
 __global__ void __launch_bounds__(kNearWarps * 32) near_build_kernel(PopDesc* dd) {
+    dep_wait();
     extern __shared__ float2 so[];  // [32 * ceil(P / 32)]
     const PopDesc& d = dd[blockIdx.y];
     if (!div_due(d)) return;
@@ -1273,6 +1281,7 @@ __global__ void __launch_bounds__(kNearWarps * 32) near_build_kernel(PopDesc* dd
 // are gathered in order into the other key buffer, which becomes the current one, and
 // *nu < P tells the refill and re-rank launches to run; otherwise *nu = P.
 __global__ void __launch_bounds__(kNsgaBlock) nsga_diversity_kernel(PopDesc* dd) {
+    dep_wait();
     constexpr int WP = kMaxPool / 2 / 32;
     __shared__ uint32_t U[WP], D[WP], Un[WP], Dn[WP];
     __shared__ uint32_t wt32[32];
@@ -1374,8 +1383,7 @@ static cudaError_t launch_dom2(const DomArgs& a, int maxN, int npops, cudaStream
     const size_t smem = (size_t)((maxN + 31) / 32) * 32 * sizeof(float2);
     cudaError_t e = raise_smem_limit(reinterpret_cast<const void*>(dom2_build_kernel), smem);
     if (e != cudaSuccess) return e;
-    dom2_build_kernel<<<dim3((maxN + RPC - 1) / RPC, npops), kDom2Warps * 32, smem, st>>>(a);
-    return cudaGetLastError();
+    return launch_dep(dom2_build_kernel, dim3((maxN + RPC - 1) / RPC, npops), dim3(kDom2Warps * 32), smem, st, a);
 }
 
 static cudaError_t launch_dom(PopDesc* dd, int npops, int maxN, int pool, int only_rebuilt, cudaStream_t st) {
@@ -1392,39 +1400,36 @@ cudaError_t nsga_enqueue_select(PopDesc* dd, int npops, int maxP, int mode, cuda
     const int maxN = (mode == 0) ? 2 * maxP : maxP;
     cudaError_t e = launch_dom(dd, npops, maxN, mode == 0 ? 1 : 0, mode == 2 ? 1 : 0, st);
     if (e != cudaSuccess) return e;
-    nsga_peel_cluster_kernel<<<npops * kPeelCluster, kPeelThreads, 0, st>>>(dd, mode);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    e = launch_dep(nsga_peel_cluster_kernel, dim3(npops * kPeelCluster), dim3(kPeelThreads), 0, st, dd, mode);
+    if (e != cudaSuccess) return e;
     if (mode == 0) {
         // a generation's pool: crowding and whole fronts from each point's own front, then
         // the cut front
-        nsga_front_crowd_kernel<<<dim3((maxN + kFrontWarps - 1) / kFrontWarps, npops), kFrontWarps * 32,
-                                  (size_t)maxN * sizeof(uint2), st>>>(dd);
-        if ((e = cudaGetLastError()) != cudaSuccess) return e;
-        nsga_cut_kernel<<<dim3((maxN + kFrontWarps - 1) / kFrontWarps, npops), kFrontWarps * 32,
-                          (size_t)maxN * 8, st>>>(dd);
-        return cudaGetLastError();
+        e = launch_dep(nsga_front_crowd_kernel, dim3((maxN + kFrontWarps - 1) / kFrontWarps, npops),
+                       dim3(kFrontWarps * 32), (size_t)maxN * sizeof(uint2), st, dd);
+        if (e != cudaSuccess) return e;
+        return launch_dep(nsga_cut_kernel, dim3((maxN + kFrontWarps - 1) / kFrontWarps, npops), dim3(kFrontWarps * 32),
+                          (size_t)maxN * 8, st, dd);
     }
-    nsga_order_kernel<<<dim3((maxN + kOrdPerCta - 1) / kOrdPerCta, 2, npops), kOrdThreads, (size_t)maxN * 8, st>>>(
-        dd, mode);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    nsga_select_kernel<<<npops, kNsgaBlock, sel_smem_bytes(maxN), st>>>(dd, mode);
-    return cudaGetLastError();
+    e = launch_dep(nsga_order_kernel, dim3((maxN + kOrdPerCta - 1) / kOrdPerCta, 2, npops), dim3(kOrdThreads),
+                   (size_t)maxN * 8, st, dd, mode);
+    if (e != cudaSuccess) return e;
+    return launch_dep(nsga_select_kernel, dim3(npops), dim3(kNsgaBlock), sel_smem_bytes(maxN), st, dd, mode);
 }
 
 cudaError_t nsga_enqueue_gather_finish(PopDesc* dd, int npops, int maxP, int maxld, cudaStream_t st) {
     (void)maxld;
-    nsga_gather_kernel<<<dim3((maxP + kGatherWarps - 1) / kGatherWarps, npops), kGatherWarps * 32, 0, st>>>(dd);
-    return cudaGetLastError();
+    return launch_dep(nsga_gather_kernel, dim3((maxP + kGatherWarps - 1) / kGatherWarps, npops),
+                      dim3(kGatherWarps * 32), 0, st, dd);
 }
 
 cudaError_t nsga_enqueue_diversity(PopDesc* dd, int npops, int maxP, cudaStream_t st) {
     constexpr int RPC = kNearWarps * kNearRows;
     const size_t smem = (size_t)((maxP + 31) / 32) * 32 * sizeof(float2);
-    near_build_kernel<<<dim3((maxP + RPC - 1) / RPC, npops), kNearWarps * 32, smem, st>>>(dd);
-    cudaError_t e = cudaGetLastError();
+    const cudaError_t e =
+        launch_dep(near_build_kernel, dim3((maxP + RPC - 1) / RPC, npops), dim3(kNearWarps * 32), smem, st, dd);
     if (e != cudaSuccess) return e;
-    nsga_diversity_kernel<<<npops, kNsgaBlock, 0, st>>>(dd);
-    return cudaGetLastError();
+    return launch_dep(nsga_diversity_kernel, dim3(npops), dim3(kNsgaBlock), 0, st, dd);
 }
 
 int32_t nsga_alloc(PopDesc& d, int P, double mut_rate, int div_interval, int Mn, std::vector<void*>& allocs,
