@@ -54,7 +54,7 @@ struct Group {
     PopDesc* dd = nullptr;
     int cap_desc = 0;
     int nb = 0, nn = 0;           // single-objective / NSGA-II descriptor counts
-    int maxP_b = 0, maxP_n = 0, maxld_n = 0;
+    int maxP_b = 0, maxP_n = 0;
     int k_mig = 0, mig_interval = 0, mig_count = 0, n_mig_inst = 0;
     std::vector<Bucket> bb, nbk;  // row-kernel buckets for each kind of population
     std::vector<void*> plan_allocs;
@@ -193,7 +193,7 @@ static int32_t build_plan(Group& g) {
         if (m->sh.mo) order.push_back(m);
     g.members = order;
     g.hd.clear();
-    g.nb = g.nn = g.maxP_b = g.maxP_n = g.maxld_n = 0;
+    g.nb = g.nn = g.maxP_b = g.maxP_n = 0;
     g.any_div = false;
     g.k_mig = g.mig_interval = g.mig_count = g.n_mig_inst = 0;
     for (Member* m : g.members) {
@@ -204,7 +204,6 @@ static int32_t build_plan(Group& g) {
         if (m->sh.mo) {
             ++g.nn;
             g.maxP_n = std::max(g.maxP_n, m->sh.Pi);
-            g.maxld_n = std::max(g.maxld_n, m->sh.ld);
             g.any_div = g.any_div || m->prm.diversity_interval > 0;
         } else {
             g.nb += m->sh.k;
@@ -277,8 +276,8 @@ static cudaError_t enqueue_generation(Group& g, bool mig) {
             if ((e = launch_rows(bucket_launch(g, b, MODE_NSGA_OFF, false), b.kind, b.tile, b.grid, g.stream)) !=
                 cudaSuccess)
                 return e;
+        // survivors, their rows into the other buffer and the buffer swap
         if ((e = nsga_enqueue_select(dn, g.nn, g.maxP_n, 0, g.stream)) != cudaSuccess) return e;
-        if ((e = nsga_enqueue_gather_finish(dn, g.nn, g.maxP_n, g.maxld_n, g.stream)) != cudaSuccess) return e;
         if (g.any_div) {
             if ((e = nsga_enqueue_diversity(dn, g.nn, g.maxP_n, g.stream)) != cudaSuccess) return e;
             for (const Bucket& b : g.nbk)

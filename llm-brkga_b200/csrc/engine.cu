@@ -725,7 +725,8 @@ int32_t brkga_get_pareto_front(brkga_engine* e, float* objectives, float* keys, 
 // an external problem (elite copies keep their fitness); the caller fills the fitness of
 // the pending rows; the commit is the elite partition (BRKGA: initially on the current
 // buffer, then with the buffer swap and generation advance of an ordinary generation) or
-// the NSGA-II selection, survivor gather and, when due, the diversity pass.
+// the NSGA-II selection (survivors moved into the other buffer) and, when due, the
+// diversity pass.
 
 // rows [first, first + count) of keys / fit (m values per row) are pending
 static void ext_pending(brkga_engine* e, int state, float* keys, float* fit, int first, int count) {
@@ -871,8 +872,7 @@ int32_t brkga_external_commit(brkga_engine* e) {
     } else if (state == 3) {
         err = nsga_enqueue_select(e->dd, 1, sh.Pi, 2, e->stream);  // re-rank the rebuilt population
     } else {
-        err = nsga_enqueue_select(e->dd, 1, sh.Pi, 0, e->stream);
-        if (err == cudaSuccess) err = nsga_enqueue_gather_finish(e->dd, 1, sh.Pi, sh.ld, e->stream);
+        err = nsga_enqueue_select(e->dd, 1, sh.Pi, 0, e->stream);  // survivors, rows, buffer swap
         if (err == cudaSuccess && nsga_diversity_due(e->nsga, e->gen + 1)) {
             err = nsga_enqueue_diversity(e->dd, 1, sh.Pi, e->stream);
             int32_t nu = sh.Pi;

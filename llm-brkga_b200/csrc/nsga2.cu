@@ -991,6 +991,39 @@ __device__ __forceinline__ unsigned long long obj_key(float v, int j) {
 
 // one pool point of nsga_front_crowd_kernel (one warp): the scan of its front, then lane
 // 0's crowding distance and survivor entries
+// A survivor's keys and objectives into the other buffer, at entry q (and q2 >= 0: the
+// second entry of a first-front point), by one warp: four 128-bit loads in flight per lane.
+__device__ __forceinline__ void copy_survivor(const PopDesc& d, int src_row, int q, int q2, int lane) {
+    const int ld4 = d.ld / 4, m = d.m, cur = d.cur;
+    const float4* src = reinterpret_cast<const float4*>(d.keys[cur]) + (size_t)src_row * ld4;
+    float4* dst = reinterpret_cast<float4*>(d.keys[cur ^ 1]) + (size_t)q * ld4;
+    float4* dst2 = (q2 >= 0) ? reinterpret_cast<float4*>(d.keys[cur ^ 1]) + (size_t)q2 * ld4 : nullptr;
+    int c = lane;
+    for (; c + 96 < ld4; c += 128) {
+        const float4 a0 = src[c], a1 = src[c + 32], a2 = src[c + 64], a3 = src[c + 96];
+        dst[c] = a0;
+        dst[c + 32] = a1;
+        dst[c + 64] = a2;
+        dst[c + 96] = a3;
+        if (dst2) {
+            dst2[c] = a0;
+            dst2[c + 32] = a1;
+            dst2[c + 64] = a2;
+            dst2[c + 96] = a3;
+        }
+    }
+    for (; c < ld4; c += 32) {
+        const float4 a = src[c];
+        dst[c] = a;
+        if (dst2) dst2[c] = a;
+    }
+    if (lane < m) {
+        const float v = d.fit[cur][(size_t)src_row * m + lane];
+        d.fit[cur ^ 1][(size_t)q * m + lane] = v;
+        if (q2 >= 0) d.fit[cur ^ 1][(size_t)q2 * m + lane] = v;
+    }
+}
+
 __device__ __forceinline__ void front_crowd_point(const PopDesc& d, const int32_t* __restrict__ ft,
                                                   const float2* __restrict__ f2, const int32_t* __restrict__ list,
                                                   const uint2* fkeys, int r0, int lane, int i, int cut,
@@ -1014,8 +1047,7 @@ __device__ __forceinline__ void front_crowd_point(const PopDesc& d, const int32_
             sc.add(obj_key(v.x, m), obj_key(v.y, m));
         }
     }
-    sc.reduce();
-    if (lane != 0) return;
+    sc.reduce();  // every lane holds the front's figures
     float cd = 0.0f;
 #pragma unroll
     for (int o = 0; o < 2; ++o) {
@@ -1036,18 +1068,21 @@ __device__ __forceinline__ void front_crowd_point(const PopDesc& d, const int32_
             }
         }
     }
-    d.ncdp[i] = cd;
+    if (lane == 0) d.ncdp[i] = cd;
     if (r < cut) {
         const int q = (r == 0) ? 2 * sc.below1 : fs + __ldg(ft + 3) + sc.below1;
-        d.nsel[q] = i;
-        d.nrank[q] = r;
-        d.ncd[q] = cd;
-        if (r == 0) {
-            d.nsel[q + 1] = i;
-            d.nrank[q + 1] = r;
-            d.ncd[q + 1] = cd;
+        if (lane == 0) {
+            d.nsel[q] = i;
+            d.nrank[q] = r;
+            d.ncd[q] = cd;
+            if (r == 0) {
+                d.nsel[q + 1] = i;
+                d.nrank[q + 1] = r;
+                d.ncd[q + 1] = cd;
+            }
+            atomicMin(s_min, (uint32_t)(sc.me0 >> 32));
         }
-        atomicMin(s_min, (uint32_t)(sc.me0 >> 32));
+        copy_survivor(d, i, q, (r == 0) ? q + 1 : -1, lane);
     }
 }
 
@@ -1090,46 +1125,71 @@ __global__ void __launch_bounds__(kFrontWarps * 32) nsga_front_crowd_kernel(PopD
 // the front's entries in (crowding descending, index, copy) order, by counting the members
 // with a smaller (crowding key, index) (every CTA stages the front's keys), a first-front
 // point as two adjacent entries; entries before P - (entries of the whole fronts) become
-// survivors.  The survivors' smallest first objective goes into the atomic minimum that
-// the gather kernel's last CTA turns into the generation's history entry.
+// survivors, and the warp copies their rows into the other buffer (the front kernel has
+// copied the whole fronts' rows).  The population's last CTA (completion counter) then
+// finishes the generation: the history entry from the survivors' smallest first objective
+// (the atomic minimum of order keys that both kernels feed), the buffer swap and the
+// generation count.
 __global__ void __launch_bounds__(kFrontWarps * 32) nsga_cut_kernel(PopDesc* dd) {
     dep_wait();
     extern __shared__ unsigned long long ckeys[];  // [cut front size]
     __shared__ uint32_t s_min;
-    const PopDesc& d = dd[blockIdx.y];
-    if (!select_active(d, 0)) return;
+    PopDesc& d = dd[blockIdx.y];
+    if (at_limit(d)) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) d.advanced = 0;
+        return;
+    }
     const int t = threadIdx.x, lane = t & 31, w = t >> 5;
     const int32_t* __restrict__ ft = d.nft;
     const int cut = __ldg(ft + 1);
     const int fs = __ldg(ft + 2 + cut), nc = __ldg(ft + 3 + cut) - fs;
     const int j0 = blockIdx.x * kFrontWarps;
-    if (j0 >= nc) return;
-    const int mult = (cut == 0) ? 2 : 1;
-    const int rb = (cut == 0) ? 0 : fs + __ldg(ft + 3);
-    const int take = d.P - rb;
-    const int32_t* __restrict__ mem = d.nlist + fs;
-    staged<kFrontWarps * 32, 4>(
-        nc, [&](int j) { return __ldg(mem + j); },
-        [&](int j, int m) { ckeys[j] = ((unsigned long long)cd_key(__ldg(d.ncdp + m)) << 32) | (uint32_t)m; });
     if (t == 0) s_min = 0xFFFFFFFFu;
-    __syncthreads();
-    const int j = j0 + w;
-    if (j < nc) {
-        const unsigned long long me = ckeys[j];
-        int c = 0;
-        for (int k = lane; k < nc; k += 32) c += (ckeys[k] < me) ? 1 : 0;
+    if (j0 < nc) {  // every CTA reaches the completion count below
+        const int mult = (cut == 0) ? 2 : 1;
+        const int rb = (cut == 0) ? 0 : fs + __ldg(ft + 3);
+        const int take = d.P - rb;
+        const int32_t* __restrict__ mem = d.nlist + fs;
+        staged<kFrontWarps * 32, 4>(
+            nc, [&](int j) { return __ldg(mem + j); },
+            [&](int j, int m) { ckeys[j] = ((unsigned long long)cd_key(__ldg(d.ncdp + m)) << 32) | (uint32_t)m; });
+        __syncthreads();
+        const int j = j0 + w;
+        if (j < nc) {
+            const unsigned long long me = ckeys[j];
+            int c = 0;
+            for (int k = lane; k < nc; k += 32) c += (ckeys[k] < me) ? 1 : 0;
 #pragma unroll
-        for (int off = 16; off >= 1; off >>= 1) c += __shfl_xor_sync(0xffffffffu, c, off);
-        if (lane < mult && mult * c + lane < take) {
-            const int m = (int)(uint32_t)me, q = rb + mult * c + lane;
-            d.nsel[q] = m;
-            d.nrank[q] = cut;
-            d.ncd[q] = __ldg(d.ncdp + m);
-            atomicMin(&s_min, okey(__ldg(d.fit[d.cur] + 2 * m)));
+            for (int off = 16; off >= 1; off >>= 1) c += __shfl_xor_sync(0xffffffffu, c, off);
+            const int m = (int)(uint32_t)me, q0 = rb + mult * c;
+            if (lane < mult && mult * c + lane < take) {
+                const int q = q0 + lane;
+                d.nsel[q] = m;
+                d.nrank[q] = cut;
+                d.ncd[q] = __ldg(d.ncdp + m);
+                atomicMin(&s_min, okey(__ldg(d.fit[d.cur] + 2 * m)));
+            }
+            if (mult * c < take) copy_survivor(d, m, q0, (mult == 2 && 2 * c + 1 < take) ? q0 + 1 : -1, lane);
         }
     }
     __syncthreads();
-    if (t == 0 && s_min != 0xFFFFFFFFu) atomicMin(d.nfmin, s_min);
+    if (t == 0) {
+        if (s_min != 0xFFFFFFFFu) atomicMin(d.nfmin, s_min);
+        __threadfence();
+        if (atomicAdd(d.done, 1) == (int)gridDim.x - 1) {
+            // +inf when no survivor's first objective is a number; then the minimum's reset
+            const uint32_t k = atomicExch(d.nfmin, 0xFFFFFFFFu);
+            const uint32_t g = d.gen + 1;
+            if (d.history && (int)g < d.hist_cap)
+                d.history[g] = (k == 0xFFFFFFFFu) ? INFINITY
+                                                  : __uint_as_float((k & 0x80000000u) ? (k & 0x7FFFFFFFu) : ~k);
+            d.cur ^= 1;
+            d.gen = g;
+            d.advanced = 1;
+            *d.done = 0;
+            __threadfence();
+        }
+    }
 }
 
 // crowding and (mode 0) survivors from the ranks and orders above; one CTA per population
@@ -1176,59 +1236,6 @@ __global__ void __launch_bounds__(kNsgaBlock) peel_op_kernel(int N, const uint32
     peel_ranks<kNsgaBlock>(N, S, Wmax, cnt, r16, ps, wt32);
     __syncthreads();
     for (int i = threadIdx.x; i < N; i += kNsgaBlock) rank[i] = r16[i];
-}
-
-// survivors -> the other pool buffer, rows [0, P), one warp per row (population
-// blockIdx.y); then the last CTA of the population (completion counter) swaps the pool
-// buffers and advances the generation.  A population at its generation limit only
-// records that it did not advance.
-constexpr int kGatherWarps = 8;
-
-__global__ void __launch_bounds__(kGatherWarps * 32) nsga_gather_kernel(PopDesc* dd) {
-    dep_wait();
-    PopDesc& d = dd[blockIdx.y];
-    if (at_limit(d)) {
-        if (blockIdx.x == 0 && threadIdx.x == 0) d.advanced = 0;
-        return;
-    }
-    const int P = d.P, ld4 = d.ld / 4, m = d.m, cur = d.cur;
-    const int lane = threadIdx.x & 31;
-    const int q = blockIdx.x * kGatherWarps + (threadIdx.x >> 5);
-    if (q < P) {
-        const size_t sq = (size_t)__ldg(d.nsel + q);
-        const float4* src = reinterpret_cast<const float4*>(d.keys[cur]) + sq * ld4;
-        float4* dst = reinterpret_cast<float4*>(d.keys[cur ^ 1]) + (size_t)q * ld4;
-        int c = lane;
-        for (; c + 96 < ld4; c += 128) {
-            const float4 a0 = src[c], a1 = src[c + 32], a2 = src[c + 64], a3 = src[c + 96];
-            dst[c] = a0;
-            dst[c + 32] = a1;
-            dst[c + 64] = a2;
-            dst[c + 96] = a3;
-        }
-        for (; c < ld4; c += 32) dst[c] = src[c];
-        if (lane < m) d.fit[cur ^ 1][(size_t)q * m + lane] = d.fit[cur][sq * m + lane];
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        if (atomicAdd(d.done, 1) == (int)gridDim.x - 1) {
-            // the generation's history entry: the survivors' smallest first objective (the
-            // crowding and cut kernels' atomic minimum of order keys; +inf when none is a
-            // number), then the minimum's reset
-            const uint32_t k = *d.nfmin;
-            const uint32_t g = d.gen + 1;
-            if (d.history && (int)g < d.hist_cap)
-                d.history[g] = (k == 0xFFFFFFFFu) ? INFINITY
-                                                  : __uint_as_float((k & 0x80000000u) ? (k & 0x7FFFFFFFu) : ~k);
-            *d.nfmin = 0xFFFFFFFFu;
-            d.cur = cur ^ 1;
-            d.gen += 1;
-            d.advanced = 1;
-            *d.done = 0;
-            __threadfence();
-        }
-    }
 }
 
 // ensure_minimum_diversity (core/population.hpp:130-182) runs after generation g when
@@ -1417,12 +1424,6 @@ cudaError_t nsga_enqueue_select(PopDesc* dd, int npops, int maxP, int mode, cuda
     return launch_dep(nsga_select_kernel, dim3(npops), dim3(kNsgaBlock), sel_smem_bytes(maxN), st, dd, mode);
 }
 
-cudaError_t nsga_enqueue_gather_finish(PopDesc* dd, int npops, int maxP, int maxld, cudaStream_t st) {
-    (void)maxld;
-    return launch_dep(nsga_gather_kernel, dim3((maxP + kGatherWarps - 1) / kGatherWarps, npops),
-                      dim3(kGatherWarps * 32), 0, st, dd);
-}
-
 cudaError_t nsga_enqueue_diversity(PopDesc* dd, int npops, int maxP, cudaStream_t st) {
     constexpr int RPC = kNearWarps * kNearRows;
     const size_t smem = (size_t)((maxP + 31) / 32) * 32 * sizeof(float2);
@@ -1545,9 +1546,9 @@ cudaError_t nsga_enqueue_generation(NsgaState& s, cudaStream_t st, bool with_div
     // offspring into pool rows [P, 2P) (core/solver.hpp:1019-1032) + their objectives
     cudaError_t e = launch_rows(nsga_rows(s, MODE_NSGA_OFF), s.kind, s.tile, s.grid, st);
     if (e != cudaSuccess) return e;
-    // ranks, crowding and survivors of the pool (core/population.hpp:409-517)
+    // ranks, crowding and survivors of the pool (core/population.hpp:409-517), the
+    // survivors' rows into the other buffer and the buffer swap
     if ((e = nsga_enqueue_select(s.dd, 1, s.P, 0, st)) != cudaSuccess) return e;
-    if ((e = nsga_enqueue_gather_finish(s.dd, 1, s.P, s.ld, st)) != cudaSuccess) return e;
     if (with_diversity && s.div_interval > 0) {
         // decided on the device: due this generation, and fewer than 70% unique
         if ((e = nsga_enqueue_diversity(s.dd, 1, s.P, st)) != cudaSuccess) return e;

@@ -32,9 +32,10 @@ int32_t nsga_alloc(PopDesc& d, int P, double mut_rate, int div_interval, int Mn,
                    size_t* bytes, cudaStream_t stream);
 int nsga_max_population();
 cudaError_t nsga_prepare(int maxP);
-// group launches over `npops` consecutive NSGA-II descriptors
+// group launches over `npops` consecutive NSGA-II descriptors; mode 0 (a generation's
+// pool) also moves the survivors' rows into the other buffer, swaps the buffers and
+// advances the generation
 cudaError_t nsga_enqueue_select(PopDesc* dd, int npops, int maxP, int mode, cudaStream_t st);
-cudaError_t nsga_enqueue_gather_finish(PopDesc* dd, int npops, int maxP, int maxld, cudaStream_t st);
 cudaError_t nsga_enqueue_diversity(PopDesc* dd, int npops, int maxP, cudaStream_t st);
 void nsga_release(NsgaState& s);
 void nsga_set_history(NsgaState& s, float* h, int cap);
