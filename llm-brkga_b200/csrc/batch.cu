@@ -692,7 +692,7 @@ size_t estimate_bytes(const brkga_problem_desc& d, const brkga_params& p) {
     const size_t rows = mo ? 2 * P : P;
     const size_t m = mo ? 2 : 1;
     size_t b = 2 * rows * ld * 4 + 2 * rows * m * 4 + rows * 4 + rows * 8 + 64 + (size_t)(p.max_generations + 2) * 4 * 4;
-    if (mo) b += rows * 4 * 3 + rows * ((rows + 31) / 32) * 4 + 64;
+    if (mo) b += rows * 4 * 4 + rows * ((rows + 31) / 32) * 4 + 64;
     switch (d.kind) {
     case BRKGA_TSP_COORDS: b += n * 8; break;
     case BRKGA_TSP_MATRIX: b += n * n * 4; break;

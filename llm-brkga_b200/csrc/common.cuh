@@ -140,11 +140,12 @@ struct PopDesc {
     uint32_t* domS;           // [2P][domW] dominance rows
     int32_t* domcnt;          // [2P] domination counts
     int32_t* nu;              // diversity pass: unique count, P when nothing was rebuilt
-    int32_t* nord;            // [2][2P] pool points in (rank, objective o, index) order
+    int32_t* nord;            // [2][2P] pool points in (rank, objective o, index) order, then
+                              // [2P] the pool's dominator counts (zero between generations)
     int32_t* nft;             // front table of the last peel: [0] ranks, [1] cut rank (-1: none),
                               // [2 + r] first position of rank r in rank order, [2 + ranks] = N
     float* ncdp;              // [2P] crowding distance of every pool point
-    int32_t* nlist;           // [2P] the last peel's fronts, members in index order, fronts in rank
+    int32_t* nlist;           // [2P] the last peel's fronts (members in no set order), fronts in rank
                               // order (front r at [nft[2 + r], nft[3 + r]); not the last front
                               // of a peel stopped at the cut)
     uint32_t* nfmin;          // survivors' smallest first objective (order key; all ones: none)

@@ -210,6 +210,88 @@ __device__ __forceinline__ void staged(int count, Ld ld, St st) {
     }
 }
 
+// A generation's pool (two objectives): the dominator counts are accumulated into a slot
+// after the two orders (nord + 2N, N = 2P), which is zero between generations: the peel
+// reads each count and clears it.
+__host__ __device__ inline int32_t* pool_counts(const PopDesc& d) { return d.nord + 4 * (size_t)d.P; }
+
+// 32 x 32 bit transpose across a warp: lane l holds row l on entry (bit c = element (l, c))
+// and column l on exit (bit r = element (r, l)); five exchange steps of halving blocks.
+__device__ __forceinline__ uint32_t warp_transpose32(uint32_t w, int lane) {
+    const uint32_t masks[5] = {0x0000FFFFu, 0x00FF00FFu, 0x0F0F0F0Fu, 0x33333333u, 0x55555555u};
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        const int s = 16 >> k;
+        const uint32_t m = masks[k];
+        const uint32_t y = __shfl_xor_sync(0xffffffffu, w, s);
+        w = (lane & s) ? ((w & ~m) | ((y & ~m) >> s)) : ((w & m) | ((y & m) << s));
+    }
+    return w;
+}
+
+// The pool's dominance rows, each unordered pair of 32-point blocks (I <= J) visited once
+// by one warp: for row r of block I against lane j of block J the four compares give
+// both directions.  Row words: block I's rows at word J directly; block J's rows at word
+// I from the other direction's ballots by a bit transpose.  Dominator counts by atomic
+// adds into pool_counts (a diagonal block adds only once).  The same compares as
+// dom2_build_kernel, so the same matrix and counts bit for bit; half the pair tests.
+constexpr int kSymWarps = 16;
+
+__global__ void __launch_bounds__(kSymWarps * 32) dom2_pool_kernel(PopDesc* dd) {
+    dep_wait();
+    __shared__ float2 srow[kSymWarps][32];
+    PopDesc& d = dd[blockIdx.y];
+    if (at_limit(d)) return;
+    const int N = 2 * d.P, W = (N + 31) / 32, Wmax = d.domW;
+    const int T = W * (W + 1) / 2;
+    const float2* __restrict__ o2 = reinterpret_cast<const float2*>(d.fit[d.cur]);
+    uint32_t* const S = d.domS;
+    int32_t* const acc = pool_counts(d);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    float2* const rows = srow[warp];
+    for (int tile = blockIdx.x * kSymWarps + warp; tile < T; tile += gridDim.x * kSymWarps) {
+        // tile = J (J + 1) / 2 + I with I <= J
+        int J = (int)((sqrtf(8.0f * (float)tile + 1.0f) - 1.0f) * 0.5f);
+        while (J * (J + 1) / 2 > tile) --J;
+        while ((J + 1) * (J + 2) / 2 <= tile) ++J;
+        const int I = tile - J * (J + 1) / 2;
+        const int i = 32 * I + lane, j = 32 * J + lane;
+        const float2 oi = (i < N) ? __ldg(o2 + i) : make_float2(NAN, NAN);
+        const float2 oj = (j < N) ? __ldg(o2 + j) : make_float2(NAN, NAN);
+        __syncwarp();
+        rows[lane] = oi;
+        __syncwarp();
+        uint32_t rw = 0u, cw = 0u;
+        int cj = 0;
+#pragma unroll 8
+        for (int r = 0; r < 32; ++r) {
+            const float2 a = rows[r];
+            const bool gt0 = a.x > oj.x, gt1 = a.y > oj.y;
+            const bool lt0 = a.x < oj.x, lt1 = a.y < oj.y;
+            const bool rdj = !gt0 && !gt1 && (lt0 || lt1);  // row 32 I + r dominates 32 J + lane
+            const uint32_t s1 = __ballot_sync(0xffffffffu, rdj);
+            const uint32_t s2 = __ballot_sync(0xffffffffu, !lt0 && !lt1 && (gt0 || gt1));
+            cj += rdj ? 1 : 0;
+            if (lane == r) {
+                rw = s1;
+                cw = s2;
+            }
+        }
+        if (i < N) {
+            S[(size_t)i * Wmax + J] = rw;
+            const int c = __popc(cw);  // points of block J dominating i
+            if (c) atomicAdd(acc + i, c);
+        }
+        if (I != J) {
+            const uint32_t tw = warp_transpose32(cw, lane);  // row j, word I
+            if (j < N) {
+                S[(size_t)j * Wmax + I] = tw;
+                if (cj) atomicAdd(acc + j, cj);
+            }
+        }
+    }
+}
+
 constexpr int kDom2Rows = 4;       // rows per warp
 constexpr int kDom2RowWarps = 4;   // row groups per CTA
 constexpr int kDom2ColGroups = 4;  // column groups: warp g of a row group takes the 32-word blocks b % 4 == g
@@ -702,10 +784,20 @@ __global__ void __cluster_dims__(kPeelCluster, 1, 1) __launch_bounds__(kPeelThre
     const int Wmax = d.domW;
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const int w0 = crank * kPeelWords;
-    // domination counts of the own columns -> count planes
+    // domination counts of the own columns -> count planes; a generation's pool takes them
+    // from the pool build's accumulator and leaves it zero for the next generation
+    int32_t* const pacc = (mode == 0) ? pool_counts(d) : nullptr;
     for (int wl = warp; wl < kPeelWords; wl += kPeelWarps) {
         const int w = w0 + wl, i = 32 * w + lane;
-        const int c = (w < W && i < N) ? __ldg(d.domcnt + i) : 0;
+        int c = 0;
+        if (w < W && i < N) {
+            if (pacc) {
+                c = pacc[i];
+                pacc[i] = 0;
+            } else {
+                c = __ldg(d.domcnt + i);
+            }
+        }
 #pragma unroll
         for (int b = 0; b < kCB; ++b) {
             const uint32_t pl = __ballot_sync(0xffffffffu, (c >> b) & 1);
@@ -1405,7 +1497,11 @@ static cudaError_t launch_dom(PopDesc* dd, int npops, int maxN, int pool, int on
 // ranks, crowding and (mode 0) survivors of every population of the group
 cudaError_t nsga_enqueue_select(PopDesc* dd, int npops, int maxP, int mode, cudaStream_t st) {
     const int maxN = (mode == 0) ? 2 * maxP : maxP;
-    cudaError_t e = launch_dom(dd, npops, maxN, mode == 0 ? 1 : 0, mode == 2 ? 1 : 0, st);
+    cudaError_t e;
+    if (mode == 0)
+        e = launch_dep(dom2_pool_kernel, dim3(2 * device_sm_count(), npops), dim3(kSymWarps * 32), 0, st, dd);
+    else
+        e = launch_dom(dd, npops, maxN, 0, mode == 2 ? 1 : 0, st);
     if (e != cudaSuccess) return e;
     e = launch_dep(nsga_peel_cluster_kernel, dim3(npops * kPeelCluster), dim3(kPeelThreads), 0, st, dd, mode);
     if (e != cudaSuccess) return e;
@@ -1458,8 +1554,12 @@ int32_t nsga_alloc(PopDesc& d, int P, double mut_rate, int div_interval, int Mn,
     d.domcnt = (int32_t*)p;
     if ((st = get(16, &p)) != BRKGA_OK) return st;
     d.nu = (int32_t*)p;
-    if ((st = get((size_t)2 * N * 4, &p)) != BRKGA_OK) return st;
+    if ((st = get((size_t)3 * N * 4, &p)) != BRKGA_OK) return st;  // two orders, then the pool counts
     d.nord = (int32_t*)p;
+    if (cudaMemsetAsync(d.nord + 2 * (size_t)N, 0, (size_t)N * 4, stream) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(BRKGA_ERR_CUDA, "NSGA-II state initialisation");
+    }
     if ((st = get((size_t)(N + 4) * 4, &p)) != BRKGA_OK) return st;
     d.nft = (int32_t*)p;
     if ((st = get((size_t)N * 4, &p)) != BRKGA_OK) return st;
