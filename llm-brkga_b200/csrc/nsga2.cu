@@ -249,15 +249,34 @@ __global__ void __launch_bounds__(kSymWarps * 32) dom2_pool_kernel(PopDesc* dd) 
     int32_t* const acc = pool_counts(d);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     float2* const rows = srow[warp];
-    for (int tile = blockIdx.x * kSymWarps + warp; tile < T; tile += gridDim.x * kSymWarps) {
-        // tile = J (J + 1) / 2 + I with I <= J
-        int J = (int)((sqrtf(8.0f * (float)tile + 1.0f) - 1.0f) * 0.5f);
+    // consecutive tiles go to different CTAs, so that every CTA (and SM) gets the same
+    // share; each warp loads the next tile's objectives before it works on the current one
+    const int nw = gridDim.x * kSymWarps;
+    auto block_pair = [](int tile, int& I, int& J) {  // tile = J (J + 1) / 2 + I with I <= J
+        J = (int)((sqrtf(8.0f * (float)tile + 1.0f) - 1.0f) * 0.5f);
         while (J * (J + 1) / 2 > tile) --J;
         while ((J + 1) * (J + 2) / 2 <= tile) ++J;
-        const int I = tile - J * (J + 1) / 2;
+        I = tile - J * (J + 1) / 2;
+    };
+    auto objectives = [&](int I, int J, float2& oi, float2& oj) {
         const int i = 32 * I + lane, j = 32 * J + lane;
-        const float2 oi = (i < N) ? __ldg(o2 + i) : make_float2(NAN, NAN);
-        const float2 oj = (j < N) ? __ldg(o2 + j) : make_float2(NAN, NAN);
+        oi = (i < N) ? __ldg(o2 + i) : make_float2(NAN, NAN);
+        oj = (j < N) ? __ldg(o2 + j) : make_float2(NAN, NAN);
+    };
+    int tile = warp * gridDim.x + blockIdx.x, I = 0, J = 0;
+    float2 oi = make_float2(NAN, NAN), oj = make_float2(NAN, NAN);
+    if (tile < T) {
+        block_pair(tile, I, J);
+        objectives(I, J, oi, oj);
+    }
+    for (; tile < T; tile += nw) {
+        int nI = 0, nJ = 0;
+        float2 noi = make_float2(NAN, NAN), noj = make_float2(NAN, NAN);
+        if (tile + nw < T) {
+            block_pair(tile + nw, nI, nJ);
+            objectives(nI, nJ, noi, noj);
+        }
+        const int i = 32 * I + lane, j = 32 * J + lane;
         __syncwarp();
         rows[lane] = oi;
         __syncwarp();
@@ -289,6 +308,10 @@ __global__ void __launch_bounds__(kSymWarps * 32) dom2_pool_kernel(PopDesc* dd) 
                 if (cj) atomicAdd(acc + j, cj);
             }
         }
+        I = nI;
+        J = nJ;
+        oi = noi;
+        oj = noj;
     }
 }
 
