@@ -130,8 +130,8 @@ __device__ __forceinline__ bool dominates_m(const float* a, const float* b, int 
 }
 
 struct DomArgs {
-    PopDesc* dd;          // engine mode: population blockIdx.y (objectives fit[cur], buffers)
-    int pool;             // engine mode: 1 = the 2P pool, 0 = the P population
+    PopDesc* dd;          // engine mode: the P population blockIdx.y (objectives fit[cur], buffers);
+                          // a generation's 2P pool goes through dom2_pool_kernel
     int only_rebuilt;     // engine mode: skip populations whose diversity pass kept them (*nu >= P)
     const float* obj;     // raw mode
     int rawN, m;
@@ -147,9 +147,8 @@ __global__ void dom_build_kernel(DomArgs a) {
     int32_t* cnt;
     if (a.dd) {
         const PopDesc& d = a.dd[blockIdx.y];
-        if (a.pool && at_limit(d)) return;
         if (a.only_rebuilt && (!d.advanced || __ldg(d.nu) >= d.P)) return;
-        N = a.pool ? 2 * d.P : d.P;
+        N = d.P;
         m = d.m;
         obj = d.fit[d.cur];
         S = d.domS;
@@ -330,9 +329,8 @@ __global__ void __launch_bounds__(kDom2Warps * 32) dom2_build_kernel(DomArgs a) 
     int32_t* cnt;
     if (a.dd) {
         const PopDesc& d = a.dd[blockIdx.y];
-        if (a.pool && at_limit(d)) return;
         if (a.only_rebuilt && (!d.advanced || __ldg(d.nu) >= d.P)) return;
-        N = a.pool ? 2 * d.P : d.P;
+        N = d.P;
         obj = d.fit[d.cur];
         S = d.domS;
         cnt = d.domcnt;
@@ -1508,11 +1506,10 @@ static cudaError_t launch_dom2(const DomArgs& a, int maxN, int npops, cudaStream
     return launch_dep(dom2_build_kernel, dim3((maxN + RPC - 1) / RPC, npops), dim3(kDom2Warps * 32), smem, st, a);
 }
 
-static cudaError_t launch_dom(PopDesc* dd, int npops, int maxN, int pool, int only_rebuilt, cudaStream_t st) {
+static cudaError_t launch_dom(PopDesc* dd, int npops, int maxN, int only_rebuilt, cudaStream_t st) {
     DomArgs a;
     std::memset(&a, 0, sizeof(a));
     a.dd = dd;
-    a.pool = pool;
     a.only_rebuilt = only_rebuilt;
     return launch_dom2(a, maxN, npops, st);
 }
@@ -1524,7 +1521,7 @@ cudaError_t nsga_enqueue_select(PopDesc* dd, int npops, int maxP, int mode, cuda
     if (mode == 0)
         e = launch_dep(dom2_pool_kernel, dim3(2 * device_sm_count(), npops), dim3(kSymWarps * 32), 0, st, dd);
     else
-        e = launch_dom(dd, npops, maxN, 0, mode == 2 ? 1 : 0, st);
+        e = launch_dom(dd, npops, maxN, mode == 2 ? 1 : 0, st);
     if (e != cudaSuccess) return e;
     e = launch_dep(nsga_peel_cluster_kernel, dim3(npops * kPeelCluster), dim3(kPeelThreads), 0, st, dd, mode);
     if (e != cudaSuccess) return e;
